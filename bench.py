@@ -1,0 +1,341 @@
+#!/usr/bin/env python
+"""Throughput of the colour-class Metropolis sweep on B200: spin-update attempts per ns.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
+
+One step = one sweep (every colour class of every replica) of the workload, inputs resident in HBM. The
+default workload is the 3D Heisenberg bcc colour sweep: 64^3 cells x 2 sites (524,288 sites), J1 = 1, J2 = 0.3,
+cubic K1 = 0.05, h = 0.1 along z, periodic, 64 replicas x 24 temperatures in [0.5, 2.5] (1,536 replicas,
+9.66 GB of float32 state: larger than L2, so no flush is needed between steps); fp32 unit vectors uniform on
+the sphere from seed 2 (drawn on the device), Philox key 1234 (+100000 per rank).
+
+Multi-GPU (torchrun, one rank per GPU): every rank sweeps its own 1,536 replicas (replicas shard with no
+exchange: weak scaling); the timed region is bracketed by barriers and the time is the max over ranks.
+
+The JSON line carries the device-timed `value`, an end-to-end `e2e` figure through the public Sampler API
+(per step: temperatures copied in from pinned host memory, the sweep, the FP64 observables and their copy back
+to the host), the HBM roofline of the dominant kernel (algorithmic bytes: 24 B per attempt = 3 float32 read +
+3 written), the sampled clocks, and the CPU baseline (the oracle port on the host cores).
+
+--impl reference times the reference's CPU path on the host: the reference itself is Python that generates
+Triton kernels and cannot travel to the GPU box, so its arithmetic is timed through the oracle port
+(oracle/cpu_sweep.c, all host threads; the NumPy restatement when the C port is not built).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+import torch
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+BYTES_PER_ATTEMPT = {"heisenberg-bcc": 24, "ising-sc-bitwise": 0.25, "ising-square": 2}
+FALLBACK_HBM_GBS = 6650.0
+
+
+# ------------------------------------------------------------------------------------------------ workloads
+def heisenberg_bcc(L=64):
+    from spin_colour_kernel_b200 import crystals as cr
+    from spin_colour_kernel_b200 import system as sy
+    c = cr.make("bcc", (1, 2))
+    return sy.System("Heisenberg bcc J1-J2", 3, c, (L, L, L), (True,) * 3, {1: 1.0, 2: 0.3}, h=(0.0, 0.0, 0.1),
+                     cubic_k1=np.full((2, L, L, L), 0.05, np.float32))
+
+
+def make_workload(name, rank, device):
+    from spin_colour_kernel_b200 import system as sy
+    from spin_colour_kernel_b200.sampler import Sampler
+    g = torch.Generator(device=device).manual_seed(2 + rank)
+    if name == "heisenberg-bcc":
+        s = heisenberg_bcc(64)
+        B = 1536
+        A = Sampler(s, B, device=device, seed=1234 + 100000 * rank)
+        T = torch.linspace(0.5, 2.5, 24).repeat_interleave(64)
+        S = torch.randn((B, 3) + s.shape, device=device, generator=g)
+        S = (S / S.norm(dim=1, keepdim=True)).contiguous()
+        cfg = {"workload": "heisenberg-bcc-64^3x2-J1J2-K1-hz", "replicas": B, "sites": s.nsite,
+               "temperatures": "24 linear in [0.5, 2.5], 64 replicas each", "spin_dtype": "float32",
+               "l2": "no flush: 9.66 GB state > 126 MB L2"}
+    elif name == "ising-sc-bitwise":
+        s = sy.ising("sc", 128)
+        B = 512                                   # one counter-legal instance of the 1024-replica workload
+        A = Sampler(s, B, device=device, seed=1 + 100000 * rank, bitwise=True)
+        T = torch.linspace(4.0, 5.0, 16)[:8].repeat_interleave(64)
+        S = A.pack(torch.randint(0, 2, (B, 1) + s.shape, device=device, generator=g, dtype=torch.int8) * 2 - 1)
+        cfg = {"workload": "ising-sc-128^3-bitwise-shared", "replicas": B, "sites": s.nsite,
+               "l2": "no flush: 128 MiB words ~ L2 size"}
+    elif name == "ising-square":
+        s = sy.ising("square", 32)
+        B = 32
+        A = Sampler(s, B, device=device, seed=1234 + 100000 * rank, packed=False)
+        T = torch.tensor([1.5, 2.0, 2.269, 3.0]).repeat_interleave(8)
+        S = A.init_spins(seed=0)
+        cfg = {"workload": "ising-square-32^2-int8", "replicas": B, "sites": s.nsite, "l2": "resident (32 KB)"}
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    A.set_temperature(T)
+    return s, A, S, T, cfg
+
+
+# ------------------------------------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.proc = None
+        self.out = None
+        try:
+            ident = str(torch.cuda.get_device_properties(device_index).uuid)
+            ident = ident if ident.startswith("GPU-") else f"GPU-{ident}"
+        except Exception:
+            ident = str(device_index)
+        self.ident = ident
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", self.ident, "-lms", "100"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def hbm_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def traffic_per_launch(kernel_tag):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary, or None."""
+    f = ROOT / "profiles" / f"{kernel_tag}.traffic.txt"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            return float(line.split(":")[1])
+    return None
+
+
+# ---------------------------------------------------------------------------------------------- CPU side
+def cpu_baseline(name, budget_s=15.0):
+    """The oracle port on the host cores over a bounded sample of the workload: (attempts/ns, cores, kind,
+    sample)."""
+    from oracle import native
+    if name != "heisenberg-bcc":
+        return None
+    s = heisenberg_bcc(64)
+    T = torch.linspace(0.5, 2.5, 24).repeat_interleave(64).numpy()
+    if native.available():
+        return native.time_heisenberg(s, T, budget_s)
+    from oracle import sweep as osw
+    g = np.random.default_rng(2)
+    x = g.standard_normal((1, 3) + s.shape).astype(np.float32)
+    x /= np.linalg.norm(x, axis=1, keepdims=True)
+    beta = np.asarray([np.float32(1.0) / np.float32(T[0])], np.float32)
+    t0 = time.perf_counter()
+    osw.sweep(s, x, beta, [1234, 0], 1, reps=[0])
+    dt = time.perf_counter() - t0
+    return {"value": s.nsite / (dt * 1e9), "unit": "attempts/ns", "cores": 1, "kind": "port",
+            "sample": "NumPy oracle: 1 replica x 1 sweep of the full 64^3 x 2 bcc lattice"}
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    name = args.workload
+    s = heisenberg_bcc(64)
+    T = torch.linspace(0.5, 2.5, 24).repeat_interleave(64).numpy()
+    from oracle import native
+    rates = []
+    if native.available():
+        for k in range(args.warmup + args.steps):
+            r = native.time_heisenberg(s, T, budget_s=0.0, sweeps=1, replicas=native.threads())
+            if k >= args.warmup:
+                rates.append(r["value"])
+        base = r
+    else:
+        base = cpu_baseline(name)
+        rates = [base["value"]]
+    v = float(np.median(rates))
+    cfg = {"workload": "heisenberg-bcc-64^3x2-J1J2-K1-hz", "replicas": 1536, "sites": s.nsite}
+    line = {"impl": "reference", "metric": "spin-update attempts/ns", "value": v, "unit": "attempts/ns",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
+            "cpu_baseline": {"value": v, "unit": "attempts/ns", "cores": base["cores"], "kind": base["kind"],
+                             "sample": base["sample"]},
+            "e2e": {"value": v, "unit": "attempts/ns", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------------------- main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--workload", default="heisenberg-bcc", choices=sorted(BYTES_PER_ATTEMPT))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = world > 1
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        return
+    import datetime
+    if dist:
+        import torch.distributed as tdist
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                 device_id=torch.device("cuda", local))
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    from spin_colour_kernel_b200 import build as bld
+    bld.build()
+    s, A, S, T, cfg = make_workload(args.workload, rank, device)
+    attempts_per_step = A.B * s.n_active
+    stream = torch.cuda.current_stream(device)
+    classes = list(A.classes)
+
+    def step(events=None):
+        if events is None:
+            A.sweep(S, 1)
+            return
+        for c, a in classes:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            A.class_update(S, c, a)
+            e1.record(stream)
+            events.append((e0, e1))
+        from spin_colour_kernel_b200 import _lib as L
+        L.check(L.lib().sck_advance(int(A.state.data_ptr()), 1, A._stream()))
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(device)
+    if dist:
+        tdist.barrier()
+    clocks = ClockSampler(device.index)
+    clocks.start()
+    time.sleep(0.25)
+    ev = []
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(args.steps):
+        step(ev)
+    t1.record(stream)
+    torch.cuda.synchronize(device)
+    clk = clocks.stop()
+    ms = t0.elapsed_time(t1)
+    kern_ms = sum(a.elapsed_time(b) for a, b in ev)
+    n_launch = len(ev)
+    if dist:
+        x = torch.tensor([ms], device=device)
+        tdist.all_reduce(x, op=tdist.ReduceOp.MAX)
+        ms = float(x.item())
+        tdist.barrier()
+
+    # end to end through the public API: temperatures in from pinned host memory, sweep, FP64 observables
+    # out to pinned host memory, every step
+    beta_h = (1.0 / T).to(torch.float32).pin_memory()
+    E = torch.empty(A.B, dtype=torch.float64, device=device)
+    M = torch.empty((A.B, s.b, s.n), dtype=torch.float64, device=device)
+    E_h = torch.empty(A.B, dtype=torch.float64).pin_memory()
+    M_h = torch.empty((A.B, s.b, s.n), dtype=torch.float64).pin_memory()
+    e2e_steps = max(3, args.steps // 2)
+    torch.cuda.synchronize(device)
+    if dist:
+        tdist.barrier()
+    u0, u1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    u0.record(stream)
+    for _ in range(e2e_steps):
+        A.beta[: A.B].copy_(beta_h, non_blocking=True)
+        A.sweep(S, 1)
+        A.observables(S, E, M)
+        E_h.copy_(E, non_blocking=True)
+        M_h.copy_(M, non_blocking=True)
+    u1.record(stream)
+    torch.cuda.synchronize(device)
+    e2e_ms = u0.elapsed_time(u1)
+    if dist:
+        x = torch.tensor([e2e_ms], device=device)
+        tdist.all_reduce(x, op=tdist.ReduceOp.MAX)
+        e2e_ms = float(x.item())
+
+    value = world * attempts_per_step * args.steps / (ms * 1e6)
+    e2e = world * attempts_per_step * e2e_steps / (e2e_ms * 1e6)
+    bpa = BYTES_PER_ATTEMPT[args.workload]
+    bytes_per_launch = attempts_per_step * bpa / len(classes)
+    achieved = bytes_per_launch / ((kern_ms / n_launch) * 1e-3) / 1e9
+    peak, peak_kind = hbm_peak()
+    traffic = traffic_per_launch(f"{args.workload}")
+    line = {
+        "metric": "spin-update attempts/ns", "value": value, "unit": "attempts/ns", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32" if s.n > 1 else "u32", "data": "synthetic",
+        "config": cfg,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "note": f"algorithmic {bpa} B/attempt; peak {peak_kind}; kernel = class update, "
+                             f"{n_launch} launches timed with CUDA events"},
+        "e2e": {"value": e2e, "unit": "attempts/ns", "h2d_bytes_per_step": int(beta_h.numel() * 4),
+                "d2h_bytes_per_step": int((E_h.numel() + M_h.numel()) * 8)},
+        "gpu_launches": n_launch + args.steps,
+        "clocks": clk,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args.workload)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        tdist.barrier()
+        tdist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,180 @@
+/*
+ * sck.h — C ABI of libsckb200.so: the colour-class Metropolis sweep of spin-colour-kernel on B200 (sm_100a).
+ *
+ * The reference crosses from host to device in exactly one place on this path: the launch of its generated
+ * Triton class kernel,
+ *     kernel[grid](src_ptr, dst_ptr, mask_ptr, k1_ptr, beta_ptr | p_ptr, state_ptr, x_only, row0[, nword],
+ *                  ALPHA=, COLOUR=, BLOCK=, SYNC=, STRIDE=, BX=, R=[, G=])
+ * (Spin_Colour_Kernel/generator.py:191-194, bitwise.py:278-281), issued only by Sampler._launch
+ * (sampler.py:191-232). This header replaces that launch and the Sampler methods built on it.
+ *
+ * Conventions (as in the reference):
+ *   - Device buffers are caller-owned and updated in place. `state` = {base_seed, sweep} (int64) lives on the
+ *     device; a sweep advances state[1] on the device, so a captured CUDA graph keeps the random stream.
+ *   - Every call is asynchronous on the given stream (a cudaStream_t passed as void*, NULL = default stream),
+ *     allocates nothing, synchronises nothing, and may be captured into a CUDA graph.
+ *   - Every function returns 0 (SCK_OK) or a negative SCK_ERR_* code; sck_last_error() explains the last
+ *     failure of the calling thread. Kernels never trap.
+ *   - Layout: S[B, n, b, L3, L2, L1] (x fastest; L3 = 1 in 2D) in the plan's storage type; packed and bitwise
+ *     storage hold W = ceil(B / 32) int32 words per site, bit j of word w = replica 32 w + j (1 = spin +1).
+ */
+#ifndef SCK_H
+#define SCK_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SCK_ABI_VERSION 1
+
+/* status codes */
+#define SCK_OK 0
+#define SCK_ERR_INVALID (-1)      /* bad descriptor or argument (ValueError in the reference) */
+#define SCK_ERR_COUNTER (-2)      /* replicas x sites >= 2^31 - 1: the int32 Philox counter would wrap */
+#define SCK_ERR_UNSUPPORTED (-3)  /* mode not available for this system (e.g. bitwise on a vector model) */
+#define SCK_ERR_CUDA (-4)         /* a CUDA runtime call failed */
+#define SCK_ERR_TIMEOUT (-5)      /* a bounded device-side wait gave up */
+
+/* storage / update modes (Sampler(packed=, bitwise=, independent=) in the reference) */
+#define SCK_MODE_INT8 0           /* Ising, int8 spins, per-replica Philox (generator.py, unpacked) */
+#define SCK_MODE_F32 1            /* any n, float32 components (XY, Heisenberg; Ising with spin_dtype=float32) */
+#define SCK_MODE_PACKED 2         /* Ising, 32 replicas per int32 word, per-replica Philox == SCK_MODE_INT8 */
+#define SCK_MODE_BITWISE 3        /* Ising multi-spin coding, one uniform per (word, site, sweep) */
+#define SCK_MODE_BITWISE_INDEP 4  /* Ising multi-spin coding, one 32-bit draw per (replica, site, sweep) */
+
+#define SCK_METROPOLIS 0
+#define SCK_BARKER 1
+
+#define SCK_MAX_BASIS 4
+#define SCK_MAX_BONDS 64          /* bonds leaving one sublattice */
+#define SCK_MAX_GROUPS 8          /* coupling groups (distinct J) per sublattice */
+#define SCK_MAX_EXTRA 8           /* bonds with an extra n x n matrix per sublattice */
+#define SCK_MAX_FACTORS 4         /* cyclic factors of the colouring group */
+
+/* One bond leaving sublattice `alpha`: (c, alpha) -> (c + d, alpha2). */
+typedef struct sck_bond {
+  int32_t alpha2;
+  int32_t d[3];                   /* cell offset along x, y, z (z = 0 in 2D) */
+  int32_t group;                  /* coupling group; bonds are listed group by group */
+  int32_t extra;                  /* slot of this bond's extra matrix, -1 if none */
+  double J64;                     /* isotropic coupling of the bond's shell (FP64, for observables) */
+} sck_bond;
+
+/* The bonds of one sublattice in local-field accumulation order: coupling groups in first-appearance
+ * order of their float J over the bond table, members in table order (generator.py:219-224). */
+typedef struct sck_sublattice {
+  int32_t n_bonds;
+  int32_t n_groups;
+  int32_t group_end[SCK_MAX_GROUPS];   /* bonds [group_end[g-1], group_end[g]) belong to group g */
+  float group_J[SCK_MAX_GROUPS];       /* float32 J of the group */
+  int32_t group_apply[SCK_MAX_GROUPS]; /* 0: J == 0, the group is loaded only for its extra matrices */
+  int32_t n_extra;                     /* extra slots, in bond-table order */
+  float extra[SCK_MAX_EXTRA][9];       /* float32 n x n matrix, row-major in a 3 x 3 block */
+  double extra64[SCK_MAX_EXTRA][9];    /* FP64 copy for observables */
+  sck_bond bonds[SCK_MAX_BONDS];
+} sck_sublattice;
+
+/* A validated system (Spin_Colour_Kernel/system.py:19-98) with its linear colouring
+ * gamma(c, alpha) = K c + o_alpha (mod m), colour index mixed-radix over the factors (colouring.py:30-36). */
+typedef struct sck_system_desc {
+  int32_t abi_version;            /* SCK_ABI_VERSION */
+  int32_t n;                      /* spin components: 1, 2 or 3 */
+  int32_t dim;                    /* lattice dimension: 2 or 3 */
+  int32_t b;                      /* basis sites */
+  int32_t L[3];                   /* L1, L2, L3 cells (L3 = 1 in 2D) */
+  int32_t periodic[3];
+  int32_t acceptance;             /* SCK_METROPOLIS or SCK_BARKER */
+  int32_t has_mask;               /* a site mask is passed with every call */
+  int32_t has_cubic;              /* per-site k1 is passed with every call (n = 3 only) */
+  float h[3];                     /* float32 field; components equal to 0 are skipped */
+  double h64[3];
+  float k2;                       /* (sx sy sz)^2 coefficient */
+  double k2_64;
+  int32_t n_factors;              /* colouring factors r (0 = one colour) */
+  int32_t m[SCK_MAX_FACTORS];
+  int32_t K[SCK_MAX_FACTORS][3];
+  int32_t o[SCK_MAX_BASIS][SCK_MAX_FACTORS];
+  int32_t n_classes;              /* sweep order: (colour, alpha) pairs, colour-major, empty classes skipped */
+  int32_t classes[128][2];
+  sck_sublattice sub[SCK_MAX_BASIS];
+} sck_system_desc;
+
+/* Device buffers of one sampler (caller-owned). */
+typedef struct sck_buffers {
+  void* spins;                    /* S in the plan's storage type, updated in place */
+  const int8_t* mask;             /* b*L3*L2*L1 bytes, nonzero = spin present; NULL without a mask */
+  const float* k1;                /* b*L3*L2*L1 floats; NULL without cubic anisotropy */
+  const float* beta;              /* one float32 inverse temperature per computed replica */
+  const void* table;              /* acceptance table: see sck_plan_table_size */
+  int64_t* state;                 /* {base_seed, sweep} */
+} sck_buffers;
+
+typedef struct sck_plan sck_plan;
+
+/* Build a plan (host-only; no device memory) for `batch` replicas in `mode`. Errors: SCK_ERR_INVALID for a
+ * malformed descriptor, SCK_ERR_COUNTER when ceil(batch) * sites >= 2^31 - 1 (sampler.py:73-74),
+ * SCK_ERR_UNSUPPORTED for a mode the system cannot run (bitwise.py:59-71, sampler.py:62-63). */
+int sck_plan_create(const sck_system_desc* desc, int32_t batch, int32_t mode, sck_plan** out);
+int sck_plan_destroy(sck_plan* plan);
+
+/* Size in elements of the acceptance table the plan reads, and its element size in bytes:
+ *   INT8 / F32 Ising / PACKED: float32 e[Bp][b][keys] with e = exp(-beta dE) (Metropolis) or exp(beta dE)
+ *       (Barker) for every reachable Ising energy change, built by the host with the same float32 arithmetic
+ *       and exp as the reference's CPU path; keys per sublattice via *keys (may be NULL).
+ *   F32 vector models: no table (0).
+ *   BITWISE: float32 p[W][2][Z+1][Z+1] (bitwise.py:79-84).  BITWISE_INDEP: int64 P[W][2][Z+1][Z+1] (:87-93). */
+int sck_plan_table_size(const sck_plan* plan, int64_t* elements, int32_t* element_bytes, int32_t* keys);
+
+/* Replicas the kernels compute (B, or 32 W for packed storage) and the number of storage rows (B or W). */
+int sck_plan_shape(const sck_plan* plan, int32_t* computed_replicas, int32_t* rows);
+
+/* One class launch: every site of class (colour, alpha) of every replica, read from `src`, written to
+ * `buf->spins` (src may equal buf->spins). colour < 0 with sync != 0 is the synchronous control (every site of
+ * the sublattice from `src`). Replaces kernel[grid](...) of generator.py:191 / bitwise.py:278. */
+int sck_class_update(const sck_plan* plan, const sck_buffers* buf, const void* src, int32_t colour,
+                     int32_t alpha, int32_t sync, void* stream);
+
+/* n_sweeps sweeps in place (Sampler.sweep, sampler.py:234-240): all classes in order, then state[1] += 1. */
+int sck_sweep(const sck_plan* plan, const sck_buffers* buf, int32_t n_sweeps, void* stream);
+
+/* Synchronous control (Sampler.sync_sweep, sampler.py:271-279): every site from the previous state;
+ * `scratch` is a caller buffer the size of the spins. */
+int sck_sync_sweep(const sck_plan* plan, const sck_buffers* buf, void* scratch, int32_t n_sweeps, void* stream);
+
+/* Sequential reference chain (Sampler.reference_sweep, sampler.py:281-293): class by class, sites one at a
+ * time in raster order (z, y, x), same counters. One thread (or warp of 32 replicas) per replica; for small
+ * systems and checks only. */
+int sck_reference_sweep(const sck_plan* plan, const sck_buffers* buf, int32_t n_sweeps, void* stream);
+
+/* FP64 observables (Sampler.energy / magnetization, sampler.py:296-345) of `batch` replicas stored as
+ * `storage` (SCK_MODE_INT8: int8 spins, SCK_MODE_F32: float32 components, SCK_MODE_PACKED: int32 words):
+ *   E[r]            = -1/2 sum_i s_i . v_i - sum_i h . s_i + sum_i a(s_i)   (r < batch)
+ *   M[r][alpha][k]  = sum over sublattice alpha of s_k                       (batch x b x n doubles)
+ * `workspace` holds per-block partial sums; its size in bytes comes from sck_observables_workspace_size.
+ * Either output may be NULL. Deterministic: the partials are summed in a fixed order. */
+int sck_observables_workspace_size(const sck_plan* plan, int32_t batch, int64_t* bytes);
+int sck_observables(const sck_plan* plan, const sck_buffers* buf, const void* spins, int32_t storage,
+                    int32_t batch, double* E, double* M, void* workspace, void* stream);
+
+/* Storage conversion (Sampler.pack / unpack, sampler.py:169-188). pack: int8 spins [B, 1, b, L3, L2, L1]
+ * (+-1, 0 masked) -> int32 words [W, 1, b, L3, L2, L1] (padding replicas 0). unpack: words -> int8 spins,
+ * masked sites 0. */
+int sck_pack(const sck_plan* plan, const int8_t* spins, int32_t* words, void* stream);
+int sck_unpack(const sck_plan* plan, const int32_t* words, const int8_t* mask, int8_t* spins, void* stream);
+
+/* Advance state[1] by `n` on the device (what a sweep does after its class launches). */
+int sck_advance(int64_t* state, int32_t n, void* stream);
+
+const char* sck_last_error(void);
+int sck_abi_version(void);
+
+/* sizeof of the ABI structs as compiled into the library, for FFI bindings to check their mirrors. */
+int sck_struct_sizes(int64_t* system_desc, int64_t* sublattice, int64_t* bond, int64_t* buffers);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SCK_H */

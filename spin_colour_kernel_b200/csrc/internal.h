@@ -1,0 +1,95 @@
+// Host-side plan and the launch parameter blocks shared by the translation units of libsckb200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "common.cuh"
+
+namespace sck {
+
+// Everything a class launch needs except the bond list of its sublattice.
+struct Common {
+  Geometry g;
+  Colouring col;
+  int B;             // replicas the kernel computes (32 W for packed storage)
+  int W;             // words per site (packed / bitwise)
+  int P, bx, rows;   // x-period of the colouring, class sites per row (ceil(L1 / P)), rows = L3 * L2
+  float h[3];
+  int hnz[3];
+  float k2;
+  int keys;          // Ising acceptance-table keys per sublattice
+  int lut_rep_stride;
+  int Z1, NT, field; // bitwise table: Z + 1, 2 (Z + 1)^2, field present
+  const void* src;
+  void* dst;
+  const int8_t* mask;
+  const float* k1;
+  const float* beta;
+  const void* table;
+  const int64_t* state;
+};
+
+struct ClassParams {
+  Common c;
+  SubDev sub;
+  int colour, alpha;
+};
+
+struct SeqParams {
+  Common c;
+  SubDev sub[SCK_MAX_BASIS];
+  int n_classes;
+  int classes[128][2];
+};
+
+struct ObsParams {
+  Geometry g;
+  int B, storage;    // 0 int8, 1 float32, 2 packed words
+  SubDev sub[SCK_MAX_BASIS];
+  SubObs obs[SCK_MAX_BASIS];
+  double h64[3];
+  double k2;
+  int blocks_per_rep;
+  const void* spins;
+  const int8_t* mask;
+  const float* k1;
+  double* partial;
+};
+
+constexpr int OBS_VALUES = 16;   // E + b * n magnetization sums (<= 12), padded
+
+}  // namespace sck
+
+struct sck_plan {
+  sck_system_desc desc;
+  sck::Geometry geom;
+  sck::Colouring col;
+  sck::SubDev sub[SCK_MAX_BASIS];
+  sck::SubObs obs[SCK_MAX_BASIS];
+  int mode, batch;
+  int Bp, W, rows_storage;
+  int P, bx;
+  int keys;
+  int Z, Z1, NP, field;
+  int ising_lut;   // Ising chain with the host-built exp table (INT8, F32 with n = 1, PACKED)
+};
+
+namespace sck {
+void set_error(const std::string& msg);
+int cuda_status(cudaError_t e, const char* where);
+
+// launchers (return SCK_OK or an error code)
+int launch_class(const sck_plan* plan, const Common& c, int colour, int alpha, cudaStream_t s);
+int launch_sequential(const sck_plan* plan, const Common& c, cudaStream_t s);
+int launch_bitwise_class(const sck_plan* plan, const Common& c, int colour, int alpha, cudaStream_t s);
+int launch_bitwise_sequential(const sck_plan* plan, const Common& c, cudaStream_t s);
+int obs_blocks_per_rep(const sck_plan* plan, int batch);
+int launch_observables(const sck_plan* plan, const void* spins, int storage, int batch, const int8_t* mask,
+                       const float* k1, double* E, double* M, void* workspace, cudaStream_t s);
+int launch_pack(const sck_plan* plan, const int8_t* spins, int32_t* words, cudaStream_t s);
+int launch_unpack(const sck_plan* plan, const int32_t* words, const int8_t* mask, int8_t* spins, cudaStream_t s);
+int launch_advance(int64_t* state, int n, cudaStream_t s);
+}  // namespace sck

@@ -1,0 +1,154 @@
+// FP64 observables (Spin_Colour_Kernel/sampler.py:296-345): energy per replica and per-sublattice
+// magnetization, read directly from int8, float32 or packed-word storage.
+//
+// Grid (blocks_per_rep, B). A thread walks sites of one replica; per site it forms the bond field
+// v_i = sum_b (J_b I + E_b) s_j in FP64, the site energy -1/2 s.v - h.s + k1 ((sx sy)^2 + (sx sz)^2 + (sy sz)^2)
+// + k2 (sx sy sz)^2 and its contribution to M[alpha][k]. Warp shuffles, then shared memory, reduce a block to one
+// partial per value; a second kernel sums the partials of a replica in block order, so results do not depend
+// on scheduling.
+#include "internal.h"
+
+namespace sck {
+
+template <int N, int STORE>
+__device__ __forceinline__ void load_spin(const ObsParams& p, int rep, int site, double (&s)[N]) {
+  const Geometry& g = p.g;
+  if constexpr (STORE == 2) {
+    const uint32_t w = ((const uint32_t*)p.spins)[(size_t)(rep >> 5) * g.nsite + site];
+    const bool present = p.mask == nullptr || p.mask[site] != 0;
+    s[0] = present ? (((w >> (rep & 31)) & 1u) ? 1.0 : -1.0) : 0.0;
+  } else if constexpr (STORE == 0) {
+    s[0] = (double)((const int8_t*)p.spins)[(size_t)rep * g.nsite + site];
+  } else {
+#pragma unroll
+    for (int k = 0; k < N; ++k) s[k] = (double)((const float*)p.spins)[((size_t)rep * N + k) * g.nsite + site];
+  }
+}
+
+template <int N, int STORE>
+__global__ void __launch_bounds__(256) observables_kernel(const __grid_constant__ ObsParams p) {
+  const Geometry& g = p.g;
+  const int rep = blockIdx.y;
+  constexpr int NV = 1 + SCK_MAX_BASIS * N;
+  double acc[NV];
+#pragma unroll
+  for (int i = 0; i < NV; ++i) acc[i] = 0.0;
+  for (int site = blockIdx.x * blockDim.x + threadIdx.x; site < g.nsite; site += p.blocks_per_rep * blockDim.x) {
+    if (p.mask != nullptr && p.mask[site] == 0) continue;
+    const int alpha = site / g.plane;
+    const int rem = site - alpha * g.plane;
+    const int z = rem / (g.L2 * g.L1);
+    const int y = (rem / g.L1) % g.L2;
+    const int x = rem % g.L1;
+    double s[N];
+    load_spin<N, STORE>(p, rep, site, s);
+    double v[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) v[k] = 0.0;
+    const SubDev& sub = p.sub[alpha];
+    const SubObs& ob = p.obs[alpha];
+    for (int bi = 0; bi < sub.n_bonds; ++bi) {
+      const BondDev bd = sub.bonds[bi];
+      const int q = neighbour_index(g, bd, x, y, z);
+      if (q < 0) continue;
+      double t[N];
+      load_spin<N, STORE>(p, rep, q, t);
+      const double J = ob.J[bi];
+#pragma unroll
+      for (int k = 0; k < N; ++k) v[k] += J * t[k];
+      if (bd.extra >= 0) {
+#pragma unroll
+        for (int k = 0; k < N; ++k)
+#pragma unroll
+          for (int l = 0; l < N; ++l) v[k] += ob.E[bd.extra][3 * k + l] * t[l];
+      }
+    }
+    double e = 0.0;
+#pragma unroll
+    for (int k = 0; k < N; ++k) e += -0.5 * s[k] * v[k] - p.h64[k] * s[k];
+    if constexpr (N == 3) {
+      if (g.has_cubic) {
+        const double k1 = (double)p.k1[site];
+        const double xy = s[0] * s[1], xz = s[0] * s[2], yz = s[1] * s[2], xyz = s[0] * s[1] * s[2];
+        e += k1 * (xy * xy + xz * xz + yz * yz) + p.k2 * xyz * xyz;
+      }
+    }
+    acc[0] += e;
+#pragma unroll
+    for (int a = 0; a < SCK_MAX_BASIS; ++a)
+      if (a == alpha) {
+#pragma unroll
+        for (int k = 0; k < N; ++k) acc[1 + a * N + k] += s[k];
+      }
+  }
+  __shared__ double red[NV][8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    double x = acc[i];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xFFFFFFFFu, x, off);
+    if (lane == 0) red[i][warp] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    double x = 0.0;
+    for (int wi = 0; wi < (int)(blockDim.x >> 5); ++wi) x += red[threadIdx.x][wi];
+    p.partial[((size_t)rep * p.blocks_per_rep + blockIdx.x) * OBS_VALUES + threadIdx.x] = x;
+  }
+}
+
+// Sum the partials of every replica in block order; E[r] and M[r][alpha][k] (B x b x n).
+__global__ void observables_finish(const double* __restrict__ partial, int B, int blocks_per_rep, int b, int n,
+                                   double* __restrict__ E, double* __restrict__ M) {
+  const int rep = blockIdx.x * blockDim.y + threadIdx.y;
+  const int v = threadIdx.x;
+  if (rep >= B || v >= 1 + b * n) return;
+  double x = 0.0;
+  for (int i = 0; i < blocks_per_rep; ++i) x += partial[((size_t)rep * blocks_per_rep + i) * OBS_VALUES + v];
+  if (v == 0) {
+    if (E != nullptr) E[rep] = x;
+  } else if (M != nullptr) {
+    M[(size_t)rep * b * n + (v - 1)] = x;
+  }
+}
+
+// Enough blocks in flight to cover the GPU, never more than the sites of one replica need.
+int obs_blocks_per_rep(const sck_plan* plan, int batch) {
+  const int per_rep = (plan->geom.nsite + 255) / 256;
+  const int want = (148 * 8 + batch - 1) / batch;
+  return want < per_rep ? (want < 1 ? 1 : want) : per_rep;
+}
+
+int launch_observables(const sck_plan* plan, const void* spins, int storage, int batch, const int8_t* mask,
+                       const float* k1, double* E, double* M, void* workspace, cudaStream_t s) {
+  ObsParams p;
+  p.g = plan->geom;
+  p.B = batch;
+  p.storage = storage == SCK_MODE_INT8 ? 0 : (storage == SCK_MODE_F32 ? 1 : 2);
+  for (int a = 0; a < SCK_MAX_BASIS; ++a) {
+    p.sub[a] = plan->sub[a];
+    p.obs[a] = plan->obs[a];
+  }
+  for (int k = 0; k < 3; ++k) p.h64[k] = plan->desc.h64[k];
+  p.k2 = plan->desc.k2_64;
+  p.blocks_per_rep = obs_blocks_per_rep(plan, batch);
+  p.spins = spins;
+  p.mask = plan->geom.has_mask ? mask : nullptr;
+  p.k1 = k1;
+  p.partial = (double*)workspace;
+  dim3 grid(p.blocks_per_rep, p.B);
+  const int n = plan->geom.n;
+  if (p.storage == 2) observables_kernel<1, 2><<<grid, 256, 0, s>>>(p);
+  else if (p.storage == 0) observables_kernel<1, 0><<<grid, 256, 0, s>>>(p);
+  else if (n == 1) observables_kernel<1, 1><<<grid, 256, 0, s>>>(p);
+  else if (n == 2) observables_kernel<2, 1><<<grid, 256, 0, s>>>(p);
+  else observables_kernel<3, 1><<<grid, 256, 0, s>>>(p);
+  int rc = cuda_status(cudaGetLastError(), "observables");
+  if (rc != SCK_OK) return rc;
+  dim3 fb(OBS_VALUES, 8);
+  observables_finish<<<(p.B + 7) / 8, fb, 0, s>>>(p.partial, p.B, p.blocks_per_rep, plan->geom.b, n, E, M);
+  return cuda_status(cudaGetLastError(), "observables finish");
+}
+
+}  // namespace sck

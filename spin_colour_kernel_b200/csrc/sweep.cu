@@ -1,0 +1,442 @@
+// Class-update kernels of the plain chains (int8 / float32 spins, packed words) and the sequential reference.
+//
+// One class launch updates every site of one (colour, sublattice) class of every replica
+// (Spin_Colour_Kernel/generator.py:150-319). A thread owns one (replica, class site); class sites of a row are
+// x0 + P j with P the x-period of the colouring, so no thread is spent on sites of other colours. Float32
+// arithmetic uses explicit round-to-nearest intrinsics in the reference's operation order (no FMA
+// contraction), so only the transcendental functions (cos, sin, exp) differ from the reference's CPU path.
+//
+// Ising never evaluates exp on the device: the energy change of an Ising flip is one of finitely many values,
+// fixed by the integer group sums G_g, the extra-bond neighbours and the own spin. The host builds, for every
+// replica, a float32 table of exp(-beta dE) (Metropolis) or exp(beta dE) (Barker) over that key space with the
+// same float32 arithmetic and exp as the reference's CPU path, so Ising decisions are bit-exact.
+#include <stdio.h>
+
+#include "internal.h"
+
+namespace sck {
+
+// ---------------------------------------------------------------------------------------------- enumeration
+// (row, j) -> site (x, y, z) of class `colour` on sublattice `alpha`; false when the row has no such site.
+__device__ __forceinline__ bool class_site(const Common& c, int colour, int alpha, long long t, int& x, int& y,
+                                           int& z) {
+  int row = (int)(t / c.bx);
+  int j = (int)(t - (long long)row * c.bx);
+  z = row / c.g.L2;
+  y = row - z * c.g.L2;
+  int x0 = 0;
+  if (colour >= 0) {
+    x0 = c.g.L1;
+    for (int q = 0; q < c.P; ++q)
+      if (colour_of(c.col, alpha, q, y, z) == colour) x0 = q;
+  }
+  x = x0 + c.P * j;
+  return x < c.g.L1;
+}
+
+__device__ __forceinline__ uint32_t counter32(long long rep, int nsite, int own) {
+  return (uint32_t)((unsigned long long)rep * (unsigned long long)nsite + (unsigned long long)own);
+}
+
+// ---------------------------------------------------------------------------------------------- Ising (LUT)
+// Spin values enter the key through their sign, so a malformed value can never index outside the table.
+template <typename T>
+__device__ __forceinline__ int spin_sign(T v) { return (v > T(0)) - (v < T(0)); }
+
+template <typename ST>
+__device__ __forceinline__ void ising_site(const Common& c, const SubDev& sub, int alpha, int rep, int x, int y,
+                                           int z, int32_t key, const ST* src, ST* dst) {
+  const Geometry& g = c.g;
+  const int own = alpha * g.plane + (z * g.L2 + y) * g.L1 + x;
+  if (g.has_mask && c.mask[own] == 0) return;
+  const size_t base = (size_t)rep * g.nsite;
+  const int s = spin_sign(src[base + own]);
+  int k = s > 0 ? 1 : 0;
+  int bi = 0;
+#pragma unroll
+  for (int gi = 0; gi < SCK_MAX_GROUPS; ++gi) {
+    if (gi < sub.n_groups) {
+      int G = 0;
+      for (; bi < sub.group_end[gi]; ++bi) {
+        const BondDev bd = sub.bonds[bi];
+        const int q = neighbour_index(g, bd, x, y, z);
+        const int t = q >= 0 ? spin_sign(src[base + q]) : 0;
+        G += t;
+        if (bd.extra >= 0) k += (t + 1) * sub.extra_stride[bd.extra];
+      }
+      k += (G + sub.group_z[gi]) * sub.key_stride[gi];
+    }
+  }
+  const float e = ((const float*)c.table)[(size_t)rep * c.lut_rep_stride + alpha * c.keys + k];
+  const Philox4 r = philox4x32_10(counter32(rep, g.nsite, own), 0u, key_lo(key), key_hi(key));
+  const float u0 = to_uniform(r.x0);
+  const bool acc = g.acceptance == SCK_BARKER ? __fmul_rn(u0, __fadd_rn(1.0f, e)) < 1.0f : u0 < e;
+  if (acc)
+    dst[base + own] = (ST)(-s);
+  else if ((const void*)src != (const void*)dst)
+    dst[base + own] = (ST)s;
+}
+
+// ------------------------------------------------------------------------------------------- vector models
+template <int N>
+__device__ __forceinline__ void vec_site(const Common& c, const SubDev& sub, int alpha, int rep, int x, int y,
+                                         int z, int32_t key, const float* src, float* dst) {
+  const Geometry& g = c.g;
+  const int own = alpha * g.plane + (z * g.L2 + y) * g.L1 + x;
+  if (g.has_mask && c.mask[own] == 0) return;
+  const size_t base = (size_t)rep * N * g.nsite;
+  float s[N], v[N];
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    s[k] = src[base + (size_t)k * g.nsite + own];
+    v[k] = 0.0f;
+  }
+  float ex[SCK_MAX_EXTRA][N];
+  int bi = 0;
+#pragma unroll
+  for (int gi = 0; gi < SCK_MAX_GROUPS; ++gi) {
+    if (gi < sub.n_groups) {
+      float gs[N];
+#pragma unroll
+      for (int k = 0; k < N; ++k) gs[k] = 0.0f;
+      for (; bi < sub.group_end[gi]; ++bi) {
+        const BondDev bd = sub.bonds[bi];
+        const int q = neighbour_index(g, bd, x, y, z);
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+          const float t = q >= 0 ? src[base + (size_t)k * g.nsite + q] : 0.0f;
+          gs[k] = __fadd_rn(gs[k], t);
+          if (bd.extra >= 0) ex[bd.extra][k] = t;
+        }
+      }
+      if (sub.apply[gi]) {
+#pragma unroll
+        for (int k = 0; k < N; ++k) v[k] = __fadd_rn(v[k], __fmul_rn(sub.J[gi], gs[k]));
+      }
+    }
+  }
+  for (int e = 0; e < sub.n_extra; ++e) {
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      float tot = 0.0f;
+      bool any = false;
+#pragma unroll
+      for (int l = 0; l < N; ++l) {
+        if ((sub.Enz[e] >> (3 * k + l)) & 1) {
+          const float term = __fmul_rn(sub.E[e][3 * k + l], ex[e][l]);
+          tot = any ? __fadd_rn(tot, term) : term;
+          any = true;
+        }
+      }
+      if (any) v[k] = __fadd_rn(v[k], tot);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < N; ++k)
+    if (c.hnz[k]) v[k] = __fadd_rn(v[k], c.h[k]);
+
+  const Philox4 r = philox4x32_10(counter32(rep, g.nsite, own), 0u, key_lo(key), key_hi(key));
+  const float u0 = to_uniform(r.x0);
+  const float TWO_PI = 6.2831855f;
+  float t[N];
+  if (N == 2) {
+    float sn, cs;
+    sincosf(__fmul_rn(TWO_PI, to_uniform(r.x1)), &sn, &cs);
+    t[0] = cs;
+    t[1 % N] = sn;
+  } else if (N == 3) {
+    const float cz = __fsub_rn(__fmul_rn(2.0f, to_uniform(r.x1)), 1.0f);
+    float sn, cs;
+    sincosf(__fmul_rn(TWO_PI, to_uniform(r.x2)), &sn, &cs);
+    const float rr = sqrtf(fmaxf(__fsub_rn(1.0f, __fmul_rn(cz, cz)), 0.0f));
+    t[0] = __fmul_rn(rr, cs);
+    t[1 % N] = __fmul_rn(rr, sn);
+    t[2 % N] = cz;
+  } else {
+    t[0] = -s[0];
+  }
+  float d = __fmul_rn(__fsub_rn(t[0], s[0]), v[0]);
+#pragma unroll
+  for (int k = 1; k < N; ++k) d = __fadd_rn(d, __fmul_rn(__fsub_rn(t[k], s[k]), v[k]));
+  float dE = -d;
+  if (N == 3 && g.has_cubic) {
+    const float k1 = c.k1[own];
+    auto aniso = [&](const float* p) {
+      const float q01 = __fmul_rn(p[0], p[1 % N]), q02 = __fmul_rn(p[0], p[2 % N]);
+      const float q12 = __fmul_rn(p[1 % N], p[2 % N]);
+      const float tri = __fmul_rn(q01, p[2 % N]);
+      const float quad = __fadd_rn(__fadd_rn(__fmul_rn(q01, q01), __fmul_rn(q02, q02)), __fmul_rn(q12, q12));
+      return __fadd_rn(__fmul_rn(k1, quad), __fmul_rn(__fmul_rn(c.k2, tri), tri));
+    };
+    dE = __fadd_rn(dE, __fsub_rn(aniso(t), aniso(s)));
+  }
+  const float beta = c.beta[rep];
+  bool acc;
+  if (g.acceptance == SCK_BARKER)
+    acc = __fmul_rn(u0, __fadd_rn(1.0f, expf(__fmul_rn(beta, dE)))) < 1.0f;
+  else
+    acc = u0 < expf(__fmul_rn(-beta, dE));
+  if (acc || (const void*)src != (const void*)dst) {
+#pragma unroll
+    for (int k = 0; k < N; ++k) dst[base + (size_t)k * g.nsite + own] = acc ? t[k] : s[k];
+  }
+}
+
+// --------------------------------------------------------------------------------------------- dispatchers
+template <int N, typename ST>
+__device__ __forceinline__ void plain_site(const Common& c, const SubDev& sub, int alpha, int rep, int x, int y,
+                                           int z, int32_t key) {
+  if constexpr (N == 1) {
+    ising_site<ST>(c, sub, alpha, rep, x, y, z, key, (const ST*)c.src, (ST*)c.dst);
+  } else {
+    vec_site<N>(c, sub, alpha, rep, x, y, z, key, (const float*)c.src, (float*)c.dst);
+  }
+}
+
+template <int N, typename ST>
+__global__ void __launch_bounds__(256) plain_class_kernel(const __grid_constant__ ClassParams p) {
+  const long long per_rep = (long long)p.c.rows * p.c.bx;
+  const long long total = per_rep * p.c.B;
+  const int32_t key = sweep_key(p.c.state);
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int rep = (int)(t / per_rep);
+    int x, y, z;
+    if (!class_site(p.c, p.colour, p.alpha, t - (long long)rep * per_rep, x, y, z)) continue;
+    plain_site<N, ST>(p.c, p.sub, p.alpha, rep, x, y, z, key);
+  }
+}
+
+// Packed storage: a warp owns one (word, class site); lane j is replica 32 w + j. Each lane runs the int8 update
+// of its replica (same Philox counter), and the new word is assembled with a ballot.
+__global__ void __launch_bounds__(256) packed_class_kernel(const __grid_constant__ ClassParams p) {
+  const Common& c = p.c;
+  const Geometry& g = c.g;
+  const int lane = threadIdx.x & 31;
+  const long long per_word = (long long)c.rows * c.bx;
+  const long long total = per_word * c.W;
+  const int32_t key = sweep_key(c.state);
+  const uint32_t* src = (const uint32_t*)c.src;
+  uint32_t* dst = (uint32_t*)c.dst;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long wi = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; wi < total; wi += nwarps) {
+    const int w = (int)(wi / per_word);
+    int x, y, z;
+    if (!class_site(c, p.colour, p.alpha, wi - (long long)w * per_word, x, y, z)) continue;
+    const int own = p.alpha * g.plane + (z * g.L2 + y) * g.L1 + x;
+    if (g.has_mask && c.mask[own] == 0) continue;
+    const size_t wb = (size_t)w * g.nsite;
+    const int s = (src[wb + own] >> lane) & 1u ? 1 : -1;
+    int k = s > 0 ? 1 : 0;
+    int bi = 0;
+#pragma unroll
+    for (int gi = 0; gi < SCK_MAX_GROUPS; ++gi) {
+      if (gi < p.sub.n_groups) {
+        int G = 0;
+        for (; bi < p.sub.group_end[gi]; ++bi) {
+          const BondDev bd = p.sub.bonds[bi];
+          const int q = neighbour_index(g, bd, x, y, z);
+          int t = 0;
+          if (q >= 0 && (!g.has_mask || c.mask[q] != 0)) t = (src[wb + q] >> lane) & 1u ? 1 : -1;
+          G += t;
+          if (bd.extra >= 0) k += (t + 1) * p.sub.extra_stride[bd.extra];
+        }
+        k += (G + p.sub.group_z[gi]) * p.sub.key_stride[gi];
+      }
+    }
+    const int rep = w * 32 + lane;
+    const float e = ((const float*)c.table)[(size_t)rep * c.lut_rep_stride + p.alpha * c.keys + k];
+    const Philox4 r = philox4x32_10(counter32(rep, g.nsite, own), 0u, key_lo(key), key_hi(key));
+    const float u0 = to_uniform(r.x0);
+    const bool acc = g.acceptance == SCK_BARKER ? __fmul_rn(u0, __fadd_rn(1.0f, e)) < 1.0f : u0 < e;
+    const bool bit = acc ? (s < 0) : (s > 0);
+    const uint32_t word = __ballot_sync(0xFFFFFFFFu, bit);
+    if (lane == 0) dst[wb + own] = word;
+  }
+}
+
+// ---------------------------------------------------------------------------------------- sequential chain
+// One thread per replica walks the classes in sweep order and, inside a class, the sites in raster order
+// (z, y, x): the definition of the chain that the parallel class launches must reproduce (sampler.py:281-293).
+template <int N, typename ST>
+__global__ void plain_sequential_kernel(const __grid_constant__ SeqParams p) {
+  const int rep = blockIdx.x * blockDim.x + threadIdx.x;
+  if (rep >= p.c.B) return;
+  const int32_t key = sweep_key(p.c.state);
+  const Geometry& g = p.c.g;
+  for (int ci = 0; ci < p.n_classes; ++ci) {
+    const int colour = p.classes[ci][0], alpha = p.classes[ci][1];
+    for (int z = 0; z < g.L3; ++z)
+      for (int y = 0; y < g.L2; ++y)
+        for (int x = 0; x < g.L1; ++x)
+          if (colour_of(p.c.col, alpha, x, y, z) == colour) plain_site<N, ST>(p.c, p.sub[alpha], alpha, rep, x, y, z, key);
+  }
+}
+
+// Packed sequential chain: one warp per word, same site order.
+__global__ void packed_sequential_kernel(const __grid_constant__ SeqParams p) {
+  const Common& c = p.c;
+  const Geometry& g = c.g;
+  const int w = blockIdx.x;
+  const int lane = threadIdx.x;
+  if (w >= c.W) return;
+  const int32_t key = sweep_key(c.state);
+  uint32_t* sp = (uint32_t*)c.dst;
+  const size_t wb = (size_t)w * g.nsite;
+  for (int ci = 0; ci < p.n_classes; ++ci) {
+    const int colour = p.classes[ci][0], alpha = p.classes[ci][1];
+    const SubDev& sub = p.sub[alpha];
+    for (int z = 0; z < g.L3; ++z)
+      for (int y = 0; y < g.L2; ++y)
+        for (int x = 0; x < g.L1; ++x) {
+          if (colour_of(c.col, alpha, x, y, z) != colour) continue;
+          const int own = alpha * g.plane + (z * g.L2 + y) * g.L1 + x;
+          if (g.has_mask && c.mask[own] == 0) continue;
+          const int s = (sp[wb + own] >> lane) & 1u ? 1 : -1;
+          int k = s > 0 ? 1 : 0;
+          int bi = 0;
+          for (int gi = 0; gi < sub.n_groups; ++gi) {
+            int G = 0;
+            for (; bi < sub.group_end[gi]; ++bi) {
+              const BondDev bd = sub.bonds[bi];
+              const int q = neighbour_index(g, bd, x, y, z);
+              int t = 0;
+              if (q >= 0 && (!g.has_mask || c.mask[q] != 0)) t = (sp[wb + q] >> lane) & 1u ? 1 : -1;
+              G += t;
+              if (bd.extra >= 0) k += (t + 1) * sub.extra_stride[bd.extra];
+            }
+            k += (G + sub.group_z[gi]) * sub.key_stride[gi];
+          }
+          const int rep = w * 32 + lane;
+          const float e = ((const float*)c.table)[(size_t)rep * c.lut_rep_stride + alpha * c.keys + k];
+          const Philox4 r = philox4x32_10(counter32(rep, g.nsite, own), 0u, key_lo(key), key_hi(key));
+          const float u0 = to_uniform(r.x0);
+          const bool acc = g.acceptance == SCK_BARKER ? __fmul_rn(u0, __fadd_rn(1.0f, e)) < 1.0f : u0 < e;
+          const uint32_t word = __ballot_sync(0xFFFFFFFFu, acc ? (s < 0) : (s > 0));
+          if (lane == 0) sp[wb + own] = word;
+          __syncwarp();
+        }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------- conversions
+__global__ void pack_kernel(const int8_t* __restrict__ spins, int32_t* __restrict__ words, int B, int W, int nsite) {
+  const long long total = (long long)W * nsite;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int w = (int)(t / nsite);
+    const int site = (int)(t - (long long)w * nsite);
+    uint32_t word = 0;
+    for (int j = 0; j < 32; ++j) {
+      const int rep = w * 32 + j;
+      if (rep < B && spins[(size_t)rep * nsite + site] > 0) word |= 1u << j;
+    }
+    words[t] = (int32_t)word;
+  }
+}
+
+__global__ void unpack_kernel(const int32_t* __restrict__ words, const int8_t* __restrict__ mask,
+                              int8_t* __restrict__ spins, int B, int nsite) {
+  const long long total = (long long)B * nsite;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int rep = (int)(t / nsite);
+    const int site = (int)(t - (long long)rep * nsite);
+    const uint32_t word = (uint32_t)words[(size_t)(rep >> 5) * nsite + site];
+    const int8_t v = (word >> (rep & 31)) & 1u ? 1 : -1;
+    spins[t] = (mask != nullptr && mask[site] == 0) ? 0 : v;
+  }
+}
+
+__global__ void advance_kernel(int64_t* state, int n) { state[1] += n; }
+
+// -------------------------------------------------------------------------------------------------- launch
+static int grid_for(long long total, int block) {
+  long long g = (total + block - 1) / block;
+  if (g > 148LL * 64) g = 148LL * 64;
+  return (int)(g < 1 ? 1 : g);
+}
+
+int launch_class(const sck_plan* plan, const Common& c, int colour, int alpha, cudaStream_t s) {
+  ClassParams p;
+  p.c = c;
+  p.sub = plan->sub[alpha];
+  p.colour = colour;
+  p.alpha = alpha;
+  if (colour < 0) {
+    p.c.P = 1;
+    p.c.bx = c.g.L1;
+  }
+  const int block = 256;
+  const long long per = (long long)p.c.rows * p.c.bx;
+  if (plan->mode == SCK_MODE_PACKED) {
+    packed_class_kernel<<<grid_for(per * c.W * 32, block), block, 0, s>>>(p);
+  } else {
+    const int grid = grid_for(per * c.B, block);
+    switch (c.g.n) {
+      case 1:
+        if (plan->mode == SCK_MODE_INT8)
+          plain_class_kernel<1, int8_t><<<grid, block, 0, s>>>(p);
+        else
+          plain_class_kernel<1, float><<<grid, block, 0, s>>>(p);
+        break;
+      case 2:
+        plain_class_kernel<2, float><<<grid, block, 0, s>>>(p);
+        break;
+      default:
+        plain_class_kernel<3, float><<<grid, block, 0, s>>>(p);
+        break;
+    }
+  }
+  return cuda_status(cudaGetLastError(), "class launch");
+}
+
+int launch_sequential(const sck_plan* plan, const Common& c, cudaStream_t s) {
+  SeqParams p;
+  p.c = c;
+  for (int a = 0; a < SCK_MAX_BASIS; ++a) p.sub[a] = plan->sub[a];
+  p.n_classes = plan->desc.n_classes;
+  for (int i = 0; i < p.n_classes; ++i) {
+    p.classes[i][0] = plan->desc.classes[i][0];
+    p.classes[i][1] = plan->desc.classes[i][1];
+  }
+  if (plan->mode == SCK_MODE_PACKED) {
+    packed_sequential_kernel<<<c.W, 32, 0, s>>>(p);
+  } else {
+    const int grid = (c.B + 63) / 64;
+    switch (c.g.n) {
+      case 1:
+        if (plan->mode == SCK_MODE_INT8)
+          plain_sequential_kernel<1, int8_t><<<grid, 64, 0, s>>>(p);
+        else
+          plain_sequential_kernel<1, float><<<grid, 64, 0, s>>>(p);
+        break;
+      case 2:
+        plain_sequential_kernel<2, float><<<grid, 64, 0, s>>>(p);
+        break;
+      default:
+        plain_sequential_kernel<3, float><<<grid, 64, 0, s>>>(p);
+        break;
+    }
+  }
+  return cuda_status(cudaGetLastError(), "sequential launch");
+}
+
+int launch_pack(const sck_plan* plan, const int8_t* spins, int32_t* words, cudaStream_t s) {
+  const long long total = (long long)plan->W * plan->geom.nsite;
+  pack_kernel<<<grid_for(total, 256), 256, 0, s>>>(spins, words, plan->batch, plan->W, plan->geom.nsite);
+  return cuda_status(cudaGetLastError(), "pack");
+}
+
+int launch_unpack(const sck_plan* plan, const int32_t* words, const int8_t* mask, int8_t* spins, cudaStream_t s) {
+  const long long total = (long long)plan->batch * plan->geom.nsite;
+  unpack_kernel<<<grid_for(total, 256), 256, 0, s>>>(words, mask, spins, plan->batch, plan->geom.nsite);
+  return cuda_status(cudaGetLastError(), "unpack");
+}
+
+int launch_advance(int64_t* state, int n, cudaStream_t s) {
+  advance_kernel<<<1, 1, 0, s>>>(state, n);
+  return cuda_status(cudaGetLastError(), "advance");
+}
+
+}  // namespace sck

@@ -1,0 +1,385 @@
+"""Sampler: the reference's sampler interface over the B200 kernels of libsckb200.so.
+
+Same constructor arguments, attributes, methods, device buffers and errors as
+Spin_Colour_Kernel/sampler.py:39-345, so code written against the reference runs unchanged:
+  Sampler(system, batch, device, seed, compact, spin_dtype, packed, bitwise, words_per_program, independent,
+          bitwise_tile, bitwise_warps, max_block)
+  .set_temperature(T)  .set_seed(seed, sweep)  .init_spins(kind, seed)  .pack(x)  .unpack(S)
+  .sweep(S, n)  .graph(S, k)  .sync_sweep(S, n)  .reference_sweep(S, n)
+  .local_field(S)  .energy(S)  .magnetization(S)
+`state` (int64 {seed, sweep}), `beta` and the acceptance tables are device tensors updated in place, so a
+captured CUDA graph keeps reading them by address. Every update runs in the CUDA kernels behind the C ABI of
+include/sck.h; there is no CPU path, and a CPU device is refused.
+
+The launch-geometry attributes of the reference (stride, bx, rows_per, block, chunks, cblock, cchunks, pblock,
+pchunks, G, ngroups, ...) are computed with the reference's rules and kept for API compatibility; the CUDA
+kernels choose their own tiling, and the chain does not depend on it.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from . import plan as P
+from .system import System
+
+COMPACT_MIN = 4
+TILE = 128
+MAX_BLOCK = 1024
+PTILE = 64
+WORD = 32
+BWG = 4
+
+
+def _num_warps(block: int) -> int:
+    return 4 if block >= 256 else (2 if block >= 128 else 1)
+
+
+def x_period(col) -> int:
+    """Period along x of a linear colouring: lcm over its factors of m_r / gcd(K_r1, m_r)."""
+    import math
+    Pd = 1
+    for r, mr in enumerate(col.m):
+        Pd = math.lcm(Pd, mr // math.gcd(int(col.K[r][0]) % mr or mr, mr))
+    return Pd
+
+
+def _ptr(t) -> int:
+    return 0 if t is None else int(t.data_ptr())
+
+
+class Sampler:
+    def __init__(self, system: System, batch: int, device="cuda", seed: int = 0, compact: bool = True,
+                 spin_dtype: torch.dtype | None = None, packed: bool | None = None, bitwise: bool = False,
+                 words_per_program: int | None = None, independent: bool = False, bitwise_tile: int | None = None,
+                 bitwise_warps: int | None = None, max_block: int = MAX_BLOCK):
+        self.sys = system
+        self.bitwise = bool(bitwise)
+        self.independent = bool(independent)
+        if self.independent and not self.bitwise:
+            raise ValueError("independent per-replica draws need bitwise=True")
+        if self.bitwise:
+            _, _, self.zmax = P.bitwise_check(system)
+            if packed is False:
+                raise ValueError("bitwise multi-spin coding uses the packed storage")
+            packed = True
+        self.packed = (system.n == 1 and int(batch) >= WORD) if packed is None else bool(packed)
+        if self.packed and system.n != 1:
+            raise ValueError("bit packing is for Ising (n = 1) only")
+        self.spin_dtype = spin_dtype or (torch.int8 if system.n == 1 else torch.float32)
+        if not self.packed and self.spin_dtype not in (torch.int8, torch.float32):
+            raise ValueError("spin_dtype must be torch.int8 (Ising) or torch.float32")
+        if self.spin_dtype == torch.int8 and system.n != 1:
+            raise ValueError("int8 storage holds Ising spins only")
+        self.B = int(batch)
+        n, b, L3, L2, L1 = system.n, system.b, system.L3, system.L2, system.L1
+        self.W = -(-self.B // WORD) if self.packed else self.B
+        self.Bp = self.W * WORD if self.packed else self.B
+        if self.Bp * b * L3 * L2 * L1 >= 2 ** 31 - 1:
+            raise ValueError("replica batch too large for the int32 Philox counter")
+        gmax = words_per_program or BWG
+        if gmax & (gmax - 1):
+            raise ValueError("words_per_program must be a power of two")
+        self.G = min(gmax, 1 << (self.W - 1).bit_length()) if self.bitwise else 1
+        self.ngroups = -(-self.W // self.G)
+        self.nrows = L3 * L2
+        if max_block < 16 or max_block & (max_block - 1):
+            raise ValueError("max_block must be a power of two >= 16")
+        self._geometry(system, compact, bitwise_tile, bitwise_warps, max_block)
+        if self.bitwise:
+            self.mode = L.MODE_BITWISE_INDEP if self.independent else L.MODE_BITWISE
+        elif self.packed:
+            self.mode = L.MODE_PACKED
+        elif self.spin_dtype == torch.int8:
+            self.mode = L.MODE_INT8
+        else:
+            self.mode = L.MODE_F32
+        self.desc = P.describe(system)
+        lib = L.lib()
+        handle = ctypes.c_void_p()
+        L.check(lib.sck_plan_create(ctypes.byref(self.desc), self.B, self.mode, ctypes.byref(handle)))
+        self._plan = handle
+        nel, eb, keys = ctypes.c_int64(), ctypes.c_int32(), ctypes.c_int32()
+        L.check(lib.sck_plan_table_size(self._plan, ctypes.byref(nel), ctypes.byref(eb), ctypes.byref(keys)))
+        self.keys = keys.value
+        self.device = torch.device(device)
+        if self.device.type != "cuda":
+            raise RuntimeError("spin_colour_kernel_b200 runs on CUDA devices (B200) only; there is no CPU path")
+        dev = self.device
+        m = system.site_mask()
+        self.mask_np = m
+        self.mask = torch.as_tensor(m.astype(np.int8), device=dev)
+        k1 = system.cubic_k1 if system.cubic_k1 is not None else np.zeros(m.shape, np.float32)
+        self.k1 = torch.as_tensor(np.asarray(k1, np.float32), device=dev)
+        self.state = torch.tensor([int(seed), 0], dtype=torch.int64, device=dev)
+        self.beta = torch.ones(self.Bp, dtype=torch.float32, device=dev)
+        self.ptab = None
+        self.lut = None
+        if self.bitwise:
+            self._table = P.p_fixed if self.independent else P.p_table
+            self.ptab = torch.as_tensor(self._table(system, np.ones(self.W)), device=dev)
+        elif system.n == 1:
+            self.lut = torch.as_tensor(P.ising_table(system, np.ones(self.Bp, np.float32), self.keys), device=dev)
+            assert self.lut.numel() == nel.value
+        self.colours = system.colour_map()
+        self.classes = P.sweep_classes(system)
+        self._mask_f = torch.as_tensor(m, device=dev).to(torch.float32)
+        self._obs_ws = {}
+        self._workspace(self.B)
+
+    def __del__(self):
+        h = getattr(self, "_plan", None)
+        if h is not None and h.value:
+            try:
+                L.lib().sck_plan_destroy(h)
+            except Exception:
+                pass
+            self._plan = None
+
+    # ------------------------------------------------------------ reference launch geometry
+    def _geometry(self, system, compact, bitwise_tile, bitwise_warps, max_block):
+        L1 = system.L1
+        self.block = min(max(16, 1 << (L1 - 1).bit_length()), max_block)
+        self.chunks = -(-L1 // self.block)
+        self.nw = _num_warps(self.block)
+        Pd = x_period(system.colouring) if compact else 1
+        Pd = Pd if Pd >= COMPACT_MIN else 1
+        self.stride = Pd
+        self.bx = -(-L1 // Pd)
+        tile_c = bitwise_tile if (self.bitwise and bitwise_tile) else TILE
+        self.rows_per = max(1, min(self.nrows, tile_c // self.bx)) if Pd > 1 else 1
+        if self.packed and not self.bitwise:
+            self.rows_per = max(1, min(self.nrows, PTILE // self.bx)) if Pd > 1 else 1
+        self.cblock = max(16, 1 << (self.rows_per * self.bx - 1).bit_length())
+        self.cchunks = 1
+        if not self.packed and self.rows_per == 1 and self.cblock > max_block:
+            self.cblock = max_block
+            self.cchunks = -(-self.bx // max_block)
+        self.cnw = _num_warps(self.cblock)
+        if self.packed:
+            nx = self.bx if Pd > 1 else L1
+            tile = TILE if self.bitwise else PTILE
+            self.pblock = min(tile, max(16, 1 << (nx - 1).bit_length()))
+            self.pchunks = -(-nx // self.pblock)
+            self.pblock_ref = min(tile, self.block)
+            self.pchunks_ref = -(-L1 // self.pblock_ref)
+            if not self.bitwise:
+                self.cnw = 4 if self.cblock * WORD >= 2048 else 2
+            elif bitwise_tile:
+                self.pblock = min(bitwise_tile, max(16, 1 << (nx - 1).bit_length()))
+                self.pchunks = -(-nx // self.pblock)
+            if self.bitwise and bitwise_warps:
+                self.cnw = self.nw = int(bitwise_warps)
+
+    # ------------------------------------------------------------ state
+    def set_temperature(self, T):
+        T = torch.as_tensor(T, dtype=torch.float32).reshape(-1).cpu()
+        beta = (1.0 / T).expand(self.B).contiguous() if T.numel() == 1 else (1.0 / T).contiguous()
+        if beta.numel() != self.B:
+            raise ValueError(f"need 1 or {self.B} temperatures, got {beta.numel()}")
+        if self.Bp > self.B:     # padding replicas of the last word: computed, never observed
+            beta = torch.cat([beta, beta[-1:].expand(self.Bp - self.B)])
+        if self.bitwise:
+            bwd = beta.reshape(self.W, WORD)
+            if not torch.all(bwd == bwd[:, :1]):
+                raise ValueError("bitwise multi-spin coding needs one temperature per word of 32 replicas")
+            self.ptab.copy_(torch.as_tensor(self._table(self.sys, bwd[:, 0].double().numpy()), device=self.device))
+        elif self.lut is not None:
+            self.lut.copy_(torch.as_tensor(P.ising_table(self.sys, beta.numpy(), self.keys), device=self.device))
+        self.beta.copy_(beta.to(self.device))
+
+    def set_seed(self, seed: int, sweep: int = 0):
+        self.state[0] = int(seed)
+        self.state[1] = int(sweep)
+
+    def init_spins(self, kind="random", seed: int = 0) -> torch.Tensor:
+        s = self.sys
+        g = torch.Generator(device="cpu").manual_seed(int(seed))
+        shape = (self.B, s.n) + s.shape
+        if kind == "ordered":
+            x = torch.zeros(shape)
+            x[:, 0] = 1.0
+        elif s.n == 1:
+            x = torch.randint(0, 2, shape, generator=g).float() * 2 - 1
+        else:
+            x = torch.randn(shape, generator=g)
+            x = x / x.norm(dim=1, keepdim=True)
+        x = x.to(self.device) * self._mask_f
+        if self.packed:
+            return self.pack(x)
+        return x.to(self.spin_dtype).contiguous()
+
+    def pack(self, x: torch.Tensor) -> torch.Tensor:
+        """(B, 1, b, L3, L2, L1) spins of +-1 (0 on masked sites) -> (W, 1, b, L3, L2, L1) int32 words."""
+        sgn = (x > 0).to(torch.int8).to(self.device).contiguous()
+        if sgn.shape[0] != self.B:
+            raise ValueError("pack expects one row per replica")
+        out = torch.empty((self.W, 1) + self.sys.shape, dtype=torch.int32, device=self.device)
+        L.check(L.lib().sck_pack(self._plan, _ptr(sgn), _ptr(out), self._stream()))
+        return out
+
+    def unpack(self, S: torch.Tensor) -> torch.Tensor:
+        """Packed words -> (B, 1, b, L3, L2, L1) int8 spins of +-1, 0 on masked sites; identity when unpacked."""
+        if not self.packed or S.dtype != torch.int32:
+            return S
+        self._check(S)
+        out = torch.empty((self.B, 1) + self.sys.shape, dtype=torch.int8, device=self.device)
+        L.check(L.lib().sck_unpack(self._plan, _ptr(S), _ptr(self.mask), _ptr(out), self._stream()))
+        return out
+
+    # ------------------------------------------------------------ launches
+    def _stream(self):
+        return ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def _check(self, S: torch.Tensor):
+        want_dtype = torch.int32 if self.packed else self.spin_dtype
+        want_shape = ((self.W, 1) if self.packed else (self.B, self.sys.n)) + self.sys.shape
+        if S.device != self.device or S.dtype != want_dtype or tuple(S.shape) != want_shape or not S.is_contiguous():
+            raise ValueError(f"spins must be a contiguous {want_dtype} tensor of shape {want_shape} on {self.device}")
+
+    def _buffers(self, S: torch.Tensor) -> L.Buffers:
+        b = L.Buffers()
+        b.spins = _ptr(S)
+        b.mask = _ptr(self.mask) if self.sys.mask is not None else 0
+        b.k1 = _ptr(self.k1) if self.sys.cubic_k1 is not None else 0
+        b.beta = _ptr(self.beta)
+        b.table = _ptr(self.ptab if self.bitwise else self.lut)
+        b.state = _ptr(self.state)
+        return b
+
+    def sweep(self, S: torch.Tensor, n: int = 1) -> torch.Tensor:
+        """n coloured sweeps in place; advances the sweep counter on the device."""
+        self._check(S)
+        buf = self._buffers(S)
+        with torch.cuda.device(self.device):
+            L.check(L.lib().sck_sweep(self._plan, ctypes.byref(buf), int(n), self._stream()))
+        return S
+
+    def class_update(self, S: torch.Tensor, colour: int, alpha: int, src: torch.Tensor | None = None):
+        """One class launch (the reference's kernel[grid](...) for class (colour, alpha))."""
+        self._check(S)
+        buf = self._buffers(S)
+        with torch.cuda.device(self.device):
+            L.check(L.lib().sck_class_update(self._plan, ctypes.byref(buf), _ptr(src) if src is not None else None,
+                                             int(colour), int(alpha), 0, self._stream()))
+        return S
+
+    def graph(self, S: torch.Tensor, k: int):
+        """Capture k sweeps (launches and counter increments) in a CUDA graph; returns its replay."""
+        with torch.cuda.device(self.device):
+            return self._graph(S, k)
+
+    def _graph(self, S: torch.Tensor, k: int):
+        s = torch.cuda.Stream(device=self.device)
+        s.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(s):
+            self.sweep(S, 1)
+        torch.cuda.current_stream(self.device).wait_stream(s)
+        torch.cuda.synchronize(self.device)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.sweep(S, k)
+        dev = self.device
+
+        def replay():
+            with torch.cuda.device(dev):
+                g.replay()
+        replay.keep = (self, S, g)
+        return replay
+
+    def sync_sweep(self, S: torch.Tensor, n: int = 1) -> torch.Tensor:
+        """The negative control: every site updated in the same step from the old state."""
+        self._check(S)
+        scratch = torch.empty_like(S)
+        buf = self._buffers(S)
+        with torch.cuda.device(self.device):
+            L.check(L.lib().sck_sync_sweep(self._plan, ctypes.byref(buf), _ptr(scratch), int(n), self._stream()))
+        return S
+
+    def reference_sweep(self, S: torch.Tensor, n: int = 1) -> torch.Tensor:
+        """Sequential reference chain on the GPU: classes in order, sites one at a time in raster order."""
+        self._check(S)
+        buf = self._buffers(S)
+        with torch.cuda.device(self.device):
+            L.check(L.lib().sck_reference_sweep(self._plan, ctypes.byref(buf), int(n), self._stream()))
+        return S
+
+    # ------------------------------------------------------------ observables
+    def local_field(self, S: torch.Tensor) -> torch.Tensor:
+        """Bond part of the local field for every site (float64, torch rolls), a slow reference helper."""
+        s = self.sys
+        D = s.crystal.D
+        S64 = self.unpack(S).double()
+        v = torch.zeros_like(S64)
+        dims = {0: 5, 1: 4, 2: 3}
+        for i, bd in enumerate(s.crystal.bonds):
+            M = torch.as_tensor(s.bond_matrix(i), dtype=torch.float64, device=S.device)
+            if not M.any():
+                continue
+            src = S64[:, :, bd.alpha2]
+            valid = torch.ones(s.shape[1:], dtype=torch.float64, device=S.device)
+            for k in range(D):
+                d = bd.delta[k]
+                if d == 0:
+                    continue
+                src = torch.roll(src, shifts=-d, dims=dims[k] - 1)
+                if not s.periodic[k]:
+                    Lk = s.box[k]
+                    idx = torch.arange(Lk, device=S.device)
+                    ok = ((idx + d) >= 0) & ((idx + d) < Lk)
+                    shp = [1, 1, 1]
+                    shp[2 - k] = Lk
+                    valid = valid * ok.to(torch.float64).reshape(shp)
+            v[:, :, bd.alpha] += torch.einsum("kl,blzyx->bkzyx", M, src * valid)
+        return v
+
+    def _workspace(self, batch: int) -> torch.Tensor:
+        ws = self._obs_ws.get(batch)
+        if ws is None:
+            nbytes = ctypes.c_int64()
+            L.check(L.lib().sck_observables_workspace_size(self._plan, int(batch), ctypes.byref(nbytes)))
+            ws = torch.empty(max(8, nbytes.value // 8), dtype=torch.float64, device=self.device)
+            self._obs_ws[batch] = ws
+        return ws
+
+    def observables(self, S: torch.Tensor, E: torch.Tensor | None = None, M: torch.Tensor | None = None):
+        """FP64 energy (B,) and per-sublattice magnetization (B, b, n) in one pass of the GPU reduction.
+
+        S is this sampler's storage (packed words, int8 or float32 spins of any number of replicas).
+        Graph-safe for the sampler's own batch: no host work, outputs may be preallocated."""
+        s = self.sys
+        if S.dtype == torch.int32 and self.packed:
+            self._check(S)
+            storage, batch = L.MODE_PACKED, self.B
+        else:
+            if S.dtype == torch.int8 and s.n == 1:
+                storage = L.MODE_INT8
+            else:
+                storage = L.MODE_F32
+                if S.dtype != torch.float32:
+                    S = S.to(torch.float32)
+            S = S.contiguous()
+            batch = int(S.shape[0])
+            if tuple(S.shape[1:]) != (s.n,) + s.shape or S.device != self.device:
+                raise ValueError(f"spins must have shape (batch, {s.n}) + {s.shape} on {self.device}")
+        if E is None:
+            E = torch.empty(batch, dtype=torch.float64, device=self.device)
+        if M is None:
+            M = torch.empty((batch, s.b, s.n), dtype=torch.float64, device=self.device)
+        buf = self._buffers(S)
+        with torch.cuda.device(self.device):
+            L.check(L.lib().sck_observables(self._plan, ctypes.byref(buf), _ptr(S), storage, batch, _ptr(E), _ptr(M),
+                                            _ptr(self._workspace(batch)), self._stream()))
+        return E, M
+
+    def energy(self, S: torch.Tensor) -> torch.Tensor:
+        """Total energy per replica, float64."""
+        return self.observables(S)[0]
+
+    def magnetization(self, S: torch.Tensor) -> torch.Tensor:
+        """Per-sublattice magnetization M_alpha, shape (B, b, n), float64."""
+        return self.observables(S)[1]

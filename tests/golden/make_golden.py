@@ -1,0 +1,159 @@
+"""Generate the golden fixtures by running the reference itself (its CPU path, the Triton interpreter).
+
+Run in the development container, where the reference source is readable:
+
+    TRITON_INTERPRET=1 python tests/golden/make_golden.py [--ref /root/reference/src] [case ...]
+
+Writes one `<case>.npz` per parity case of cases.py (initial spins, spins after recorded sweeps, energies and
+magnetizations per sweep, the temperatures, the acceptance tables of bitwise cases) plus `philox.npz`
+(Triton's own rand4x / randint4x outputs) and `quickstart.json`. Nothing on the GPU side reads the
+reference: the fixtures are the committed record of its outputs.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import time
+from pathlib import Path
+
+os.environ.setdefault("TRITON_INTERPRET", "1")
+HERE = Path(__file__).resolve().parent
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference/src")
+    ap.add_argument("cases", nargs="*")
+    a = ap.parse_args(argv)
+    os.environ.setdefault("SCK_CACHE", str(Path("/tmp") / "sck_golden_cache"))
+    sys.path.insert(0, a.ref)
+    sys.path.insert(0, str(HERE))
+    import numpy as np
+    import torch
+    from Spin_Colour_Kernel import bitwise as bw
+    from Spin_Colour_Kernel import crystals as cr
+    from Spin_Colour_Kernel import system as sy
+    from Spin_Colour_Kernel.sampler import Sampler
+
+    import cases as C
+
+    names = a.cases or list(C.CASES) + ["philox", "quickstart", "tables"]
+    for name in names:
+        t0 = time.time()
+        if name == "philox":
+            _philox(np, torch, bw)
+        elif name == "quickstart":
+            _quickstart(torch, sy, Sampler)
+        elif name == "tables":
+            _tables(np, bw, sy, cr)
+        else:
+            case = C.CASES[name]
+            s = case["build"](sy, cr)
+            kw = C.sampler_kwargs(case)
+            if case.get("ref_packed") is not None:
+                kw["packed"] = case["ref_packed"]
+            B = case["B"]
+            A = Sampler(s, B, device="cpu", seed=case["seed"], **kw)
+            T = C.temperatures(case["T"], B)
+            A.set_temperature(torch.from_numpy(T))
+            S = A.init_spins(seed=case["init"])
+            rec = {"T": T, "S0": A.unpack(S).numpy().copy(), "E": [], "M": [], "ptab": []}
+            if A.packed:
+                rec["W0"] = S.numpy().copy()
+            every = case.get("record_every", 1)
+            keep = set(range(1, case["sweeps"] + 1)) if every else {1, 2, 10, 50, 100, case["sweeps"]}
+            if A.bitwise:
+                rec["ptab"] = A.ptab.numpy().copy()
+            snaps, snap_ids = [], []
+            for k in range(1, case["sweeps"] + 1):
+                A.sweep(S)
+                x = A.unpack(S)
+                rec["E"].append(A.energy(S).numpy().copy())
+                rec["M"].append(A.magnetization(S).numpy().copy())
+                if k in keep:
+                    snaps.append(x.numpy().copy())
+                    snap_ids.append(k)
+            out = dict(T=rec["T"], S0=rec["S0"], E=np.stack(rec["E"]), M=np.stack(rec["M"]),
+                       snaps=np.stack(snaps), snap_ids=np.asarray(snap_ids), n_colours=s.colouring.n_colours,
+                       classes=np.asarray(A.classes, np.int64), stride=A.stride, bx=A.bx, rows_per=A.rows_per)
+            if A.packed:
+                out["W0"] = rec["W0"]
+                out["Wend"] = S.numpy().copy()
+            if A.bitwise:
+                out["ptab"] = rec["ptab"]
+            np.savez_compressed(HERE / f"{name}.npz", **out)
+        print(f"{name}: {time.time() - t0:.1f} s", flush=True)
+
+
+def _philox(np, torch, bw):
+    import triton
+    import triton.language as tl
+
+    @triton.jit
+    def k4(out_ptr, seed, N: tl.constexpr):
+        off = tl.arange(0, N)
+        a, b, c, d = tl.rand4x(seed, off * 7919 + 3)
+        tl.store(out_ptr + off, a)
+        tl.store(out_ptr + N + off, b)
+        tl.store(out_ptr + 2 * N + off, c)
+        tl.store(out_ptr + 3 * N + off, d)
+
+    @triton.jit
+    def ki(out_ptr, seed, N: tl.constexpr):
+        off = tl.arange(0, N)
+        a, b, c, d = tl.randint4x(seed, off * 104729 + 11)
+        tl.store(out_ptr + off, a.to(tl.int32, bitcast=True))
+        tl.store(out_ptr + N + off, b.to(tl.int32, bitcast=True))
+        tl.store(out_ptr + 2 * N + off, c.to(tl.int32, bitcast=True))
+        tl.store(out_ptr + 3 * N + off, d.to(tl.int32, bitcast=True))
+
+    seeds = [0, 1, 12345, 123457, 2147483628, bw.sweep_seed(1234, 0), bw.sweep_seed(1234, 199)]
+    N = 256
+    U, R = [], []
+    for sd in seeds:
+        out = torch.zeros(4 * N)
+        k4[(1,)](out, sd, N=N)
+        U.append(out.numpy().reshape(4, N).copy())
+        outi = torch.zeros(4 * N, dtype=torch.int32)
+        ki[(1,)](outi, sd, N=N)
+        R.append(outi.numpy().view(np.uint32).reshape(4, N).copy())
+    np.savez_compressed(HERE / "philox.npz", seeds=np.asarray(seeds, np.int64), N=N, rand4x=np.stack(U),
+                        randint4x=np.stack(R), offset_mul=7919, offset_add=3, int_mul=104729, int_add=11,
+                        sweep_seeds=np.asarray([[bw.sweep_seed(b, s) for s in range(0, 50)] for b in (0, 1, 1234, 99991)]))
+
+
+def _quickstart(torch, sy, Sampler):
+    """The reference's quick start: 3 systems, 2 replicas, seed 11, T = 1.5, init seed 2, 20 sweeps."""
+    rows = []
+    for s in [sy.ising("square", 8), sy.xy("sc", 4), sy.heisenberg("triangular", 6)]:
+        A = Sampler(s, 2, device="cpu", seed=11)
+        A.set_temperature(1.5)
+        S = A.init_spins(seed=2)
+        A.sweep(S, 20)
+        e = (A.energy(S).double() / s.n_active).tolist()
+        rows.append(dict(name=s.name, colours=s.colouring.n_colours, energy_per_site=e))
+    (HERE / "quickstart.json").write_text(json.dumps(rows, indent=1))
+
+
+def _tables(np, bw, sy, cr):
+    betas = np.array([0.25, 0.5, 1.0 / 2.269, 1.0 / 4.5115, 2.0])
+    out = {}
+    for key, s in {"square": sy.ising("square", 4), "sc": sy.ising("sc", 4), "fcc": sy.ising("fcc", 4),
+                   "triangular": sy.ising("triangular", 6)}.items():
+        for acc in ("metropolis", "barker"):
+            s.acceptance = acc
+            out[f"{key}_{acc}_p"] = bw.p_table(s, betas)
+            out[f"{key}_{acc}_P"] = bw.p_fixed(s, betas)
+    m = sy.System("masked h", 1, cr.make("square"), (8, 8), (True, True), {1: 1.0}, h=(0.3,),
+                  mask=np.random.default_rng(0).random((1, 1, 8, 8)) > 0.25)
+    out["masked_h_metropolis_p"] = bw.p_table(m, betas)
+    out["masked_h_metropolis_P"] = bw.p_fixed(m, betas)
+    out["betas"] = betas
+    np.savez_compressed(HERE / "tables.npz", **out)
+
+
+if __name__ == "__main__":
+    main()

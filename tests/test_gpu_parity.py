@@ -1,0 +1,274 @@
+"""GPU parity: the CUDA kernels against the reference's recorded outputs and the CPU oracle.
+
+Ising (int8, float32, packed, bitwise shared and independent) must be bit-exact. XY and Heisenberg must agree
+within per-spin |delta| <= 1e-5 over the recorded trajectories; their transcendental functions (cos, sin, exp)
+are the device's, not NumPy's, so a decision whose uniform falls within a few ulp of the acceptance
+probability can flip. The tests report the fraction of spins outside the tolerance (such flips) and bound it.
+"""
+
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+import cases as C
+from oracle import bitwise as obw
+from oracle import observables as obs
+from oracle import sweep as osw
+from spin_colour_kernel_b200 import crystals as cr
+from spin_colour_kernel_b200 import system as sy
+
+pytestmark = pytest.mark.gpu
+GOLD = Path(__file__).resolve().parent / "golden"
+VEC_TOL = 1e-5
+
+
+def _have(name):
+    return (GOLD / f"{name}.npz").exists()
+
+
+PLAIN = [k for k in C.CASES if _have(k) and not C.CASES[k].get("bitwise")]
+BITWISE = [k for k in C.CASES if _have(k) and C.CASES[k].get("bitwise")]
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from spin_colour_kernel_b200 import build
+    build.build()
+
+
+def _sampler(case, s, **over):
+    from spin_colour_kernel_b200.sampler import Sampler
+    kw = C.sampler_kwargs(case)
+    kw.update(over)
+    return Sampler(s, case["B"], device="cuda", seed=case["seed"], **kw)
+
+
+def _spins(A, S):
+    x = A.unpack(S)
+    return x.cpu().numpy()
+
+
+def _compare(name, s, got, ref, record):
+    if s.n == 1:
+        diff = int((got != ref).sum())
+        assert diff == 0, f"{name}: {diff} Ising spins differ"
+    else:
+        d = np.abs(got.astype(np.float64) - ref.astype(np.float64))
+        site_bad = (d > VEC_TOL).any(axis=1)
+        frac = float(site_bad.mean())
+        record.append(frac)
+        assert frac <= 0.02, f"{name}: {frac:.4f} of spins beyond {VEC_TOL} (flipped decisions)"
+
+
+@pytest.mark.parametrize("name", PLAIN)
+def test_cuda_chain_matches_reference_fixture(name):
+    case = C.CASES[name]
+    g = dict(np.load(GOLD / f"{name}.npz"))
+    s = case["build"](sy, cr)
+    A = _sampler(case, s)
+    A.set_temperature(torch.from_numpy(g["T"]))
+    S = A.init_spins(seed=case["init"])
+    assert np.array_equal(_spins(A, S), g["S0"].astype(_spins(A, S).dtype)), "initial spins differ"
+    snaps = {int(k): i for i, k in enumerate(g["snap_ids"])}
+    fracs = []
+    for k in range(1, case["sweeps"] + 1):
+        A.sweep(S)
+        if k in snaps:
+            _compare(name, s, _spins(A, S), g["snaps"][snaps[k]], fracs)
+            E = A.energy(S).cpu().numpy()
+            if s.n == 1:
+                np.testing.assert_allclose(E, g["E"][k - 1], rtol=1e-12, atol=1e-9)
+                np.testing.assert_allclose(A.magnetization(S).cpu().numpy(), g["M"][k - 1], rtol=1e-12, atol=1e-9)
+    if s.n == 1:
+        assert int(A.state[1]) == case["sweeps"]
+    print(f"{name}: fraction of spins beyond tolerance per recorded sweep: {fracs}")
+
+
+@pytest.mark.parametrize("name", BITWISE)
+def test_cuda_bitwise_matches_reference_fixture(name):
+    case = C.CASES[name]
+    g = dict(np.load(GOLD / f"{name}.npz"))
+    s = case["build"](sy, cr)
+    A = _sampler(case, s)
+    A.set_temperature(torch.from_numpy(g["T"]))
+    assert np.array_equal(A.ptab.cpu().numpy(), g["ptab"])
+    S = A.init_spins(seed=case["init"])
+    assert np.array_equal(S.cpu().numpy(), g["W0"])
+    for k in range(1, case["sweeps"] + 1):
+        A.sweep(S)
+        assert np.array_equal(_spins(A, S), g["snaps"][k - 1]), f"{name}: sweep {k}"
+    m = torch.as_tensor(s.site_mask(), device="cuda")
+    assert torch.all(A.unpack(S)[:, 0][:, ~m] == 0)
+
+
+@pytest.mark.parametrize("name", ["ising_sc5_odd", "heis_bcc2", "nanodot_small", "xy_sc1055", "ising_square4_barker"])
+def test_parallel_equals_sequential_chain_on_gpu(name):
+    """The class launches equal the sequential per-site chain (same counters), spin for spin."""
+    case = C.CASES[name]
+    s = case["build"](sy, cr)
+    A, R = _sampler(case, s), _sampler(case, s)
+    for X in (A, R):
+        X.set_temperature(1.5)
+    S1 = A.init_spins(seed=2)
+    S2 = S1.clone()
+    for _ in range(2):
+        A.sweep(S1)
+        R.reference_sweep(S2)
+        assert torch.equal(S1, S2)
+
+
+@pytest.mark.parametrize("independent", [False, True])
+def test_bitwise_parallel_equals_sequential_on_gpu(independent):
+    s = sy.System("Ising sc odd", 1, cr.make("sc"), (5, 5, 5), (True,) * 3, {1: 1.0})
+    from spin_colour_kernel_b200.sampler import Sampler
+    A = Sampler(s, 96, device="cuda", seed=2, bitwise=True, independent=independent)
+    R = Sampler(s, 96, device="cuda", seed=2, bitwise=True, independent=independent)
+    for X in (A, R):
+        X.set_temperature(4.5)
+    S1 = A.init_spins(seed=1)
+    S2 = S1.clone()
+    A.sweep(S1, 2)
+    R.reference_sweep(S2, 2)
+    assert torch.equal(S1, S2)
+
+
+def test_packed_equals_int8_on_larger_box():
+    """Packed storage (32 replicas per word, per-replica Philox) equals the int8 chain spin for spin, with a
+    partial last word, an odd periodic box and a field."""
+    from spin_colour_kernel_b200.sampler import Sampler
+    s = sy.System("Ising sc h", 1, cr.make("sc"), (12, 10, 14), (True,) * 3, {1: 1.0}, h=(0.15,))
+    B = 72
+    P = Sampler(s, B, device="cuda", seed=5)
+    I8 = Sampler(s, B, device="cuda", seed=5, packed=False)
+    assert P.packed and not I8.packed
+    T = torch.linspace(2.5, 6.0, B)
+    for X in (P, I8):
+        X.set_temperature(T)
+    Sp, S8 = P.init_spins(seed=9), I8.init_spins(seed=9)
+    assert torch.equal(P.unpack(Sp), S8)
+    P.sweep(Sp, 3)
+    I8.sweep(S8, 3)
+    assert torch.equal(P.unpack(Sp), S8)
+    assert torch.allclose(P.energy(Sp), I8.energy(S8), rtol=0, atol=1e-9)
+
+
+def test_graph_replay_equals_plain_sweeps():
+    from spin_colour_kernel_b200.sampler import Sampler
+    s = C.heisenberg_bcc_j1j2(sy, cr, 6)
+    A = Sampler(s, 8, device="cuda", seed=7)
+    Bs = Sampler(s, 8, device="cuda", seed=7)
+    for X in (A, Bs):
+        X.set_temperature(torch.linspace(0.5, 2.5, 8))
+    S1 = A.init_spins(seed=2)
+    S2 = S1.clone()
+    rep = A.graph(S1, 3)          # one warm-up sweep, then 3 captured sweeps per replay
+    rep()
+    rep()
+    Bs.sweep(S2, 7)
+    assert torch.equal(S1, S2)
+    assert int(A.state[1]) == 7
+    # in-place temperature change is seen by the captured graph
+    A.set_temperature(torch.full((8,), 0.01))
+    Bs.set_temperature(torch.full((8,), 0.01))
+    rep()
+    Bs.sweep(S2, 3)
+    assert torch.equal(S1, S2)
+
+
+def test_observables_match_oracle_fp64():
+    from spin_colour_kernel_b200.sampler import Sampler
+    for s in (sy.nanodot(Rd=2.5, L=3), C.heisenberg_bcc_j1j2(sy, cr, 4), C.xy_disk(sy, cr, "triangular", 12),
+              sy.ising("fcc", 4)):
+        A = Sampler(s, 5, device="cuda", seed=1)
+        S = A.init_spins(seed=3)
+        E, M = A.observables(S)
+        x = A.unpack(S).cpu().numpy()
+        np.testing.assert_allclose(E.cpu().numpy(), obs.energy(s, x), rtol=1e-12, atol=1e-9)
+        np.testing.assert_allclose(M.cpu().numpy(), obs.magnetization(x), rtol=1e-12, atol=1e-9)
+
+
+def test_sync_sweep_matches_oracle():
+    from spin_colour_kernel_b200.sampler import Sampler
+    from oracle.sweep import sync_sweep
+    s = sy.ising("square", 8)
+    A = Sampler(s, 4, device="cuda", seed=3, packed=False)
+    A.set_temperature(2.2)
+    S = A.init_spins(seed=1)
+    x = S.cpu().numpy().copy()
+    A.sync_sweep(S, 2)
+    sync_sweep(s, x, np.full(4, np.float32(1.0) / np.float32(2.2), np.float32), [3, 0], 2)
+    assert np.array_equal(S.cpu().numpy(), x)
+
+
+def test_refusals_and_counter_limit():
+    from spin_colour_kernel_b200.sampler import Sampler
+    with pytest.raises(ValueError, match="Ising"):
+        Sampler(sy.heisenberg("sc", 4), 32, device="cuda", bitwise=True)
+    with pytest.raises(ValueError, match="uniform"):
+        Sampler(sy.System("J1-J2", 1, cr.make("sc", (1, 2)), (4, 4, 4), (True,) * 3, {1: 1.0, 2: 0.5}), 32,
+                device="cuda", bitwise=True)
+    with pytest.raises(ValueError, match="Philox"):
+        Sampler(sy.ising("sc", 128), 1024, device="cuda", bitwise=True)
+    A = Sampler(sy.ising("square", 4), 64, device="cuda", bitwise=True)
+    A.set_temperature(torch.tensor([2.0] * 32 + [3.0] * 32))
+    with pytest.raises(ValueError, match="word"):
+        A.set_temperature(torch.linspace(2.0, 3.0, 64))
+
+
+# ------------------------------------------------------------------ full-size workloads, checked on a few replicas
+def test_workload3_full_size_replicas_match_oracle():
+    """Heisenberg bcc 64^3 cells (524,288 sites), J1 = 1, J2 = 0.3, K1 = 0.05, h = 0.1 z, 1536 replicas at
+    24 temperatures in [0.5, 2.5]: two sweeps of the whole batch on the GPU; replicas 0, 777 and 1535 are
+    recomputed by the oracle on their own (their Philox counters depend only on their own index)."""
+    from spin_colour_kernel_b200.sampler import Sampler
+    s = C.heisenberg_bcc_j1j2(sy, cr, 64)
+    B = 1536
+    A = Sampler(s, B, device="cuda", seed=1234)
+    T = torch.linspace(0.5, 2.5, 24).repeat_interleave(64)
+    A.set_temperature(T)
+    g = torch.Generator(device="cuda").manual_seed(2)
+    S = torch.randn((B, 3) + s.shape, device="cuda", generator=g)
+    S = (S / S.norm(dim=1, keepdim=True)).contiguous()
+    pick = [0, 777, 1535]
+    x = S[pick].cpu().numpy().copy()
+    A.sweep(S, 2)
+    got = S[pick].cpu().numpy()
+    beta = (np.float32(1.0) / T.numpy()[pick]).astype(np.float32)
+    osw.sweep(s, x, beta, [1234, 0], 2, reps=pick)
+    d = np.abs(got.astype(np.float64) - x)
+    frac = float((d > VEC_TOL).any(axis=1).mean())
+    print(f"workload 3 full size: fraction of spins beyond {VEC_TOL}: {frac:.2e}")
+    assert frac <= 1e-3
+    norms = torch.linalg.vector_norm(S.float(), dim=1)
+    assert torch.allclose(norms, torch.ones_like(norms), atol=1e-5)
+
+
+@pytest.mark.parametrize("independent", [False, True])
+def test_workload2_full_size_words_match_oracle(independent):
+    """3D Ising sc L=128, bitwise, as two counter-legal instances of 512 replicas (base seeds 1 and 2; the
+    reference refuses 1024 x 128^3 >= 2^31 - 1 counters). One sweep of each instance on the GPU; words 0 and 15
+    of each instance (64 replicas) are recomputed by the oracle on their own."""
+    from spin_colour_kernel_b200.sampler import Sampler
+    s = sy.ising("sc", 128)
+    T16 = torch.linspace(4.0, 5.0, 16)
+    for inst, seed in enumerate((1, 2)):
+        A = Sampler(s, 512, device="cuda", seed=seed, bitwise=True, independent=independent)
+        T = T16[8 * inst: 8 * inst + 8].repeat_interleave(64)
+        A.set_temperature(T)
+        g = torch.Generator(device="cuda").manual_seed(1 + inst)
+        S = A.pack(torch.randint(0, 2, (512, 1) + s.shape, device="cuda", generator=g, dtype=torch.int8) * 2 - 1)
+        words = [0, 15]
+        x = A.unpack(S).cpu().numpy()
+        ref = np.concatenate([x[32 * w: 32 * w + 32, 0] for w in words]).astype(np.int64)
+        table = A.ptab.cpu().numpy()[words]
+        A.sweep(S)
+        got = A.unpack(S).cpu().numpy()
+        got = np.concatenate([got[32 * w: 32 * w + 32, 0] for w in words])
+        ref = obw.sweep(s, ref, table, seed, 0, independent=independent, words=words)
+        assert np.array_equal(got, ref)
