@@ -52,20 +52,21 @@ def heisenberg_bcc(L=64):
                      cubic_k1=np.full((2, L, L, L), 0.05, np.float32))
 
 
-def make_workload(name, rank, device):
+def make_workload(name, rank, device, L=64, replicas=1536):
     from spin_colour_kernel_b200 import system as sy
     from spin_colour_kernel_b200.sampler import Sampler
     g = torch.Generator(device=device).manual_seed(2 + rank)
     if name == "heisenberg-bcc":
-        s = heisenberg_bcc(64)
-        B = 1536
+        s = heisenberg_bcc(L)
+        B = replicas
         A = Sampler(s, B, device=device, seed=1234 + 100000 * rank)
-        T = torch.linspace(0.5, 2.5, 24).repeat_interleave(64)
+        T = torch.linspace(0.5, 2.5, 24).repeat_interleave(-(-B // 24))[:B]
         S = torch.randn((B, 3) + s.shape, device=device, generator=g)
         S = (S / S.norm(dim=1, keepdim=True)).contiguous()
-        cfg = {"workload": "heisenberg-bcc-64^3x2-J1J2-K1-hz", "replicas": B, "sites": s.nsite,
-               "temperatures": "24 linear in [0.5, 2.5], 64 replicas each", "spin_dtype": "float32",
-               "l2": "no flush: 9.66 GB state > 126 MB L2"}
+        gb = B * 3 * s.nsite * 4 / 1e9
+        cfg = {"workload": f"heisenberg-bcc-{L}^3x2-J1J2-K1-hz", "replicas": B, "sites": s.nsite,
+               "temperatures": f"24 linear in [0.5, 2.5], {-(-B // 24)} replicas each", "spin_dtype": "float32",
+               "l2": f"no flush: {gb:.2f} GB state > 126 MB L2"}
     elif name == "ising-sc-bitwise":
         s = sy.ising("sc", 128)
         B = 512                                   # one counter-legal instance of the 1024-replica workload
@@ -219,6 +220,8 @@ def main():
     ap.add_argument("--workload", default="heisenberg-bcc", choices=sorted(BYTES_PER_ATTEMPT))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--L", type=int, default=64, help="heisenberg-bcc cells per axis (profiling runs use less)")
+    ap.add_argument("--replicas", type=int, default=1536, help="heisenberg-bcc replicas")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -237,7 +240,7 @@ def main():
     torch.cuda.set_device(device)
     from spin_colour_kernel_b200 import build as bld
     bld.build()
-    s, A, S, T, cfg = make_workload(args.workload, rank, device)
+    s, A, S, T, cfg = make_workload(args.workload, rank, device, args.L, args.replicas)
     attempts_per_step = A.B * s.n_active
     stream = torch.cuda.current_stream(device)
     classes = list(A.classes)
