@@ -61,10 +61,31 @@ static Common make_common(const sck_plan* plan, const sck_buffers* buf, const vo
   c.beta = buf->beta;
   c.table = buf->table;
   c.state = buf->state;
+  c.fd_bx = make_fastdiv((uint32_t)c.bx);
+  c.fd_L1 = make_fastdiv((uint32_t)c.g.L1);
+  c.fd_L2 = make_fastdiv((uint32_t)c.g.L2);
+  for (int r = 0; r < SCK_MAX_FACTORS; ++r) c.fd_m[r] = make_fastdiv((uint32_t)c.col.m[r]);
   return c;
 }
 
 static bool is_bitwise(int mode) { return mode == SCK_MODE_BITWISE || mode == SCK_MODE_BITWISE_INDEP; }
+
+// Replicas per group of the L2 pipeline, or 0 when the sweep runs class by class over all replicas: the
+// specialised kernels only, a state larger than the budget, at least as many groups as classes.
+static int pipeline_group(const sck_plan* p) {
+  if (!p->spec || p->l2_budget <= 0) return 0;
+  const int C = p->desc.n_classes;
+  if (C < 2 || C > 8) return 0;
+  const long long per_rep = (long long)p->geom.nsite * p->geom.n * (p->mode == SCK_MODE_INT8 ? 1 : 4);
+  if (per_rep * p->Bp <= p->l2_budget) return 0;
+  long long group = p->l2_budget / ((long long)C * per_rep);
+  if (p->geom.n > 1) group &= ~1ll;
+  if (group < 1) return 0;
+  const long long cap = (65535 / 8) * (p->geom.n > 1 ? 2 : 1);   // grid rows: tasks x units per task
+  if (group > cap) group = cap;
+  if ((p->Bp + group - 1) / group < C) return 0;
+  return (int)group;
+}
 
 static int check_buffers(const sck_plan* plan, const sck_buffers* buf, bool need_spins) {
   if (plan == nullptr || buf == nullptr) return fail(SCK_ERR_INVALID, "null plan or buffers");
@@ -308,7 +329,24 @@ int sck_plan_create(const sck_system_desc* d, int32_t batch, int32_t mode, sck_p
   while ((1 << np) <= Zmax) ++np;
   p->NP = np < 1 ? 1 : np;
   p->field = (d->n == 1 && d->h64[0] != 0.0) ? 1 : 0;
+  p->spec = find_spec(p);
+  p->l2_budget = 72ll << 20;
   *out = p;
+  return SCK_OK;
+}
+
+int sck_plan_tune(sck_plan* plan, int32_t specialised, int64_t l2_budget_bytes) {
+  if (plan == nullptr || l2_budget_bytes < 0) return fail(SCK_ERR_INVALID, "null plan or negative budget");
+  plan->spec = specialised ? find_spec(plan) : 0;
+  plan->l2_budget = l2_budget_bytes;
+  return SCK_OK;
+}
+
+int sck_plan_path(const sck_plan* plan, int32_t* specialised, int64_t* l2_budget_bytes, int32_t* group) {
+  if (plan == nullptr) return fail(SCK_ERR_INVALID, "null plan");
+  if (specialised) *specialised = plan->spec;
+  if (l2_budget_bytes) *l2_budget_bytes = plan->l2_budget;
+  if (group) *group = pipeline_group(plan);
   return SCK_OK;
 }
 
@@ -363,6 +401,25 @@ int sck_sweep(const sck_plan* plan, const sck_buffers* buf, int32_t n_sweeps, vo
   if (rc != SCK_OK) return rc;
   if (n_sweeps < 0) return fail(SCK_ERR_INVALID, "negative sweep count");
   cudaStream_t s = (cudaStream_t)stream;
+  if (n_sweeps == 0) return SCK_OK;
+  if (plan->spec) {
+    const Common c = make_common(plan, buf, buf->spins);
+    const int group = pipeline_group(plan);
+    if (group > 0) {
+      rc = launch_spec_pipeline(plan, c, n_sweeps, group, s);
+      if (rc != SCK_OK) return rc;
+      return launch_advance(buf->state, n_sweeps, s);
+    }
+    for (int k = 0; k < n_sweeps; ++k) {
+      for (int i = 0; i < plan->desc.n_classes; ++i) {
+        rc = launch_spec_class(plan, c, plan->desc.classes[i][0], plan->desc.classes[i][1], s);
+        if (rc != SCK_OK) return rc;
+      }
+      rc = launch_advance(buf->state, 1, s);
+      if (rc != SCK_OK) return rc;
+    }
+    return SCK_OK;
+  }
   for (int k = 0; k < n_sweeps; ++k) {
     for (int i = 0; i < plan->desc.n_classes; ++i) {
       rc = class_launch(plan, buf, buf->spins, plan->desc.classes[i][0], plan->desc.classes[i][1], s);

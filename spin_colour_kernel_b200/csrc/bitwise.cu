@@ -15,22 +15,6 @@
 
 namespace sck {
 
-__device__ __forceinline__ bool class_site_bw(const Common& c, int colour, int alpha, long long t, int& x, int& y,
-                                              int& z) {
-  int row = (int)(t / c.bx);
-  int j = (int)(t - (long long)row * c.bx);
-  z = row / c.g.L2;
-  y = row - z * c.g.L2;
-  int x0 = 0;
-  if (colour >= 0) {
-    x0 = c.g.L1;
-    for (int q = 0; q < c.P; ++q)
-      if (colour_of(c.col, alpha, q, y, z) == colour) x0 = q;
-  }
-  x = x0 + c.P * j;
-  return x < c.g.L1;
-}
-
 constexpr int bitlen(int v) { return v <= 0 ? 0 : 1 + bitlen(v >> 1); }
 
 // Count planes of one (word, site): returns z_eff; planes c[0..NP).
@@ -159,18 +143,18 @@ __device__ __forceinline__ void independent_site(const Common& c, const SubDev& 
   dst[wb + own] = s0 ^ acc;
 }
 
+// Grid (ceil(rows * bx / 256), units): units are groups of four words (shared) or words (independent).
 template <int ZM, bool INDEP>
 __global__ void __launch_bounds__(256) bitwise_class_kernel(const __grid_constant__ ClassParams p) {
   const Common& c = p.c;
-  const long long per = (long long)c.rows * c.bx;
+  const uint32_t per = (uint32_t)c.rows * (uint32_t)c.bx;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= per) return;
+  int x, y, z;
+  if (!class_site(c, p.colour, p.alpha, t, x, y, z)) return;
   const int units = INDEP ? c.W : (c.W + 3) / 4;
-  const long long total = per * units;
   const int32_t key = sweep_key(c.state);
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    const int u = (int)(t / per);
-    int x, y, z;
-    if (!class_site_bw(c, p.colour, p.alpha, t - (long long)u * per, x, y, z)) continue;
+  for (int u = blockIdx.y; u < units; u += gridDim.y) {
     if (INDEP)
       independent_site<ZM>(c, p.sub, p.alpha, u, x, y, z, key, (const uint32_t*)c.src, (uint32_t*)c.dst);
     else
@@ -201,7 +185,7 @@ __global__ void bitwise_sequential_kernel(const __grid_constant__ SeqParams p) {
 }
 
 template <bool INDEP>
-static void class_dispatch(int Z, const ClassParams& p, int grid, cudaStream_t s) {
+static void class_dispatch(int Z, const ClassParams& p, dim3 grid, cudaStream_t s) {
   if (Z <= 4) bitwise_class_kernel<4, INDEP><<<grid, 256, 0, s>>>(p);
   else if (Z <= 6) bitwise_class_kernel<6, INDEP><<<grid, 256, 0, s>>>(p);
   else if (Z <= 8) bitwise_class_kernel<8, INDEP><<<grid, 256, 0, s>>>(p);
@@ -228,19 +212,15 @@ int launch_bitwise_class(const sck_plan* plan, const Common& c, int colour, int 
   p.sub = plan->sub[alpha];
   p.colour = colour;
   p.alpha = alpha;
-  if (colour < 0) {
-    p.c.P = 1;
-    p.c.bx = c.g.L1;
-  }
+  if (colour < 0) set_rows(p.c, 1, c.g.L1);
   const bool indep = plan->mode == SCK_MODE_BITWISE_INDEP;
-  const long long units = indep ? c.W : (c.W + 3) / 4;
-  long long total = (long long)p.c.rows * p.c.bx * units;
-  long long grid = (total + 255) / 256;
-  if (grid > 148LL * 64) grid = 148LL * 64;
+  const int units = indep ? c.W : (c.W + 3) / 4;
+  const uint32_t per = (uint32_t)p.c.rows * (uint32_t)p.c.bx;
+  const dim3 grid((per + 255) / 256, (unsigned)(units < 65535 ? units : 65535));
   if (indep)
-    class_dispatch<true>(plan->Z, p, (int)grid, s);
+    class_dispatch<true>(plan->Z, p, grid, s);
   else
-    class_dispatch<false>(plan->Z, p, (int)grid, s);
+    class_dispatch<false>(plan->Z, p, grid, s);
   return cuda_status(cudaGetLastError(), "bitwise class launch");
 }
 

@@ -53,6 +53,26 @@ struct SubObs {
   double E[SCK_MAX_EXTRA][9];
 };
 
+// ------------------------------------------------------------------------------------------- fast division
+// Division by a runtime-invariant divisor d >= 1 through one 32x32->64 multiply and a shift (Granlund and
+// Montgomery, PLDI'94): with l = ceil(log2 d), m = ceil(2^(31+l) / d) fits in 32 bits and
+// floor(n m / 2^(31+l)) = floor(n / d) for every 0 <= n < 2^31 (the rounding error n (m d - 2^(31+l)) /
+// (d 2^(31+l)) stays below 2^-l <= 1/d).
+struct FastDiv {
+  uint32_t m, s;
+};
+
+inline FastDiv make_fastdiv(uint32_t d) {
+  uint32_t l = 0;
+  while ((1ull << l) < d) ++l;
+  const unsigned long long m = ((1ull << (31 + l)) + d - 1) / d;
+  return FastDiv{(uint32_t)m, 31 + l};
+}
+
+__host__ __device__ __forceinline__ uint32_t fdiv(uint32_t n, FastDiv f) {
+  return (uint32_t)(((unsigned long long)n * f.m) >> f.s);
+}
+
 // ------------------------------------------------------------------------------------------------- helpers
 __host__ __device__ inline int colour_of(const Colouring& c, int a, int x, int y, int z) {
   int idx = 0;
@@ -63,12 +83,14 @@ __host__ __device__ inline int colour_of(const Colouring& c, int a, int x, int y
   return idx;
 }
 
-// Neighbour coordinate along one axis: periodic wrap, or -1 outside an open box.
+// Neighbour coordinate along one axis: periodic wrap, or -1 outside an open box. Offsets are bounded by the
+// descriptor check (|d| <= 64); the remainder is taken only when a tiny box needs more than one wrap.
 __device__ __forceinline__ int wrap_axis(int x, int d, int L, int periodic) {
   int q = x + d;
   if (periodic) {
-    q %= L;
     if (q < 0) q += L;
+    else if (q >= L) q -= L;
+    if ((unsigned)q >= (unsigned)L) q = ((q % L) + L) % L;
     return q;
   }
   return (q >= 0 && q < L) ? q : -1;

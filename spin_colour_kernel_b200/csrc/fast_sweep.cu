@@ -1,0 +1,385 @@
+// Specialised class kernels for the common crystals and the L2-resident group pipeline.
+//
+// Specialisation. When a system's bond lists equal one of the compile-time tables of lattices.h (one coupling
+// group per shell, no extra matrices), its class launches run kernels in which every neighbour offset is a
+// constant: the wrapped coordinates of a site are formed once for offsets -R..R per axis and every bond costs
+// one add and one load per component. Ising keeps the integer key and the host table (bit-exact); vector models
+// run two replicas per thread in packed float32x2 arithmetic (add.rn.f32x2 / mul.rn.f32x2, round-to-nearest
+// per lane, same operation order as the generic kernel), with proposal trigonometry and exp on the SFU
+// (__sinf / __cosf on [-pi, pi], __expf): per-spin differences from the reference stay ~1e-6.
+//
+// Group pipeline. A sweep visits its C classes in order, and each class launch reads the whole state. When the
+// state is larger than L2, the replicas are cut into groups whose C-group working set fits in L2, and launch k
+// runs class c on group k - c for every c at once (a diagonal over (group, class)): the C launches that touch a
+// group run back to back, so after its first read from HBM a group stays in L2 until its sweep is done. Each
+// replica's chain is unchanged: its classes still run in order, one launch after another.
+#include <type_traits>
+
+#include "internal.h"
+#include "lattices.h"
+
+namespace sck {
+
+// Wrapped coordinates of one site for compile-time offsets -R..R on each axis.
+template <int R>
+struct Around {
+  int xo[2 * R + 1], yo[2 * R + 1], zo[2 * R + 1];
+  bool xv[2 * R + 1], yv[2 * R + 1], zv[2 * R + 1];
+
+  __device__ __forceinline__ Around(const Geometry& g, int x, int y, int z) {
+#pragma unroll
+    for (int d = -R; d <= R; ++d) {
+      const int qx = wrap_axis(x, d, g.L1, g.per[0]);
+      const int qy = wrap_axis(y, d, g.L2, g.per[1]);
+      const int qz = wrap_axis(z, d, g.L3, g.per[2]);
+      xv[d + R] = qx >= 0;
+      yv[d + R] = qy >= 0;
+      zv[d + R] = qz >= 0;
+      xo[d + R] = qx < 0 ? 0 : qx;
+      yo[d + R] = (qy < 0 ? 0 : qy) * g.L1;
+      zo[d + R] = (qz < 0 ? 0 : qz) * g.L2 * g.L1;
+    }
+  }
+  __device__ __forceinline__ int index(const Geometry& g, const BondC b) const {
+    return b.a2 * g.plane + zo[b.dz + R] + yo[b.dy + R] + xo[b.dx + R];
+  }
+  __device__ __forceinline__ bool valid(const BondC b) const { return xv[b.dx + R] && yv[b.dy + R] && zv[b.dz + R]; }
+};
+
+struct Task {
+  int colour, alpha, rep_begin, rep_end, sweep_offset;
+};
+
+constexpr int kMaxTasks = 8;
+
+struct SpecParams {
+  Common c;
+  float J[SCK_MAX_BASIS][SCK_MAX_GROUPS];
+  int n_tasks;
+  int units_per_task;     // grid.y slots per task (replicas, or replica pairs for vector models)
+  Task tasks[kMaxTasks];
+};
+
+__device__ __forceinline__ int32_t sweep_key_at(const int64_t* state, int offset) {
+  const uint64_t v = (uint64_t)state[0] * 1000003ull + (uint64_t)(state[1] + offset) * 7919ull + 12345ull;
+  return (int32_t)((int64_t)v % 2147483629ll);
+}
+
+__device__ __forceinline__ uint32_t counter_of(int rep, int nsite, int own) {
+  return (uint32_t)((unsigned long long)rep * (unsigned long long)nsite + (unsigned long long)own);
+}
+
+template <typename T>
+__device__ __forceinline__ int sgn(T v) { return (v > T(0)) - (v < T(0)); }
+
+// Compile-time loop: f(std::integral_constant<int, I>) for I in [B, E).
+template <int I, int E, class F>
+__device__ __forceinline__ void static_for(F&& f) {
+  if constexpr (I < E) {
+    f(std::integral_constant<int, I>{});
+    static_for<I + 1, E>(f);
+  }
+}
+
+template <class Lat, int A, int G>
+struct GroupRange {
+  static constexpr int begin = G == 0 ? 0 : Lat::group_end(A, G - 1);
+  static constexpr int end = Lat::group_end(A, G);
+};
+
+// ---------------------------------------------------------------------------------------------------- Ising
+template <class Lat, int A, typename ST>
+__device__ __forceinline__ void ising_spec_site(const Common& c, int rep, int x, int y, int z, int32_t key) {
+  const Geometry& g = c.g;
+  const int own = A * g.plane + (z * g.L2 + y) * g.L1 + x;
+  if (g.has_mask && c.mask[own] == 0) return;
+  const ST* src = (const ST*)c.src;
+  ST* dst = (ST*)c.dst;
+  const size_t base = (size_t)rep * g.nsite;
+  const int s = sgn(src[base + own]);
+  const Around<Lat::reach> nb(g, x, y, z);
+  int k = s > 0 ? 1 : 0;
+  int stride = 2;
+  static_for<0, Lat::groups>([&](auto gc) {
+    using R = GroupRange<Lat, A, decltype(gc)::value>;
+    int G = 0;
+    static_for<R::begin, R::end>([&](auto ic) {
+      constexpr BondC bd = Lat::bond(A, decltype(ic)::value);
+      G += nb.valid(bd) ? sgn(src[base + nb.index(g, bd)]) : 0;
+    });
+    k += (G + (R::end - R::begin)) * stride;
+    stride *= 2 * (R::end - R::begin) + 1;
+  });
+  const float e = ((const float*)c.table)[(size_t)rep * c.lut_rep_stride + A * c.keys + k];
+  const Philox4 r = philox4x32_10(counter_of(rep, g.nsite, own), 0u, key_lo(key), key_hi(key));
+  const float u0 = to_uniform(r.x0);
+  const bool acc = g.acceptance == SCK_BARKER ? __fmul_rn(u0, __fadd_rn(1.0f, e)) < 1.0f : u0 < e;
+  if (acc) dst[base + own] = (ST)(-s);
+}
+
+// --------------------------------------------------------------------------------------------- vector models
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+
+// sin and cos of phi in [0, 2 pi] through the SFU on the reduced range [-pi, pi].
+__device__ __forceinline__ void sincos_2pi(float phi, float& sn, float& cs) {
+  const float red = phi - 3.14159265358979f;
+  sn = -__sinf(red);
+  cs = -__cosf(red);
+}
+
+// Two replicas (lanes .x and .y) of one class site. `two` = false runs lane y as a copy of lane x and stores
+// lane x only (an odd replica count).
+template <class Lat, int A, int N>
+__device__ __forceinline__ void vec_spec_pair(const Common& c, const float (&J)[SCK_MAX_GROUPS], int rep0, bool two,
+                                              int x, int y, int z, int32_t key) {
+  const Geometry& g = c.g;
+  const int own = A * g.plane + (z * g.L2 + y) * g.L1 + x;
+  if (g.has_mask && c.mask[own] == 0) return;
+  const float* src = (const float*)c.src;
+  float* dst = (float*)c.dst;
+  const int rep1 = two ? rep0 + 1 : rep0;
+  const size_t b0 = (size_t)rep0 * N * g.nsite, b1 = (size_t)rep1 * N * g.nsite;
+  const Around<Lat::reach> nb(g, x, y, z);
+  float2 s[N], v[N];
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    s[k] = make_float2(src[b0 + (size_t)k * g.nsite + own], src[b1 + (size_t)k * g.nsite + own]);
+    v[k] = f2(0.0f);
+  }
+  static_for<0, Lat::groups>([&](auto gc) {
+    constexpr int gi = decltype(gc)::value;
+    using R = GroupRange<Lat, A, gi>;
+    float2 gs[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) gs[k] = f2(0.0f);
+    static_for<R::begin, R::end>([&](auto ic) {
+      constexpr BondC bd = Lat::bond(A, decltype(ic)::value);
+      const int q = nb.index(g, bd);
+      const bool ok = nb.valid(bd);
+#pragma unroll
+      for (int k = 0; k < N; ++k) {
+        const float2 t = ok ? make_float2(src[b0 + (size_t)k * g.nsite + q], src[b1 + (size_t)k * g.nsite + q]) : f2(0.0f);
+        gs[k] = __fadd2_rn(gs[k], t);
+      }
+    });
+#pragma unroll
+    for (int k = 0; k < N; ++k) v[k] = __fadd2_rn(v[k], __fmul2_rn(f2(J[gi]), gs[k]));
+  });
+#pragma unroll
+  for (int k = 0; k < N; ++k)
+    if (c.hnz[k]) v[k] = __fadd2_rn(v[k], f2(c.h[k]));
+
+  const Philox4 ra = philox4x32_10(counter_of(rep0, g.nsite, own), 0u, key_lo(key), key_hi(key));
+  const Philox4 rb = two ? philox4x32_10(counter_of(rep1, g.nsite, own), 0u, key_lo(key), key_hi(key)) : ra;
+  const float2 u0 = make_float2(to_uniform(ra.x0), to_uniform(rb.x0));
+  const float TWO_PI = 6.2831855f;
+  float2 t[N];
+  if constexpr (N == 2) {
+    float sa, ca, sb, cb;
+    sincos_2pi(__fmul_rn(TWO_PI, to_uniform(ra.x1)), sa, ca);
+    sincos_2pi(__fmul_rn(TWO_PI, to_uniform(rb.x1)), sb, cb);
+    t[0] = make_float2(ca, cb);
+    t[1] = make_float2(sa, sb);
+  } else {
+    const float2 u1 = make_float2(to_uniform(ra.x1), to_uniform(rb.x1));
+    const float2 cz = __fadd2_rn(__fmul2_rn(f2(2.0f), u1), f2(-1.0f));
+    float sa, ca, sb, cb;
+    sincos_2pi(__fmul_rn(TWO_PI, to_uniform(ra.x2)), sa, ca);
+    sincos_2pi(__fmul_rn(TWO_PI, to_uniform(rb.x2)), sb, cb);
+    const float2 w = __fadd2_rn(f2(1.0f), __fmul2_rn(f2(-1.0f), __fmul2_rn(cz, cz)));
+    const float2 rr = make_float2(sqrtf(fmaxf(w.x, 0.0f)), sqrtf(fmaxf(w.y, 0.0f)));
+    t[0] = __fmul2_rn(rr, make_float2(ca, cb));
+    t[1] = __fmul2_rn(rr, make_float2(sa, sb));
+    t[2] = cz;
+  }
+  const float2 m1 = f2(-1.0f);
+  float2 d = __fmul2_rn(__fadd2_rn(t[0], __fmul2_rn(m1, s[0])), v[0]);
+#pragma unroll
+  for (int k = 1; k < N; ++k) d = __fadd2_rn(d, __fmul2_rn(__fadd2_rn(t[k], __fmul2_rn(m1, s[k])), v[k]));
+  float2 dE = __fmul2_rn(m1, d);
+  if constexpr (N == 3) {
+    if (g.has_cubic) {
+      const float2 k1 = f2(c.k1[own]);
+      const float2 k2 = f2(c.k2);
+      auto aniso = [&](const float2* p) {
+        const float2 q01 = __fmul2_rn(p[0], p[1]), q02 = __fmul2_rn(p[0], p[2]), q12 = __fmul2_rn(p[1], p[2]);
+        const float2 tri = __fmul2_rn(q01, p[2]);
+        const float2 quad = __fadd2_rn(__fadd2_rn(__fmul2_rn(q01, q01), __fmul2_rn(q02, q02)), __fmul2_rn(q12, q12));
+        return __fadd2_rn(__fmul2_rn(k1, quad), __fmul2_rn(__fmul2_rn(k2, tri), tri));
+      };
+      dE = __fadd2_rn(dE, __fadd2_rn(aniso(t), __fmul2_rn(m1, aniso(s))));
+    }
+  }
+  const float2 beta = make_float2(c.beta[rep0], c.beta[rep1]);
+  bool acc0, acc1;
+  if (g.acceptance == SCK_BARKER) {
+    const float2 xb = __fmul2_rn(beta, dE);
+    acc0 = __fmul_rn(u0.x, __fadd_rn(1.0f, __expf(xb.x))) < 1.0f;
+    acc1 = __fmul_rn(u0.y, __fadd_rn(1.0f, __expf(xb.y))) < 1.0f;
+  } else {
+    const float2 xm = __fmul2_rn(__fmul2_rn(m1, beta), dE);
+    acc0 = u0.x < __expf(xm.x);
+    acc1 = u0.y < __expf(xm.y);
+  }
+  if (acc0) {
+#pragma unroll
+    for (int k = 0; k < N; ++k) dst[b0 + (size_t)k * g.nsite + own] = t[k].x;
+  }
+  if (two && acc1) {
+#pragma unroll
+    for (int k = 0; k < N; ++k) dst[b1 + (size_t)k * g.nsite + own] = t[k].y;
+  }
+}
+
+// ------------------------------------------------------------------------------------------------- kernels
+// Grid (ceil(rows * bx / 256), n_tasks * units_per_task). Block y-slot -> (task, replica or replica pair).
+template <class Lat, int N, typename ST>
+__global__ void __launch_bounds__(256) spec_task_kernel(const __grid_constant__ SpecParams p) {
+  const uint32_t per = (uint32_t)p.c.rows * (uint32_t)p.c.bx;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= per) return;
+  const int ti = blockIdx.y / p.units_per_task;
+  const int unit = blockIdx.y - ti * p.units_per_task;
+  const Task task = p.tasks[ti];
+  constexpr int per_unit = N == 1 ? 1 : 2;
+  const int rep = task.rep_begin + unit * per_unit;
+  if (rep >= task.rep_end) return;
+  int x, y, z;
+  if (!class_site(p.c, task.colour, task.alpha, t, x, y, z)) return;
+  const int32_t key = sweep_key_at(p.c.state, task.sweep_offset);
+#pragma unroll
+  for (int a = 0; a < Lat::b; ++a) {
+    if (a == task.alpha) {
+      if constexpr (N == 1) {
+        switch (a) {
+          case 0: ising_spec_site<Lat, 0, ST>(p.c, rep, x, y, z, key); break;
+          case 1: ising_spec_site<Lat, (Lat::b > 1 ? 1 : 0), ST>(p.c, rep, x, y, z, key); break;
+          case 2: ising_spec_site<Lat, (Lat::b > 2 ? 2 : 0), ST>(p.c, rep, x, y, z, key); break;
+          default: ising_spec_site<Lat, (Lat::b > 3 ? 3 : 0), ST>(p.c, rep, x, y, z, key); break;
+        }
+      } else {
+        const bool two = rep + 1 < task.rep_end;
+        switch (a) {
+          case 0: vec_spec_pair<Lat, 0, N>(p.c, p.J[0], rep, two, x, y, z, key); break;
+          case 1: vec_spec_pair<Lat, (Lat::b > 1 ? 1 : 0), N>(p.c, p.J[1], rep, two, x, y, z, key); break;
+          case 2: vec_spec_pair<Lat, (Lat::b > 2 ? 2 : 0), N>(p.c, p.J[2], rep, two, x, y, z, key); break;
+          default: vec_spec_pair<Lat, (Lat::b > 3 ? 3 : 0), N>(p.c, p.J[3], rep, two, x, y, z, key); break;
+        }
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------ host: matching
+template <class Lat>
+static bool matches(const sck_plan* p) {
+  const sck_system_desc& d = p->desc;
+  if (d.b != Lat::b || d.dim != Lat::dim) return false;
+  for (int a = 0; a < d.b; ++a) {
+    const sck_sublattice& s = d.sub[a];
+    if (s.n_groups != Lat::groups || s.n_bonds != Lat::n_bonds(a) || s.n_extra != 0) return false;
+    for (int gi = 0; gi < s.n_groups; ++gi)
+      if (!s.group_apply[gi] || s.group_end[gi] != Lat::group_end(a, gi)) return false;
+    for (int i = 0; i < s.n_bonds; ++i) {
+      const BondC b = Lat::bond(a, i);
+      const sck_bond& e = s.bonds[i];
+      if (e.alpha2 != b.a2 || e.d[0] != b.dx || e.d[1] != b.dy || e.d[2] != b.dz || e.extra != -1) return false;
+    }
+  }
+  return true;
+}
+
+int find_spec(const sck_plan* p) {
+  if (p->mode != SCK_MODE_INT8 && p->mode != SCK_MODE_F32) return 0;
+  if (matches<Lat_square_1>(p)) return Lat_square_1::id;
+  if (matches<Lat_triangular_1>(p)) return Lat_triangular_1::id;
+  if (matches<Lat_sc_1>(p)) return Lat_sc_1::id;
+  if (matches<Lat_bcc_1>(p)) return Lat_bcc_1::id;
+  if (matches<Lat_bcc_1_2>(p)) return Lat_bcc_1_2::id;
+  if (matches<Lat_fcc_1>(p)) return Lat_fcc_1::id;
+  return 0;
+}
+
+// ------------------------------------------------------------------------------------------- host: launches
+template <class Lat>
+static void launch_lat(const sck_plan* plan, const SpecParams& p, dim3 grid, cudaStream_t s) {
+  if (plan->geom.n == 1) {
+    if (plan->mode == SCK_MODE_INT8)
+      spec_task_kernel<Lat, 1, int8_t><<<grid, 256, 0, s>>>(p);
+    else
+      spec_task_kernel<Lat, 1, float><<<grid, 256, 0, s>>>(p);
+  } else if (plan->geom.n == 2) {
+    spec_task_kernel<Lat, 2, float><<<grid, 256, 0, s>>>(p);
+  } else {
+    spec_task_kernel<Lat, 3, float><<<grid, 256, 0, s>>>(p);
+  }
+}
+
+static int launch_tasks(const sck_plan* plan, SpecParams& p, cudaStream_t s) {
+  const uint32_t per = (uint32_t)p.c.rows * (uint32_t)p.c.bx;
+  const int per_unit = plan->geom.n == 1 ? 1 : 2;
+  int most = 1;
+  for (int i = 0; i < p.n_tasks; ++i) {
+    const int n = p.tasks[i].rep_end - p.tasks[i].rep_begin;
+    if (n > most) most = n;
+  }
+  p.units_per_task = (most + per_unit - 1) / per_unit;
+  const long long ys = (long long)p.units_per_task * p.n_tasks;
+  if (ys > 65535) return cuda_status(cudaErrorInvalidConfiguration, "task launch: too many replicas per launch");
+  const dim3 grid((per + 255) / 256, (unsigned)ys);
+  switch (plan->spec) {
+    case Lat_square_1::id: launch_lat<Lat_square_1>(plan, p, grid, s); break;
+    case Lat_triangular_1::id: launch_lat<Lat_triangular_1>(plan, p, grid, s); break;
+    case Lat_sc_1::id: launch_lat<Lat_sc_1>(plan, p, grid, s); break;
+    case Lat_bcc_1::id: launch_lat<Lat_bcc_1>(plan, p, grid, s); break;
+    case Lat_bcc_1_2::id: launch_lat<Lat_bcc_1_2>(plan, p, grid, s); break;
+    default: launch_lat<Lat_fcc_1>(plan, p, grid, s); break;
+  }
+  return cuda_status(cudaGetLastError(), "specialised class launch");
+}
+
+static SpecParams spec_params(const sck_plan* plan, const Common& c) {
+  SpecParams p;
+  memset(&p, 0, sizeof(p));
+  p.c = c;
+  for (int a = 0; a < SCK_MAX_BASIS; ++a)
+    for (int gi = 0; gi < SCK_MAX_GROUPS; ++gi) p.J[a][gi] = plan->sub[a].J[gi];
+  return p;
+}
+
+// One class over all replicas, in chunks of at most 65535 grid rows.
+int launch_spec_class(const sck_plan* plan, const Common& c, int colour, int alpha, cudaStream_t s) {
+  SpecParams p = spec_params(plan, c);
+  const int per_unit = plan->geom.n == 1 ? 1 : 2;
+  const int chunk = 65535 * per_unit;
+  for (int r0 = 0; r0 < c.B; r0 += chunk) {
+    p.n_tasks = 1;
+    p.tasks[0] = Task{colour, alpha, r0, r0 + chunk < c.B ? r0 + chunk : c.B, 0};
+    const int rc = launch_tasks(plan, p, s);
+    if (rc != SCK_OK) return rc;
+  }
+  return SCK_OK;
+}
+
+// n sweeps as a diagonal over (sweep-major group unit, class); state[1] is advanced by the caller.
+int launch_spec_pipeline(const sck_plan* plan, const Common& c, int n_sweeps, int group, cudaStream_t s) {
+  const int C = plan->desc.n_classes;
+  const int ngroups = (c.B + group - 1) / group;
+  const long long units = (long long)n_sweeps * ngroups;
+  SpecParams p = spec_params(plan, c);
+  for (long long k = 0; k < units + C - 1; ++k) {
+    p.n_tasks = 0;
+    for (int ci = 0; ci < C; ++ci) {
+      const long long u = k - ci;
+      if (u < 0 || u >= units) continue;
+      const int sw = (int)(u / ngroups), gi = (int)(u - (long long)sw * ngroups);
+      const int r0 = gi * group, r1 = r0 + group < c.B ? r0 + group : c.B;
+      p.tasks[p.n_tasks++] = Task{plan->desc.classes[ci][0], plan->desc.classes[ci][1], r0, r1, sw};
+    }
+    const int rc = launch_tasks(plan, p, s);
+    if (rc != SCK_OK) return rc;
+  }
+  return SCK_OK;
+}
+
+}  // namespace sck

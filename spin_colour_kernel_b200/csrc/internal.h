@@ -30,7 +30,48 @@ struct Common {
   const float* beta;
   const void* table;
   const int64_t* state;
+  FastDiv fd_bx, fd_L1, fd_L2, fd_m[SCK_MAX_FACTORS];
 };
+
+// (t = row * bx + j) -> class site (x, y, z) of class `colour` on sublattice `alpha`, false when the row holds
+// no site of the class. Along a row the colour has period P and each colour of the row appears at most once
+// per period, so the row's first site x0 is found by stepping the per-factor residues through one period.
+__device__ __forceinline__ bool class_site(const Common& c, int colour, int alpha, uint32_t t, int& x, int& y,
+                                           int& z) {
+  const uint32_t row = fdiv(t, c.fd_bx);
+  const int j = (int)(t - row * (uint32_t)c.bx);
+  z = (int)fdiv(row, c.fd_L2);
+  y = (int)row - z * c.g.L2;
+  int x0 = 0;
+  if (colour >= 0) {
+    int g[SCK_MAX_FACTORS];
+#pragma unroll
+    for (int r = 0; r < SCK_MAX_FACTORS; ++r) {
+      if (r < c.col.r) {
+        const uint32_t v = (uint32_t)(c.col.K[r][1] * y + c.col.K[r][2] * z + c.col.o[alpha][r]);
+        g[r] = (int)(v - fdiv(v, c.fd_m[r]) * (uint32_t)c.col.m[r]);
+      }
+    }
+    x0 = c.g.L1;
+    for (int q = 0; q < c.P; ++q) {
+      int idx = 0;
+#pragma unroll
+      for (int r = 0; r < SCK_MAX_FACTORS; ++r) {
+        if (r < c.col.r) {
+          idx = idx * c.col.m[r] + g[r];
+          g[r] += c.col.K[r][0];
+          if (g[r] >= c.col.m[r]) g[r] -= c.col.m[r];
+        }
+      }
+      if (idx == colour) {
+        x0 = q;
+        break;
+      }
+    }
+  }
+  x = x0 + c.P * j;
+  return x < c.g.L1;
+}
 
 struct ClassParams {
   Common c;
@@ -53,6 +94,7 @@ struct ObsParams {
   double h64[3];
   double k2;
   int blocks_per_rep;
+  FastDiv fd_plane, fd_L1, fd_L2;
   const void* spins;
   const int8_t* mask;
   const float* k1;
@@ -75,9 +117,12 @@ struct sck_plan {
   int keys;
   int Z, Z1, NP, field;
   int ising_lut;   // Ising chain with the host-built exp table (INT8, F32 with n = 1, PACKED)
+  int spec;        // id of the matching compile-time lattice table (lattices.h), 0 = generic kernels
+  long long l2_budget;  // bytes of L2 the group pipeline may fill
 };
 
 namespace sck {
+void set_rows(Common& c, int P, int bx);
 void set_error(const std::string& msg);
 int cuda_status(cudaError_t e, const char* where);
 
@@ -92,4 +137,7 @@ int launch_observables(const sck_plan* plan, const void* spins, int storage, int
 int launch_pack(const sck_plan* plan, const int8_t* spins, int32_t* words, cudaStream_t s);
 int launch_unpack(const sck_plan* plan, const int32_t* words, const int8_t* mask, int8_t* spins, cudaStream_t s);
 int launch_advance(int64_t* state, int n, cudaStream_t s);
+int find_spec(const sck_plan* plan);
+int launch_spec_class(const sck_plan* plan, const Common& c, int colour, int alpha, cudaStream_t s);
+int launch_spec_pipeline(const sck_plan* plan, const Common& c, int n_sweeps, int group, cudaStream_t s);
 }  // namespace sck

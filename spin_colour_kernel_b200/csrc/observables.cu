@@ -35,11 +35,12 @@ __global__ void __launch_bounds__(256) observables_kernel(const __grid_constant_
   for (int i = 0; i < NV; ++i) acc[i] = 0.0;
   for (int site = blockIdx.x * blockDim.x + threadIdx.x; site < g.nsite; site += p.blocks_per_rep * blockDim.x) {
     if (p.mask != nullptr && p.mask[site] == 0) continue;
-    const int alpha = site / g.plane;
+    const int alpha = (int)fdiv((uint32_t)site, p.fd_plane);
     const int rem = site - alpha * g.plane;
-    const int z = rem / (g.L2 * g.L1);
-    const int y = (rem / g.L1) % g.L2;
-    const int x = rem % g.L1;
+    const int row = (int)fdiv((uint32_t)rem, p.fd_L1);
+    const int x = rem - row * g.L1;
+    const int z = (int)fdiv((uint32_t)row, p.fd_L2);
+    const int y = row - z * g.L2;
     double s[N];
     load_spin<N, STORE>(p, rep, site, s);
     double v[N];
@@ -133,6 +134,10 @@ int launch_observables(const sck_plan* plan, const void* spins, int storage, int
   for (int k = 0; k < 3; ++k) p.h64[k] = plan->desc.h64[k];
   p.k2 = plan->desc.k2_64;
   p.blocks_per_rep = obs_blocks_per_rep(plan, batch);
+  p.fd_plane = make_fastdiv((uint32_t)plan->geom.plane);
+  p.fd_L1 = make_fastdiv((uint32_t)plan->geom.L1);
+  p.fd_L2 = make_fastdiv((uint32_t)plan->geom.L2);
+  if (batch > 65535) return cuda_status(cudaErrorInvalidConfiguration, "observables: batch above 65535");
   p.spins = spins;
   p.mask = plan->geom.has_mask ? mask : nullptr;
   p.k1 = k1;

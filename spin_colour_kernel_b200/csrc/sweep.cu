@@ -16,24 +16,6 @@
 
 namespace sck {
 
-// ---------------------------------------------------------------------------------------------- enumeration
-// (row, j) -> site (x, y, z) of class `colour` on sublattice `alpha`; false when the row has no such site.
-__device__ __forceinline__ bool class_site(const Common& c, int colour, int alpha, long long t, int& x, int& y,
-                                           int& z) {
-  int row = (int)(t / c.bx);
-  int j = (int)(t - (long long)row * c.bx);
-  z = row / c.g.L2;
-  y = row - z * c.g.L2;
-  int x0 = 0;
-  if (colour >= 0) {
-    x0 = c.g.L1;
-    for (int q = 0; q < c.P; ++q)
-      if (colour_of(c.col, alpha, q, y, z) == colour) x0 = q;
-  }
-  x = x0 + c.P * j;
-  return x < c.g.L1;
-}
-
 __device__ __forceinline__ uint32_t counter32(long long rep, int nsite, int own) {
   return (uint32_t)((unsigned long long)rep * (unsigned long long)nsite + (unsigned long long)own);
 }
@@ -193,38 +175,36 @@ __device__ __forceinline__ void plain_site(const Common& c, const SubDev& sub, i
   }
 }
 
+// Grid (ceil(rows * bx / 256), replicas): thread t of a replica owns class site t = row * bx + j.
 template <int N, typename ST>
 __global__ void __launch_bounds__(256) plain_class_kernel(const __grid_constant__ ClassParams p) {
-  const long long per_rep = (long long)p.c.rows * p.c.bx;
-  const long long total = per_rep * p.c.B;
+  const uint32_t per_rep = (uint32_t)p.c.rows * (uint32_t)p.c.bx;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= per_rep) return;
+  int x, y, z;
+  if (!class_site(p.c, p.colour, p.alpha, t, x, y, z)) return;
   const int32_t key = sweep_key(p.c.state);
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    const int rep = (int)(t / per_rep);
-    int x, y, z;
-    if (!class_site(p.c, p.colour, p.alpha, t - (long long)rep * per_rep, x, y, z)) continue;
-    plain_site<N, ST>(p.c, p.sub, p.alpha, rep, x, y, z, key);
-  }
+  for (int rep = blockIdx.y; rep < p.c.B; rep += gridDim.y) plain_site<N, ST>(p.c, p.sub, p.alpha, rep, x, y, z, key);
 }
 
 // Packed storage: a warp owns one (word, class site); lane j is replica 32 w + j. Each lane runs the int8 update
 // of its replica (same Philox counter), and the new word is assembled with a ballot.
+// Grid (ceil(rows * bx / 8), words), 8 warps per block.
 __global__ void __launch_bounds__(256) packed_class_kernel(const __grid_constant__ ClassParams p) {
   const Common& c = p.c;
   const Geometry& g = c.g;
   const int lane = threadIdx.x & 31;
-  const long long per_word = (long long)c.rows * c.bx;
-  const long long total = per_word * c.W;
+  const uint32_t per_word = (uint32_t)c.rows * (uint32_t)c.bx;
+  const uint32_t t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (t >= per_word) return;
+  int x, y, z;
+  if (!class_site(c, p.colour, p.alpha, t, x, y, z)) return;
+  const int own = p.alpha * g.plane + (z * g.L2 + y) * g.L1 + x;
+  if (g.has_mask && c.mask[own] == 0) return;
   const int32_t key = sweep_key(c.state);
   const uint32_t* src = (const uint32_t*)c.src;
   uint32_t* dst = (uint32_t*)c.dst;
-  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-  for (long long wi = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; wi < total; wi += nwarps) {
-    const int w = (int)(wi / per_word);
-    int x, y, z;
-    if (!class_site(c, p.colour, p.alpha, wi - (long long)w * per_word, x, y, z)) continue;
-    const int own = p.alpha * g.plane + (z * g.L2 + y) * g.L1 + x;
-    if (g.has_mask && c.mask[own] == 0) continue;
+  for (int w = blockIdx.y; w < c.W; w += gridDim.y) {
     const size_t wb = (size_t)w * g.nsite;
     const int s = (src[wb + own] >> lane) & 1u ? 1 : -1;
     int k = s > 0 ? 1 : 0;
@@ -236,10 +216,10 @@ __global__ void __launch_bounds__(256) packed_class_kernel(const __grid_constant
         for (; bi < p.sub.group_end[gi]; ++bi) {
           const BondDev bd = p.sub.bonds[bi];
           const int q = neighbour_index(g, bd, x, y, z);
-          int t = 0;
-          if (q >= 0 && (!g.has_mask || c.mask[q] != 0)) t = (src[wb + q] >> lane) & 1u ? 1 : -1;
-          G += t;
-          if (bd.extra >= 0) k += (t + 1) * p.sub.extra_stride[bd.extra];
+          int tv = 0;
+          if (q >= 0 && (!g.has_mask || c.mask[q] != 0)) tv = (src[wb + q] >> lane) & 1u ? 1 : -1;
+          G += tv;
+          if (bd.extra >= 0) k += (tv + 1) * p.sub.extra_stride[bd.extra];
         }
         k += (G + p.sub.group_z[gi]) * p.sub.key_stride[gi];
       }
@@ -320,41 +300,44 @@ __global__ void packed_sequential_kernel(const __grid_constant__ SeqParams p) {
 }
 
 // ---------------------------------------------------------------------------------------------- conversions
+// Grid (ceil(nsite / 256), words).
 __global__ void pack_kernel(const int8_t* __restrict__ spins, int32_t* __restrict__ words, int B, int W, int nsite) {
-  const long long total = (long long)W * nsite;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    const int w = (int)(t / nsite);
-    const int site = (int)(t - (long long)w * nsite);
+  const int site = blockIdx.x * blockDim.x + threadIdx.x;
+  if (site >= nsite) return;
+  for (int w = blockIdx.y; w < W; w += gridDim.y) {
     uint32_t word = 0;
     for (int j = 0; j < 32; ++j) {
       const int rep = w * 32 + j;
       if (rep < B && spins[(size_t)rep * nsite + site] > 0) word |= 1u << j;
     }
-    words[t] = (int32_t)word;
+    words[(size_t)w * nsite + site] = (int32_t)word;
   }
 }
 
+// Grid (ceil(nsite / 256), replicas).
 __global__ void unpack_kernel(const int32_t* __restrict__ words, const int8_t* __restrict__ mask,
                               int8_t* __restrict__ spins, int B, int nsite) {
-  const long long total = (long long)B * nsite;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    const int rep = (int)(t / nsite);
-    const int site = (int)(t - (long long)rep * nsite);
+  const int site = blockIdx.x * blockDim.x + threadIdx.x;
+  if (site >= nsite) return;
+  const bool present = mask == nullptr || mask[site] != 0;
+  for (int rep = blockIdx.y; rep < B; rep += gridDim.y) {
     const uint32_t word = (uint32_t)words[(size_t)(rep >> 5) * nsite + site];
     const int8_t v = (word >> (rep & 31)) & 1u ? 1 : -1;
-    spins[t] = (mask != nullptr && mask[site] == 0) ? 0 : v;
+    spins[(size_t)rep * nsite + site] = present ? v : 0;
   }
 }
 
 __global__ void advance_kernel(int64_t* state, int n) { state[1] += n; }
 
 // -------------------------------------------------------------------------------------------------- launch
-static int grid_for(long long total, int block) {
-  long long g = (total + block - 1) / block;
-  if (g > 148LL * 64) g = 148LL * 64;
-  return (int)(g < 1 ? 1 : g);
+static dim3 grid2(uint32_t per_unit, int per_block, int units) {
+  return dim3((per_unit + per_block - 1) / per_block, (unsigned)(units < 65535 ? units : 65535));
+}
+
+void set_rows(Common& c, int P, int bx) {
+  c.P = P;
+  c.bx = bx;
+  c.fd_bx = make_fastdiv((uint32_t)bx);
 }
 
 int launch_class(const sck_plan* plan, const Common& c, int colour, int alpha, cudaStream_t s) {
@@ -363,28 +346,24 @@ int launch_class(const sck_plan* plan, const Common& c, int colour, int alpha, c
   p.sub = plan->sub[alpha];
   p.colour = colour;
   p.alpha = alpha;
-  if (colour < 0) {
-    p.c.P = 1;
-    p.c.bx = c.g.L1;
-  }
-  const int block = 256;
-  const long long per = (long long)p.c.rows * p.c.bx;
+  if (colour < 0) set_rows(p.c, 1, c.g.L1);
+  const uint32_t per = (uint32_t)p.c.rows * (uint32_t)p.c.bx;
   if (plan->mode == SCK_MODE_PACKED) {
-    packed_class_kernel<<<grid_for(per * c.W * 32, block), block, 0, s>>>(p);
+    packed_class_kernel<<<grid2(per, 8, c.W), 256, 0, s>>>(p);
   } else {
-    const int grid = grid_for(per * c.B, block);
+    const dim3 grid = grid2(per, 256, c.B);
     switch (c.g.n) {
       case 1:
         if (plan->mode == SCK_MODE_INT8)
-          plain_class_kernel<1, int8_t><<<grid, block, 0, s>>>(p);
+          plain_class_kernel<1, int8_t><<<grid, 256, 0, s>>>(p);
         else
-          plain_class_kernel<1, float><<<grid, block, 0, s>>>(p);
+          plain_class_kernel<1, float><<<grid, 256, 0, s>>>(p);
         break;
       case 2:
-        plain_class_kernel<2, float><<<grid, block, 0, s>>>(p);
+        plain_class_kernel<2, float><<<grid, 256, 0, s>>>(p);
         break;
       default:
-        plain_class_kernel<3, float><<<grid, block, 0, s>>>(p);
+        plain_class_kernel<3, float><<<grid, 256, 0, s>>>(p);
         break;
     }
   }
@@ -423,14 +402,14 @@ int launch_sequential(const sck_plan* plan, const Common& c, cudaStream_t s) {
 }
 
 int launch_pack(const sck_plan* plan, const int8_t* spins, int32_t* words, cudaStream_t s) {
-  const long long total = (long long)plan->W * plan->geom.nsite;
-  pack_kernel<<<grid_for(total, 256), 256, 0, s>>>(spins, words, plan->batch, plan->W, plan->geom.nsite);
+  pack_kernel<<<grid2(plan->geom.nsite, 256, plan->W), 256, 0, s>>>(spins, words, plan->batch, plan->W,
+                                                                    plan->geom.nsite);
   return cuda_status(cudaGetLastError(), "pack");
 }
 
 int launch_unpack(const sck_plan* plan, const int32_t* words, const int8_t* mask, int8_t* spins, cudaStream_t s) {
-  const long long total = (long long)plan->batch * plan->geom.nsite;
-  unpack_kernel<<<grid_for(total, 256), 256, 0, s>>>(words, mask, spins, plan->batch, plan->geom.nsite);
+  unpack_kernel<<<grid2(plan->geom.nsite, 256, plan->batch), 256, 0, s>>>(words, mask, spins, plan->batch,
+                                                                         plan->geom.nsite);
   return cuda_status(cudaGetLastError(), "unpack");
 }
 

@@ -131,6 +131,17 @@ class Sampler:
         self._obs_ws = {}
         self._workspace(self.B)
 
+    def tune(self, specialised: bool = True, l2_budget: int = 72 << 20):
+        """Execution choices of sweep (specialised lattice kernels, L2 group-pipeline budget in bytes)."""
+        L.check(L.lib().sck_plan_tune(self._plan, int(bool(specialised)), int(l2_budget)))
+        return self.path()
+
+    def path(self) -> dict:
+        """The sweep path the plan will take: specialised table id (0 = generic), budget, pipeline group."""
+        sp, bud, grp = ctypes.c_int32(), ctypes.c_int64(), ctypes.c_int32()
+        L.check(L.lib().sck_plan_path(self._plan, ctypes.byref(sp), ctypes.byref(bud), ctypes.byref(grp)))
+        return {"specialised": sp.value, "l2_budget": bud.value, "group": grp.value}
+
     def __del__(self):
         h = getattr(self, "_plan", None)
         if h is not None and h.value:
