@@ -222,6 +222,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--L", type=int, default=64, help="heisenberg-bcc cells per axis (profiling runs use less)")
     ap.add_argument("--replicas", type=int, default=1536, help="heisenberg-bcc replicas")
+    ap.add_argument("--path", default="auto", choices=["auto", "classwise", "generic"],
+                    help="sweep path: autotuned (default), specialised class by class, or generic kernels")
+    ap.add_argument("--l2-mb", type=float, default=None, help="L2 budget of the group pipeline (MiB)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -241,6 +244,12 @@ def main():
     from spin_colour_kernel_b200 import build as bld
     bld.build()
     s, A, S, T, cfg = make_workload(args.workload, rank, device, args.L, args.replicas)
+    if args.path == "classwise":
+        A.tune(True, 0)
+    elif args.path == "generic":
+        A.tune(False, 0)
+    elif args.l2_mb is not None:
+        A.tune(True, int(args.l2_mb * (1 << 20)))
     attempts_per_step = A.B * s.n_active
     stream = torch.cuda.current_stream(device)
     classes = list(A.classes)
