@@ -20,18 +20,34 @@
 
 namespace sck {
 
-// Wrapped coordinates of one site for compile-time offsets -R..R on each axis.
-template <int R>
+// Wrapped coordinates of one site for compile-time offsets -R..R on each axis. PER: every axis of the box is
+// periodic (2D systems never offset along z) and each extent is at least R, so one conditional add or subtract
+// wraps an offset and no validity is tracked; otherwise open axes mark neighbours outside the box invalid.
+template <int R, bool PER>
 struct Around {
   int xo[2 * R + 1], yo[2 * R + 1], zo[2 * R + 1];
   bool xv[2 * R + 1], yv[2 * R + 1], zv[2 * R + 1];
 
+  __device__ __forceinline__ static int wrap1(int x, int d, int L) {
+    int q = x + d;
+    q += q < 0 ? L : 0;
+    q -= q >= L ? L : 0;
+    return q;
+  }
+
   __device__ __forceinline__ Around(const Geometry& g, int x, int y, int z) {
 #pragma unroll
     for (int d = -R; d <= R; ++d) {
-      const int qx = wrap_axis(x, d, g.L1, g.per[0]);
-      const int qy = wrap_axis(y, d, g.L2, g.per[1]);
-      const int qz = wrap_axis(z, d, g.L3, g.per[2]);
+      int qx, qy, qz;
+      if constexpr (PER) {
+        qx = wrap1(x, d, g.L1);
+        qy = wrap1(y, d, g.L2);
+        qz = g.dim == 3 ? wrap1(z, d, g.L3) : z;
+      } else {
+        qx = wrap_axis(x, d, g.L1, g.per[0]);
+        qy = wrap_axis(y, d, g.L2, g.per[1]);
+        qz = wrap_axis(z, d, g.L3, g.per[2]);
+      }
       xv[d + R] = qx >= 0;
       yv[d + R] = qy >= 0;
       zv[d + R] = qz >= 0;
@@ -43,7 +59,10 @@ struct Around {
   __device__ __forceinline__ int index(const Geometry& g, const BondC b) const {
     return b.a2 * g.plane + zo[b.dz + R] + yo[b.dy + R] + xo[b.dx + R];
   }
-  __device__ __forceinline__ bool valid(const BondC b) const { return xv[b.dx + R] && yv[b.dy + R] && zv[b.dz + R]; }
+  __device__ __forceinline__ bool valid(const BondC b) const {
+    if constexpr (PER) return true;
+    return xv[b.dx + R] && yv[b.dy + R] && zv[b.dz + R];
+  }
 };
 
 struct Task {
@@ -88,16 +107,15 @@ struct GroupRange {
 };
 
 // ---------------------------------------------------------------------------------------------------- Ising
-template <class Lat, int A, typename ST>
+template <class Lat, int A, typename ST, bool PER>
 __device__ __forceinline__ void ising_spec_site(const Common& c, int rep, int x, int y, int z, int32_t key) {
   const Geometry& g = c.g;
   const int own = A * g.plane + (z * g.L2 + y) * g.L1 + x;
   if (g.has_mask && c.mask[own] == 0) return;
-  const ST* src = (const ST*)c.src;
-  ST* dst = (ST*)c.dst;
-  const size_t base = (size_t)rep * g.nsite;
-  const int s = sgn(src[base + own]);
-  const Around<Lat::reach> nb(g, x, y, z);
+  const ST* src = (const ST*)c.src + (size_t)rep * g.nsite;
+  ST* dst = (ST*)c.dst + (size_t)rep * g.nsite;
+  const int s = sgn(src[own]);
+  const Around<Lat::reach, PER> nb(g, x, y, z);
   int k = s > 0 ? 1 : 0;
   int stride = 2;
   static_for<0, Lat::groups>([&](auto gc) {
@@ -105,7 +123,7 @@ __device__ __forceinline__ void ising_spec_site(const Common& c, int rep, int x,
     int G = 0;
     static_for<R::begin, R::end>([&](auto ic) {
       constexpr BondC bd = Lat::bond(A, decltype(ic)::value);
-      G += nb.valid(bd) ? sgn(src[base + nb.index(g, bd)]) : 0;
+      G += nb.valid(bd) ? sgn(src[nb.index(g, bd)]) : 0;
     });
     k += (G + (R::end - R::begin)) * stride;
     stride *= 2 * (R::end - R::begin) + 1;
@@ -114,7 +132,7 @@ __device__ __forceinline__ void ising_spec_site(const Common& c, int rep, int x,
   const Philox4 r = philox4x32_10(counter_of(rep, g.nsite, own), 0u, key_lo(key), key_hi(key));
   const float u0 = to_uniform(r.x0);
   const bool acc = g.acceptance == SCK_BARKER ? __fmul_rn(u0, __fadd_rn(1.0f, e)) < 1.0f : u0 < e;
-  if (acc) dst[base + own] = (ST)(-s);
+  if (acc) dst[own] = (ST)(-s);
 }
 
 // --------------------------------------------------------------------------------------------- vector models
@@ -129,22 +147,26 @@ __device__ __forceinline__ void sincos_2pi(float phi, float& sn, float& cs) {
 
 // Two replicas (lanes .x and .y) of one class site. `two` = false runs lane y as a copy of lane x and stores
 // lane x only (an odd replica count).
-template <class Lat, int A, int N>
+template <class Lat, int A, int N, bool PER>
 __device__ __forceinline__ void vec_spec_pair(const Common& c, const float (&J)[SCK_MAX_GROUPS], int rep0, bool two,
                                               int x, int y, int z, int32_t key) {
   const Geometry& g = c.g;
   const int own = A * g.plane + (z * g.L2 + y) * g.L1 + x;
   if (g.has_mask && c.mask[own] == 0) return;
-  const float* src = (const float*)c.src;
-  float* dst = (float*)c.dst;
+  // one base pointer for the pair: component k of replica rep0 + j sits at k * NS + j * RS (uniform offsets)
+  const float* base = (const float*)c.src + (size_t)rep0 * N * g.nsite;
+  float* obase = (float*)c.dst + (size_t)rep0 * N * g.nsite;
+  const size_t NS = (size_t)g.nsite, RS = two ? (size_t)N * g.nsite : 0;
   const int rep1 = two ? rep0 + 1 : rep0;
-  const size_t b0 = (size_t)rep0 * N * g.nsite, b1 = (size_t)rep1 * N * g.nsite;
-  const Around<Lat::reach> nb(g, x, y, z);
+  const Around<Lat::reach, PER> nb(g, x, y, z);
   float2 s[N], v[N];
+  {
+    const float* po = base + own;
 #pragma unroll
-  for (int k = 0; k < N; ++k) {
-    s[k] = make_float2(src[b0 + (size_t)k * g.nsite + own], src[b1 + (size_t)k * g.nsite + own]);
-    v[k] = f2(0.0f);
+    for (int k = 0; k < N; ++k) {
+      s[k] = make_float2(po[k * NS], po[k * NS + RS]);
+      v[k] = f2(0.0f);
+    }
   }
   static_for<0, Lat::groups>([&](auto gc) {
     constexpr int gi = decltype(gc)::value;
@@ -154,11 +176,11 @@ __device__ __forceinline__ void vec_spec_pair(const Common& c, const float (&J)[
     for (int k = 0; k < N; ++k) gs[k] = f2(0.0f);
     static_for<R::begin, R::end>([&](auto ic) {
       constexpr BondC bd = Lat::bond(A, decltype(ic)::value);
-      const int q = nb.index(g, bd);
+      const float* pq = base + nb.index(g, bd);
       const bool ok = nb.valid(bd);
 #pragma unroll
       for (int k = 0; k < N; ++k) {
-        const float2 t = ok ? make_float2(src[b0 + (size_t)k * g.nsite + q], src[b1 + (size_t)k * g.nsite + q]) : f2(0.0f);
+        const float2 t = ok ? make_float2(pq[k * NS], pq[k * NS + RS]) : f2(0.0f);
         gs[k] = __fadd2_rn(gs[k], t);
       }
     });
@@ -221,19 +243,20 @@ __device__ __forceinline__ void vec_spec_pair(const Common& c, const float (&J)[
     acc0 = u0.x < __expf(xm.x);
     acc1 = u0.y < __expf(xm.y);
   }
+  float* po = obase + own;
   if (acc0) {
 #pragma unroll
-    for (int k = 0; k < N; ++k) dst[b0 + (size_t)k * g.nsite + own] = t[k].x;
+    for (int k = 0; k < N; ++k) po[k * NS] = t[k].x;
   }
   if (two && acc1) {
 #pragma unroll
-    for (int k = 0; k < N; ++k) dst[b1 + (size_t)k * g.nsite + own] = t[k].y;
+    for (int k = 0; k < N; ++k) po[k * NS + RS] = t[k].y;
   }
 }
 
 // ------------------------------------------------------------------------------------------------- kernels
 // Grid (ceil(rows * bx / 256), n_tasks * units_per_task). Block y-slot -> (task, replica or replica pair).
-template <class Lat, int N, typename ST>
+template <class Lat, int N, typename ST, bool PER>
 __global__ void __launch_bounds__(256) spec_task_kernel(const __grid_constant__ SpecParams p) {
   const uint32_t per = (uint32_t)p.c.rows * (uint32_t)p.c.bx;
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -252,18 +275,18 @@ __global__ void __launch_bounds__(256) spec_task_kernel(const __grid_constant__ 
     if (a == task.alpha) {
       if constexpr (N == 1) {
         switch (a) {
-          case 0: ising_spec_site<Lat, 0, ST>(p.c, rep, x, y, z, key); break;
-          case 1: ising_spec_site<Lat, (Lat::b > 1 ? 1 : 0), ST>(p.c, rep, x, y, z, key); break;
-          case 2: ising_spec_site<Lat, (Lat::b > 2 ? 2 : 0), ST>(p.c, rep, x, y, z, key); break;
-          default: ising_spec_site<Lat, (Lat::b > 3 ? 3 : 0), ST>(p.c, rep, x, y, z, key); break;
+          case 0: ising_spec_site<Lat, 0, ST, PER>(p.c, rep, x, y, z, key); break;
+          case 1: ising_spec_site<Lat, (Lat::b > 1 ? 1 : 0), ST, PER>(p.c, rep, x, y, z, key); break;
+          case 2: ising_spec_site<Lat, (Lat::b > 2 ? 2 : 0), ST, PER>(p.c, rep, x, y, z, key); break;
+          default: ising_spec_site<Lat, (Lat::b > 3 ? 3 : 0), ST, PER>(p.c, rep, x, y, z, key); break;
         }
       } else {
         const bool two = rep + 1 < task.rep_end;
         switch (a) {
-          case 0: vec_spec_pair<Lat, 0, N>(p.c, p.J[0], rep, two, x, y, z, key); break;
-          case 1: vec_spec_pair<Lat, (Lat::b > 1 ? 1 : 0), N>(p.c, p.J[1], rep, two, x, y, z, key); break;
-          case 2: vec_spec_pair<Lat, (Lat::b > 2 ? 2 : 0), N>(p.c, p.J[2], rep, two, x, y, z, key); break;
-          default: vec_spec_pair<Lat, (Lat::b > 3 ? 3 : 0), N>(p.c, p.J[3], rep, two, x, y, z, key); break;
+          case 0: vec_spec_pair<Lat, 0, N, PER>(p.c, p.J[0], rep, two, x, y, z, key); break;
+          case 1: vec_spec_pair<Lat, (Lat::b > 1 ? 1 : 0), N, PER>(p.c, p.J[1], rep, two, x, y, z, key); break;
+          case 2: vec_spec_pair<Lat, (Lat::b > 2 ? 2 : 0), N, PER>(p.c, p.J[2], rep, two, x, y, z, key); break;
+          default: vec_spec_pair<Lat, (Lat::b > 3 ? 3 : 0), N, PER>(p.c, p.J[3], rep, two, x, y, z, key); break;
         }
       }
     }
@@ -301,18 +324,34 @@ int find_spec(const sck_plan* p) {
 }
 
 // ------------------------------------------------------------------------------------------- host: launches
-template <class Lat>
-static void launch_lat(const sck_plan* plan, const SpecParams& p, dim3 grid, cudaStream_t s) {
+template <class Lat, bool PER>
+static void launch_lat_per(const sck_plan* plan, const SpecParams& p, dim3 grid, cudaStream_t s) {
   if (plan->geom.n == 1) {
     if (plan->mode == SCK_MODE_INT8)
-      spec_task_kernel<Lat, 1, int8_t><<<grid, 256, 0, s>>>(p);
+      spec_task_kernel<Lat, 1, int8_t, PER><<<grid, 256, 0, s>>>(p);
     else
-      spec_task_kernel<Lat, 1, float><<<grid, 256, 0, s>>>(p);
+      spec_task_kernel<Lat, 1, float, PER><<<grid, 256, 0, s>>>(p);
   } else if (plan->geom.n == 2) {
-    spec_task_kernel<Lat, 2, float><<<grid, 256, 0, s>>>(p);
+    spec_task_kernel<Lat, 2, float, PER><<<grid, 256, 0, s>>>(p);
   } else {
-    spec_task_kernel<Lat, 3, float><<<grid, 256, 0, s>>>(p);
+    spec_task_kernel<Lat, 3, float, PER><<<grid, 256, 0, s>>>(p);
   }
+}
+
+// All axes periodic (2D: x and y) with every extent >= the bond reach: the branch-free wrap applies.
+template <class Lat>
+static bool periodic_box(const sck_plan* plan) {
+  const Geometry& g = plan->geom;
+  if (!g.per[0] || !g.per[1] || g.L1 < Lat::reach || g.L2 < Lat::reach) return false;
+  return g.dim == 2 || (g.per[2] && g.L3 >= Lat::reach);
+}
+
+template <class Lat>
+static void launch_lat(const sck_plan* plan, const SpecParams& p, dim3 grid, cudaStream_t s) {
+  if (periodic_box<Lat>(plan))
+    launch_lat_per<Lat, true>(plan, p, grid, s);
+  else
+    launch_lat_per<Lat, false>(plan, p, grid, s);
 }
 
 static int launch_tasks(const sck_plan* plan, SpecParams& p, cudaStream_t s) {

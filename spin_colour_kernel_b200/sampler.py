@@ -109,6 +109,8 @@ class Sampler:
         self.device = torch.device(device)
         if self.device.type != "cuda":
             raise RuntimeError("spin_colour_kernel_b200 runs on CUDA devices (B200) only; there is no CPU path")
+        if self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
         dev = self.device
         m = system.site_mask()
         self.mask_np = m
