@@ -222,8 +222,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--L", type=int, default=64, help="heisenberg-bcc cells per axis (profiling runs use less)")
     ap.add_argument("--replicas", type=int, default=1536, help="heisenberg-bcc replicas")
-    ap.add_argument("--path", default="auto", choices=["auto", "classwise", "generic"],
-                    help="sweep path: autotuned (default), specialised class by class, or generic kernels")
+    ap.add_argument("--path", default="auto", choices=["auto", "autotune", "classwise", "lattice", "generic"],
+                    help="sweep path: plan default, autotuned, row/lattice kernels class by class, lattice kernels "
+                         "only, or generic kernels")
     ap.add_argument("--l2-mb", type=float, default=None, help="L2 budget of the group pipeline (MiB)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -245,18 +246,26 @@ def main():
     bld.build()
     s, A, S, T, cfg = make_workload(args.workload, rank, device, args.L, args.replicas)
     if args.path == "classwise":
-        A.tune(True, 0)
+        A.tune(2, 0, 0)
+    elif args.path == "lattice":
+        A.tune(1, 0, 0)
     elif args.path == "generic":
-        A.tune(False, 0)
+        A.tune(0, 0, 0)
+    elif args.path == "autotune":
+        from spin_colour_kernel_b200.autotune import autotune
+        cfg["autotune"] = autotune(A, S, use_cache=False)
     elif args.l2_mb is not None:
-        A.tune(True, int(args.l2_mb * (1 << 20)))
+        A.tune(2, int(args.l2_mb * (1 << 20)), 0)
     attempts_per_step = A.B * s.n_active
     stream = torch.cuda.current_stream(device)
     classes = list(A.classes)
     path = A.path()
     C = len(classes)
     groups = -(-A.Bp // path["group"]) if path["group"] else 0
-    launches_per_sweep = (groups + C - 1) if groups else C * (-(-A.Bp // (65535 * (2 if s.n > 1 else 1))))
+    if path["resident"]:
+        launches_per_sweep = 1
+    else:
+        launches_per_sweep = (groups + C - 1) if groups else C * (-(-A.Bp // (65535 * (2 if s.n > 1 else 1))))
 
     for _ in range(args.warmup):
         A.sweep(S, 1)
@@ -326,7 +335,7 @@ def main():
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "note": f"algorithmic {bpa} B/attempt; peak {peak_kind}; kernel = "
-                             f"{'specialised' if path['specialised'] else 'generic'} class update, "
+                             f"{['generic', 'lattice', 'row'][path['specialised'] // 100]} class update, "
                              f"{launches_per_sweep} launches per sweep (L2 group {path['group']}), "
                              f"step times from CUDA events"},
         "e2e": {"value": e2e, "unit": "attempts/ns", "h2d_bytes_per_step": int(beta_h.numel() * 4),

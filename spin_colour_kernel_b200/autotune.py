@@ -49,11 +49,15 @@ def _store(d: dict) -> None:
         pass
 
 
+RESIDENT_LIMIT = 200 << 10
+
+
 def candidates(sampler):
-    out = [(False, 0)]
-    spec = sampler.tune(True, 0)["specialised"] > 0
-    if spec:
-        out += [(True, mb << 20) for mb in CANDIDATE_BUDGETS_MB]
+    """(specialised, l2_budget, resident_limit) triples worth timing for this sampler."""
+    out = [(0, 0, 0), (0, 0, RESIDENT_LIMIT)]
+    kind = sampler.tune(2, 0, 0)["specialised"] // 100
+    for level in range(1, kind + 1):
+        out += [(level, mb << 20, 0) for mb in CANDIDATE_BUDGETS_MB]
     return out
 
 
@@ -63,15 +67,15 @@ def autotune(sampler, S: torch.Tensor, sweeps: int = 3, use_cache: bool = True) 
     cache = _load() if use_cache else {}
     if key in cache:
         c = cache[key]
-        sampler.tune(c["specialised"] > 0, c["l2_budget"])
+        sampler.tune(c["specialised"] > 0, c["l2_budget"], c["resident_limit"])
         return dict(c, cached=True)
     saved = sampler.state.clone()
     work = S.clone()
     results = []
     seen = set()
-    for spec, budget in candidates(sampler):
-        p = sampler.tune(spec, budget)
-        sig = (p["specialised"], p["group"])
+    for spec, budget, resident in candidates(sampler):
+        p = sampler.tune(spec, budget, resident)
+        sig = (p["specialised"], p["group"], p["resident"])
         if sig in seen:
             continue
         seen.add(sig)
@@ -82,13 +86,15 @@ def autotune(sampler, S: torch.Tensor, sweeps: int = 3, use_cache: bool = True) 
         sampler.sweep(work, sweeps)
         b.record(stream)
         torch.cuda.synchronize(sampler.device)
-        results.append((a.elapsed_time(b) / sweeps, spec, budget, p))
+        results.append((a.elapsed_time(b) / sweeps, spec, budget, resident, p))
     sampler.state.copy_(saved)
     del work
-    ms, spec, budget, p = min(results, key=lambda r: r[0])
-    sampler.tune(spec, budget)
-    choice = {"specialised": p["specialised"], "l2_budget": budget, "group": p["group"], "ms_per_sweep": ms,
-              "tried": [{"specialised": r[3]["specialised"], "group": r[3]["group"], "ms": r[0]} for r in results]}
+    ms, spec, budget, resident, p = min(results, key=lambda r: r[0])
+    sampler.tune(spec, budget, resident)
+    choice = {"specialised": p["specialised"], "l2_budget": budget, "resident_limit": resident, "group": p["group"],
+              "resident": p["resident"], "ms_per_sweep": ms,
+              "tried": [{"specialised": r[4]["specialised"], "group": r[4]["group"], "resident": r[4]["resident"],
+                         "ms": r[0]} for r in results]}
     if use_cache:
         cache[key] = choice
         _store(cache)

@@ -5,6 +5,7 @@
 #include <string>
 
 #include "internal.h"
+#include "spec.cuh"
 
 namespace sck {
 
@@ -69,6 +70,15 @@ static Common make_common(const sck_plan* plan, const sck_buffers* buf, const vo
 }
 
 static bool is_bitwise(int mode) { return mode == SCK_MODE_BITWISE || mode == SCK_MODE_BITWISE_INDEP; }
+
+constexpr long long kResidentDefault = 200ll << 10;
+constexpr long long kResidentMax = 220ll << 10;
+
+// Whole sweeps in shared memory: int8 / float32 storage and a replica within the resident limit.
+static bool use_resident(const sck_plan* p) {
+  if (p->mode != SCK_MODE_INT8 && p->mode != SCK_MODE_F32) return false;
+  return p->resident_limit > 0 && (long long)resident_bytes(p) <= p->resident_limit;
+}
 
 // Replicas per group of the L2 pipeline, or 0 when the sweep runs class by class over all replicas: the
 // specialised kernels only, a state larger than the budget, at least as many groups as classes.
@@ -330,23 +340,31 @@ int sck_plan_create(const sck_system_desc* d, int32_t batch, int32_t mode, sck_p
   p->NP = np < 1 ? 1 : np;
   p->field = (d->n == 1 && d->h64[0] != 0.0) ? 1 : 0;
   p->spec = find_spec(p);
+  p->row_kernels = 1;
   p->l2_budget = 72ll << 20;
+  p->resident_limit = kResidentDefault;
   *out = p;
   return SCK_OK;
 }
 
-int sck_plan_tune(sck_plan* plan, int32_t specialised, int64_t l2_budget_bytes) {
-  if (plan == nullptr || l2_budget_bytes < 0) return fail(SCK_ERR_INVALID, "null plan or negative budget");
+int sck_plan_tune(sck_plan* plan, int32_t specialised, int64_t l2_budget_bytes, int64_t resident_limit_bytes) {
+  if (plan == nullptr || l2_budget_bytes < 0 || resident_limit_bytes < 0)
+    return fail(SCK_ERR_INVALID, "null plan or negative budget");
+  if (resident_limit_bytes > kResidentMax) return fail(SCK_ERR_INVALID, "resident limit above 220 KiB of shared memory");
   plan->spec = specialised ? find_spec(plan) : 0;
+  plan->row_kernels = specialised >= 2 ? 1 : 0;
   plan->l2_budget = l2_budget_bytes;
+  plan->resident_limit = resident_limit_bytes;
   return SCK_OK;
 }
 
-int sck_plan_path(const sck_plan* plan, int32_t* specialised, int64_t* l2_budget_bytes, int32_t* group) {
+int sck_plan_path(const sck_plan* plan, int32_t* specialised, int64_t* l2_budget_bytes, int32_t* group,
+                  int32_t* resident) {
   if (plan == nullptr) return fail(SCK_ERR_INVALID, "null plan");
-  if (specialised) *specialised = plan->spec;
+  if (specialised) *specialised = plan->spec ? (row_kernel_ok(plan) ? 2 : 1) * 100 + plan->spec : 0;
   if (l2_budget_bytes) *l2_budget_bytes = plan->l2_budget;
   if (group) *group = pipeline_group(plan);
+  if (resident) *resident = use_resident(plan) ? 1 : 0;
   return SCK_OK;
 }
 
@@ -402,6 +420,12 @@ int sck_sweep(const sck_plan* plan, const sck_buffers* buf, int32_t n_sweeps, vo
   if (n_sweeps < 0) return fail(SCK_ERR_INVALID, "negative sweep count");
   cudaStream_t s = (cudaStream_t)stream;
   if (n_sweeps == 0) return SCK_OK;
+  if (use_resident(plan)) {
+    const Common c = make_common(plan, buf, buf->spins);
+    rc = launch_resident(plan, c, n_sweeps, s);
+    if (rc != SCK_OK) return rc;
+    return launch_advance(buf->state, n_sweeps, s);
+  }
   if (plan->spec) {
     const Common c = make_common(plan, buf, buf->spins);
     const int group = pipeline_group(plan);

@@ -114,6 +114,12 @@ __device__ __forceinline__ int32_t sweep_key(const int64_t* state) {
   return (int32_t)(sv % 2147483629ll);
 }
 
+// The key of sweep state[1] + offset (kernels that run several sweeps of one call).
+__device__ __forceinline__ int32_t sweep_key_at(const int64_t* state, int offset) {
+  const uint64_t v = (uint64_t)state[0] * 1000003ull + (uint64_t)(state[1] + offset) * 7919ull + 12345ull;
+  return (int32_t)((int64_t)v % 2147483629ll);
+}
+
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11) with counter (c0, c1, 0, 0) and key (k0, k1): the
 // generator of Triton's randint4x. Each round multiplies c0 and c2 by the round constants, keeps the low
 // halves and mixes the high halves with the other words and the key; the key steps by the Weyl constants.

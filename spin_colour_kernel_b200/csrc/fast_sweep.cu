@@ -6,17 +6,15 @@
 // one add and one load per component. Ising keeps the integer key and the host table (bit-exact); vector models
 // run two replicas per thread in packed float32x2 arithmetic (add.rn.f32x2 / mul.rn.f32x2, round-to-nearest
 // per lane, same operation order as the generic kernel), with proposal trigonometry and exp on the SFU
-// (__sinf / __cosf on [-pi, pi], __expf): per-spin differences from the reference stay ~1e-6.
+// (__sinf / __cosf on [-pi, pi], __expf): per-spin differences from the reference stay ~1e-6. Lattices whose
+// classes alternate along x run the row kernels of rowpair.cu instead when their box allows it.
 //
 // Group pipeline. A sweep visits its C classes in order, and each class launch reads the whole state. When the
 // state is larger than L2, the replicas are cut into groups whose C-group working set fits in L2, and launch k
 // runs class c on group k - c for every c at once (a diagonal over (group, class)): the C launches that touch a
 // group run back to back, so after its first read from HBM a group stays in L2 until its sweep is done. Each
 // replica's chain is unchanged: its classes still run in order, one launch after another.
-#include <type_traits>
-
-#include "internal.h"
-#include "lattices.h"
+#include "spec.cuh"
 
 namespace sck {
 
@@ -65,47 +63,6 @@ struct Around {
   }
 };
 
-struct Task {
-  int colour, alpha, rep_begin, rep_end, sweep_offset;
-};
-
-constexpr int kMaxTasks = 8;
-
-struct SpecParams {
-  Common c;
-  float J[SCK_MAX_BASIS][SCK_MAX_GROUPS];
-  int n_tasks;
-  int units_per_task;     // grid.y slots per task (replicas, or replica pairs for vector models)
-  Task tasks[kMaxTasks];
-};
-
-__device__ __forceinline__ int32_t sweep_key_at(const int64_t* state, int offset) {
-  const uint64_t v = (uint64_t)state[0] * 1000003ull + (uint64_t)(state[1] + offset) * 7919ull + 12345ull;
-  return (int32_t)((int64_t)v % 2147483629ll);
-}
-
-__device__ __forceinline__ uint32_t counter_of(int rep, int nsite, int own) {
-  return (uint32_t)((unsigned long long)rep * (unsigned long long)nsite + (unsigned long long)own);
-}
-
-template <typename T>
-__device__ __forceinline__ int sgn(T v) { return (v > T(0)) - (v < T(0)); }
-
-// Compile-time loop: f(std::integral_constant<int, I>) for I in [B, E).
-template <int I, int E, class F>
-__device__ __forceinline__ void static_for(F&& f) {
-  if constexpr (I < E) {
-    f(std::integral_constant<int, I>{});
-    static_for<I + 1, E>(f);
-  }
-}
-
-template <class Lat, int A, int G>
-struct GroupRange {
-  static constexpr int begin = G == 0 ? 0 : Lat::group_end(A, G - 1);
-  static constexpr int end = Lat::group_end(A, G);
-};
-
 // ---------------------------------------------------------------------------------------------------- Ising
 template <class Lat, int A, typename ST, bool PER>
 __device__ __forceinline__ void ising_spec_site(const Common& c, int rep, int x, int y, int z, int32_t key) {
@@ -136,15 +93,6 @@ __device__ __forceinline__ void ising_spec_site(const Common& c, int rep, int x,
 }
 
 // --------------------------------------------------------------------------------------------- vector models
-__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
-
-// sin and cos of phi in [0, 2 pi] through the SFU on the reduced range [-pi, pi].
-__device__ __forceinline__ void sincos_2pi(float phi, float& sn, float& cs) {
-  const float red = phi - 3.14159265358979f;
-  sn = -__sinf(red);
-  cs = -__cosf(red);
-}
-
 // Two replicas (lanes .x and .y) of one class site. `two` = false runs lane y as a copy of lane x and stores
 // lane x only (an odd replica count).
 template <class Lat, int A, int N, bool PER>
@@ -190,59 +138,9 @@ __device__ __forceinline__ void vec_spec_pair(const Common& c, const float (&J)[
 #pragma unroll
   for (int k = 0; k < N; ++k)
     if (c.hnz[k]) v[k] = __fadd2_rn(v[k], f2(c.h[k]));
-
-  const Philox4 ra = philox4x32_10(counter_of(rep0, g.nsite, own), 0u, key_lo(key), key_hi(key));
-  const Philox4 rb = two ? philox4x32_10(counter_of(rep1, g.nsite, own), 0u, key_lo(key), key_hi(key)) : ra;
-  const float2 u0 = make_float2(to_uniform(ra.x0), to_uniform(rb.x0));
-  const float TWO_PI = 6.2831855f;
   float2 t[N];
-  if constexpr (N == 2) {
-    float sa, ca, sb, cb;
-    sincos_2pi(__fmul_rn(TWO_PI, to_uniform(ra.x1)), sa, ca);
-    sincos_2pi(__fmul_rn(TWO_PI, to_uniform(rb.x1)), sb, cb);
-    t[0] = make_float2(ca, cb);
-    t[1] = make_float2(sa, sb);
-  } else {
-    const float2 u1 = make_float2(to_uniform(ra.x1), to_uniform(rb.x1));
-    const float2 cz = __fadd2_rn(__fmul2_rn(f2(2.0f), u1), f2(-1.0f));
-    float sa, ca, sb, cb;
-    sincos_2pi(__fmul_rn(TWO_PI, to_uniform(ra.x2)), sa, ca);
-    sincos_2pi(__fmul_rn(TWO_PI, to_uniform(rb.x2)), sb, cb);
-    const float2 w = __fadd2_rn(f2(1.0f), __fmul2_rn(f2(-1.0f), __fmul2_rn(cz, cz)));
-    const float2 rr = make_float2(sqrtf(fmaxf(w.x, 0.0f)), sqrtf(fmaxf(w.y, 0.0f)));
-    t[0] = __fmul2_rn(rr, make_float2(ca, cb));
-    t[1] = __fmul2_rn(rr, make_float2(sa, sb));
-    t[2] = cz;
-  }
-  const float2 m1 = f2(-1.0f);
-  float2 d = __fmul2_rn(__fadd2_rn(t[0], __fmul2_rn(m1, s[0])), v[0]);
-#pragma unroll
-  for (int k = 1; k < N; ++k) d = __fadd2_rn(d, __fmul2_rn(__fadd2_rn(t[k], __fmul2_rn(m1, s[k])), v[k]));
-  float2 dE = __fmul2_rn(m1, d);
-  if constexpr (N == 3) {
-    if (g.has_cubic) {
-      const float2 k1 = f2(c.k1[own]);
-      const float2 k2 = f2(c.k2);
-      auto aniso = [&](const float2* p) {
-        const float2 q01 = __fmul2_rn(p[0], p[1]), q02 = __fmul2_rn(p[0], p[2]), q12 = __fmul2_rn(p[1], p[2]);
-        const float2 tri = __fmul2_rn(q01, p[2]);
-        const float2 quad = __fadd2_rn(__fadd2_rn(__fmul2_rn(q01, q01), __fmul2_rn(q02, q02)), __fmul2_rn(q12, q12));
-        return __fadd2_rn(__fmul2_rn(k1, quad), __fmul2_rn(__fmul2_rn(k2, tri), tri));
-      };
-      dE = __fadd2_rn(dE, __fadd2_rn(aniso(t), __fmul2_rn(m1, aniso(s))));
-    }
-  }
-  const float2 beta = make_float2(c.beta[rep0], c.beta[rep1]);
   bool acc0, acc1;
-  if (g.acceptance == SCK_BARKER) {
-    const float2 xb = __fmul2_rn(beta, dE);
-    acc0 = __fmul_rn(u0.x, __fadd_rn(1.0f, __expf(xb.x))) < 1.0f;
-    acc1 = __fmul_rn(u0.y, __fadd_rn(1.0f, __expf(xb.y))) < 1.0f;
-  } else {
-    const float2 xm = __fmul2_rn(__fmul2_rn(m1, beta), dE);
-    acc0 = u0.x < __expf(xm.x);
-    acc1 = u0.y < __expf(xm.y);
-  }
+  finish_pair<N>(c, own, rep0, rep1, two, key, s, v, t, acc0, acc1);
   float* po = obase + own;
   if (acc0) {
 #pragma unroll
@@ -270,27 +168,15 @@ __global__ void __launch_bounds__(256) spec_task_kernel(const __grid_constant__ 
   int x, y, z;
   if (!class_site(p.c, task.colour, task.alpha, t, x, y, z)) return;
   const int32_t key = sweep_key_at(p.c.state, task.sweep_offset);
-#pragma unroll
-  for (int a = 0; a < Lat::b; ++a) {
-    if (a == task.alpha) {
-      if constexpr (N == 1) {
-        switch (a) {
-          case 0: ising_spec_site<Lat, 0, ST, PER>(p.c, rep, x, y, z, key); break;
-          case 1: ising_spec_site<Lat, (Lat::b > 1 ? 1 : 0), ST, PER>(p.c, rep, x, y, z, key); break;
-          case 2: ising_spec_site<Lat, (Lat::b > 2 ? 2 : 0), ST, PER>(p.c, rep, x, y, z, key); break;
-          default: ising_spec_site<Lat, (Lat::b > 3 ? 3 : 0), ST, PER>(p.c, rep, x, y, z, key); break;
-        }
-      } else {
-        const bool two = rep + 1 < task.rep_end;
-        switch (a) {
-          case 0: vec_spec_pair<Lat, 0, N, PER>(p.c, p.J[0], rep, two, x, y, z, key); break;
-          case 1: vec_spec_pair<Lat, (Lat::b > 1 ? 1 : 0), N, PER>(p.c, p.J[1], rep, two, x, y, z, key); break;
-          case 2: vec_spec_pair<Lat, (Lat::b > 2 ? 2 : 0), N, PER>(p.c, p.J[2], rep, two, x, y, z, key); break;
-          default: vec_spec_pair<Lat, (Lat::b > 3 ? 3 : 0), N, PER>(p.c, p.J[3], rep, two, x, y, z, key); break;
-        }
-      }
+  static_for<0, Lat::b>([&](auto ac) {
+    constexpr int a = decltype(ac)::value;
+    if (a != task.alpha) return;
+    if constexpr (N == 1) {
+      ising_spec_site<Lat, a, ST, PER>(p.c, rep, x, y, z, key);
+    } else {
+      vec_spec_pair<Lat, a, N, PER>(p.c, p.J[a], rep, rep + 1 < task.rep_end, x, y, z, key);
     }
-  }
+  });
 }
 
 // ------------------------------------------------------------------------------------------ host: matching
@@ -355,7 +241,6 @@ static void launch_lat(const sck_plan* plan, const SpecParams& p, dim3 grid, cud
 }
 
 static int launch_tasks(const sck_plan* plan, SpecParams& p, cudaStream_t s) {
-  const uint32_t per = (uint32_t)p.c.rows * (uint32_t)p.c.bx;
   const int per_unit = plan->geom.n == 1 ? 1 : 2;
   int most = 1;
   for (int i = 0; i < p.n_tasks; ++i) {
@@ -365,6 +250,8 @@ static int launch_tasks(const sck_plan* plan, SpecParams& p, cudaStream_t s) {
   p.units_per_task = (most + per_unit - 1) / per_unit;
   const long long ys = (long long)p.units_per_task * p.n_tasks;
   if (ys > 65535) return cuda_status(cudaErrorInvalidConfiguration, "task launch: too many replicas per launch");
+  if (row_kernel_ok(plan)) return launch_row_tasks(plan, p, (int)ys, s);
+  const uint32_t per = (uint32_t)p.c.rows * (uint32_t)p.c.bx;
   const dim3 grid((per + 255) / 256, (unsigned)ys);
   switch (plan->spec) {
     case Lat_square_1::id: launch_lat<Lat_square_1>(plan, p, grid, s); break;
@@ -383,6 +270,7 @@ static SpecParams spec_params(const sck_plan* plan, const Common& c) {
   p.c = c;
   for (int a = 0; a < SCK_MAX_BASIS; ++a)
     for (int gi = 0; gi < SCK_MAX_GROUPS; ++gi) p.J[a][gi] = plan->sub[a].J[gi];
+  p.segs_per_row = plan->geom.L1 / 64;
   return p;
 }
 

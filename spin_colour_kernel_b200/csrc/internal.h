@@ -118,7 +118,9 @@ struct sck_plan {
   int Z, Z1, NP, field;
   int ising_lut;   // Ising chain with the host-built exp table (INT8, F32 with n = 1, PACKED)
   int spec;        // id of the matching compile-time lattice table (lattices.h), 0 = generic kernels
+  int row_kernels; // row kernels (rowpair.cu) allowed for eligible specialised systems
   long long l2_budget;  // bytes of L2 the group pipeline may fill
+  long long resident_limit;  // largest replica (bytes) whose sweeps run resident in shared memory; 0 = never
 };
 
 namespace sck {
@@ -138,6 +140,8 @@ int launch_pack(const sck_plan* plan, const int8_t* spins, int32_t* words, cudaS
 int launch_unpack(const sck_plan* plan, const int32_t* words, const int8_t* mask, int8_t* spins, cudaStream_t s);
 int launch_advance(int64_t* state, int n, cudaStream_t s);
 int find_spec(const sck_plan* plan);
+size_t resident_bytes(const sck_plan* plan);
+int launch_resident(const sck_plan* plan, const Common& c, int n_sweeps, cudaStream_t s);
 int launch_spec_class(const sck_plan* plan, const Common& c, int colour, int alpha, cudaStream_t s);
 int launch_spec_pipeline(const sck_plan* plan, const Common& c, int n_sweeps, int group, cudaStream_t s);
 }  // namespace sck

@@ -1,0 +1,124 @@
+// Shared pieces of the specialised class kernels (fast_sweep.cu, rowpair.cu): task lists of the L2 group
+// pipeline, compile-time loops over the lattice tables, and the second half of a vector-model update (proposal,
+// energy change, anisotropy, acceptance) for two replicas in packed float32x2 arithmetic.
+#pragma once
+
+#include <type_traits>
+
+#include "internal.h"
+#include "lattices.h"
+
+namespace sck {
+
+struct Task {
+  int colour, alpha, rep_begin, rep_end, sweep_offset;
+};
+
+constexpr int kMaxTasks = 8;
+
+struct SpecParams {
+  Common c;
+  float J[SCK_MAX_BASIS][SCK_MAX_GROUPS];
+  int n_tasks;
+  int units_per_task;     // grid.y slots per task (replicas, or replica pairs for vector models)
+  int segs_per_row;       // row kernels: 64-cell segments per row
+  Task tasks[kMaxTasks];
+};
+
+__device__ __forceinline__ uint32_t counter_of(int rep, int nsite, int own) {
+  return (uint32_t)((unsigned long long)rep * (unsigned long long)nsite + (unsigned long long)own);
+}
+
+template <typename T>
+__device__ __forceinline__ int sgn(T v) { return (v > T(0)) - (v < T(0)); }
+
+// Compile-time loop: f(std::integral_constant<int, I>) for I in [B, E).
+template <int I, int E, class F>
+__device__ __forceinline__ void static_for(F&& f) {
+  if constexpr (I < E) {
+    f(std::integral_constant<int, I>{});
+    static_for<I + 1, E>(f);
+  }
+}
+
+template <class Lat, int A, int G>
+struct GroupRange {
+  static constexpr int begin = G == 0 ? 0 : Lat::group_end(A, G - 1);
+  static constexpr int end = Lat::group_end(A, G);
+};
+
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+
+// sin and cos of phi in [0, 2 pi] through the SFU on the reduced range [-pi, pi].
+__device__ __forceinline__ void sincos_2pi(float phi, float& sn, float& cs) {
+  const float red = phi - 3.14159265358979f;
+  sn = -__sinf(red);
+  cs = -__cosf(red);
+}
+
+// Proposal, energy change with cubic anisotropy, and Metropolis / Barker decision of two replicas (lane .x =
+// rep0, lane .y = rep1) of site `own`, given their spins s and local fields v (field included). Returns the
+// proposals in t and the decisions in acc0 / acc1. Same operation order as the reference's kernel
+// (generator.py:275-305); packed float32x2 operations round each lane to nearest.
+template <int N>
+__device__ __forceinline__ void finish_pair(const Common& c, int own, int rep0, int rep1, bool two, int32_t key,
+                                            const float2 (&s)[N], const float2 (&v)[N], float2 (&t)[N], bool& acc0,
+                                            bool& acc1) {
+  const Geometry& g = c.g;
+  const Philox4 ra = philox4x32_10(counter_of(rep0, g.nsite, own), 0u, key_lo(key), key_hi(key));
+  const Philox4 rb = two ? philox4x32_10(counter_of(rep1, g.nsite, own), 0u, key_lo(key), key_hi(key)) : ra;
+  const float2 u0 = make_float2(to_uniform(ra.x0), to_uniform(rb.x0));
+  const float TWO_PI = 6.2831855f;
+  if constexpr (N == 2) {
+    float sa, ca, sb, cb;
+    sincos_2pi(__fmul_rn(TWO_PI, to_uniform(ra.x1)), sa, ca);
+    sincos_2pi(__fmul_rn(TWO_PI, to_uniform(rb.x1)), sb, cb);
+    t[0] = make_float2(ca, cb);
+    t[1] = make_float2(sa, sb);
+  } else {
+    const float2 u1 = make_float2(to_uniform(ra.x1), to_uniform(rb.x1));
+    const float2 cz = __fadd2_rn(__fmul2_rn(f2(2.0f), u1), f2(-1.0f));
+    float sa, ca, sb, cb;
+    sincos_2pi(__fmul_rn(TWO_PI, to_uniform(ra.x2)), sa, ca);
+    sincos_2pi(__fmul_rn(TWO_PI, to_uniform(rb.x2)), sb, cb);
+    const float2 w = __fadd2_rn(f2(1.0f), __fmul2_rn(f2(-1.0f), __fmul2_rn(cz, cz)));
+    const float2 rr = make_float2(sqrtf(fmaxf(w.x, 0.0f)), sqrtf(fmaxf(w.y, 0.0f)));
+    t[0] = __fmul2_rn(rr, make_float2(ca, cb));
+    t[1] = __fmul2_rn(rr, make_float2(sa, sb));
+    t[2] = cz;
+  }
+  const float2 m1 = f2(-1.0f);
+  float2 d = __fmul2_rn(__fadd2_rn(t[0], __fmul2_rn(m1, s[0])), v[0]);
+#pragma unroll
+  for (int k = 1; k < N; ++k) d = __fadd2_rn(d, __fmul2_rn(__fadd2_rn(t[k], __fmul2_rn(m1, s[k])), v[k]));
+  float2 dE = __fmul2_rn(m1, d);
+  if constexpr (N == 3) {
+    if (g.has_cubic) {
+      const float2 k1 = f2(c.k1[own]);
+      const float2 k2 = f2(c.k2);
+      auto aniso = [&](const float2* p) {
+        const float2 q01 = __fmul2_rn(p[0], p[1]), q02 = __fmul2_rn(p[0], p[2]), q12 = __fmul2_rn(p[1], p[2]);
+        const float2 tri = __fmul2_rn(q01, p[2]);
+        const float2 quad = __fadd2_rn(__fadd2_rn(__fmul2_rn(q01, q01), __fmul2_rn(q02, q02)), __fmul2_rn(q12, q12));
+        return __fadd2_rn(__fmul2_rn(k1, quad), __fmul2_rn(__fmul2_rn(k2, tri), tri));
+      };
+      dE = __fadd2_rn(dE, __fadd2_rn(aniso(t), __fmul2_rn(m1, aniso(s))));
+    }
+  }
+  const float2 beta = make_float2(c.beta[rep0], c.beta[rep1]);
+  if (g.acceptance == SCK_BARKER) {
+    const float2 xb = __fmul2_rn(beta, dE);
+    acc0 = __fmul_rn(u0.x, __fadd_rn(1.0f, __expf(xb.x))) < 1.0f;
+    acc1 = __fmul_rn(u0.y, __fadd_rn(1.0f, __expf(xb.y))) < 1.0f;
+  } else {
+    const float2 xm = __fmul2_rn(__fmul2_rn(m1, beta), dE);
+    acc0 = u0.x < __expf(xm.x);
+    acc1 = u0.y < __expf(xm.y);
+  }
+}
+
+// Row kernels (rowpair.cu): eligibility and the task launch.
+bool row_kernel_ok(const sck_plan* plan);
+int launch_row_tasks(const sck_plan* plan, const SpecParams& p, int ys, cudaStream_t s);
+
+}  // namespace sck

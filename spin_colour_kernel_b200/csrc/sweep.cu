@@ -25,14 +25,15 @@ __device__ __forceinline__ uint32_t counter32(long long rep, int nsite, int own)
 template <typename T>
 __device__ __forceinline__ int spin_sign(T v) { return (v > T(0)) - (v < T(0)); }
 
+// src / dst point at replica `rep`'s block (global memory, or shared memory in the resident kernel); rep only
+// selects the random stream and the table row.
 template <typename ST>
 __device__ __forceinline__ void ising_site(const Common& c, const SubDev& sub, int alpha, int rep, int x, int y,
                                            int z, int32_t key, const ST* src, ST* dst) {
   const Geometry& g = c.g;
   const int own = alpha * g.plane + (z * g.L2 + y) * g.L1 + x;
   if (g.has_mask && c.mask[own] == 0) return;
-  const size_t base = (size_t)rep * g.nsite;
-  const int s = spin_sign(src[base + own]);
+  const int s = spin_sign(src[own]);
   int k = s > 0 ? 1 : 0;
   int bi = 0;
 #pragma unroll
@@ -42,7 +43,7 @@ __device__ __forceinline__ void ising_site(const Common& c, const SubDev& sub, i
       for (; bi < sub.group_end[gi]; ++bi) {
         const BondDev bd = sub.bonds[bi];
         const int q = neighbour_index(g, bd, x, y, z);
-        const int t = q >= 0 ? spin_sign(src[base + q]) : 0;
+        const int t = q >= 0 ? spin_sign(src[q]) : 0;
         G += t;
         if (bd.extra >= 0) k += (t + 1) * sub.extra_stride[bd.extra];
       }
@@ -54,9 +55,9 @@ __device__ __forceinline__ void ising_site(const Common& c, const SubDev& sub, i
   const float u0 = to_uniform(r.x0);
   const bool acc = g.acceptance == SCK_BARKER ? __fmul_rn(u0, __fadd_rn(1.0f, e)) < 1.0f : u0 < e;
   if (acc)
-    dst[base + own] = (ST)(-s);
+    dst[own] = (ST)(-s);
   else if ((const void*)src != (const void*)dst)
-    dst[base + own] = (ST)s;
+    dst[own] = (ST)s;
 }
 
 // ------------------------------------------------------------------------------------------- vector models
@@ -66,11 +67,11 @@ __device__ __forceinline__ void vec_site(const Common& c, const SubDev& sub, int
   const Geometry& g = c.g;
   const int own = alpha * g.plane + (z * g.L2 + y) * g.L1 + x;
   if (g.has_mask && c.mask[own] == 0) return;
-  const size_t base = (size_t)rep * N * g.nsite;
+  const int NS = g.nsite;
   float s[N], v[N];
 #pragma unroll
   for (int k = 0; k < N; ++k) {
-    s[k] = src[base + (size_t)k * g.nsite + own];
+    s[k] = src[k * NS + own];
     v[k] = 0.0f;
   }
   float ex[SCK_MAX_EXTRA][N];
@@ -86,7 +87,7 @@ __device__ __forceinline__ void vec_site(const Common& c, const SubDev& sub, int
         const int q = neighbour_index(g, bd, x, y, z);
 #pragma unroll
         for (int k = 0; k < N; ++k) {
-          const float t = q >= 0 ? src[base + (size_t)k * g.nsite + q] : 0.0f;
+          const float t = q >= 0 ? src[k * NS + q] : 0.0f;
           gs[k] = __fadd_rn(gs[k], t);
           if (bd.extra >= 0) ex[bd.extra][k] = t;
         }
@@ -160,7 +161,7 @@ __device__ __forceinline__ void vec_site(const Common& c, const SubDev& sub, int
     acc = u0 < expf(__fmul_rn(-beta, dE));
   if (acc || (const void*)src != (const void*)dst) {
 #pragma unroll
-    for (int k = 0; k < N; ++k) dst[base + (size_t)k * g.nsite + own] = acc ? t[k] : s[k];
+    for (int k = 0; k < N; ++k) dst[k * NS + own] = acc ? t[k] : s[k];
   }
 }
 
@@ -168,10 +169,11 @@ __device__ __forceinline__ void vec_site(const Common& c, const SubDev& sub, int
 template <int N, typename ST>
 __device__ __forceinline__ void plain_site(const Common& c, const SubDev& sub, int alpha, int rep, int x, int y,
                                            int z, int32_t key) {
+  const size_t base = (size_t)rep * N * c.g.nsite;
   if constexpr (N == 1) {
-    ising_site<ST>(c, sub, alpha, rep, x, y, z, key, (const ST*)c.src, (ST*)c.dst);
+    ising_site<ST>(c, sub, alpha, rep, x, y, z, key, (const ST*)c.src + base, (ST*)c.dst + base);
   } else {
-    vec_site<N>(c, sub, alpha, rep, x, y, z, key, (const float*)c.src, (float*)c.dst);
+    vec_site<N>(c, sub, alpha, rep, x, y, z, key, (const float*)c.src + base, (float*)c.dst + base);
   }
 }
 
@@ -232,6 +234,81 @@ __global__ void __launch_bounds__(256) packed_class_kernel(const __grid_constant
     const bool bit = acc ? (s < 0) : (s > 0);
     const uint32_t word = __ballot_sync(0xFFFFFFFFu, bit);
     if (lane == 0) dst[wb + own] = word;
+  }
+}
+
+// ---------------------------------------------------------------------------------------- resident sweeps
+// A replica small enough for shared memory stays there for all n sweeps of one call: one block per replica
+// loads its spins once, runs every class of every sweep with a block barrier between classes (a class reads
+// only other classes, so the barrier is the whole dependency), and writes the spins back once. Sweep k of the
+// call uses the key of state[1] + k, as n separate sweeps would.
+struct ResidentParams {
+  Common c;
+  SubDev sub[SCK_MAX_BASIS];
+  int n_classes;
+  int classes[128][2];
+  int n_sweeps;
+};
+
+template <int N, typename ST>
+__global__ void __launch_bounds__(1024) resident_kernel(const __grid_constant__ ResidentParams p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ST* S = reinterpret_cast<ST*>(smem_raw);
+  const int rep = blockIdx.x;
+  const int n = N * p.c.g.nsite;
+  ST* home = (ST*)p.c.dst + (size_t)rep * n;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) S[i] = home[i];
+  __syncthreads();
+  const uint32_t per = (uint32_t)p.c.rows * (uint32_t)p.c.bx;
+  for (int sw = 0; sw < p.n_sweeps; ++sw) {
+    const int32_t key = sweep_key_at(p.c.state, sw);
+    for (int ci = 0; ci < p.n_classes; ++ci) {
+      const int colour = p.classes[ci][0], alpha = p.classes[ci][1];
+      for (uint32_t t = threadIdx.x; t < per; t += blockDim.x) {
+        int x, y, z;
+        if (!class_site(p.c, colour, alpha, t, x, y, z)) continue;
+        if constexpr (N == 1)
+          ising_site<ST>(p.c, p.sub[alpha], alpha, rep, x, y, z, key, S, S);
+        else
+          vec_site<N>(p.c, p.sub[alpha], alpha, rep, x, y, z, key, (const float*)S, (float*)S);
+      }
+      __syncthreads();
+    }
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) home[i] = S[i];
+}
+
+template <int N, typename ST>
+static int launch_resident_t(const ResidentParams& p, int threads, size_t smem, cudaStream_t s) {
+  cudaError_t e = cudaFuncSetAttribute(resident_kernel<N, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return cuda_status(e, "resident kernel shared memory");
+  resident_kernel<N, ST><<<p.c.B, threads, smem, s>>>(p);
+  return cuda_status(cudaGetLastError(), "resident launch");
+}
+
+size_t resident_bytes(const sck_plan* plan) {
+  return (size_t)plan->geom.n * plan->geom.nsite * (plan->mode == SCK_MODE_INT8 ? 1 : 4);
+}
+
+int launch_resident(const sck_plan* plan, const Common& c, int n_sweeps, cudaStream_t s) {
+  ResidentParams p;
+  p.c = c;
+  for (int a = 0; a < SCK_MAX_BASIS; ++a) p.sub[a] = plan->sub[a];
+  p.n_classes = plan->desc.n_classes;
+  for (int i = 0; i < p.n_classes; ++i) {
+    p.classes[i][0] = plan->desc.classes[i][0];
+    p.classes[i][1] = plan->desc.classes[i][1];
+  }
+  p.n_sweeps = n_sweeps;
+  const uint32_t per = (uint32_t)c.rows * (uint32_t)c.bx;
+  int threads = (int)((per + 31) / 32 * 32);
+  threads = threads < 128 ? 128 : (threads > 1024 ? 1024 : threads);
+  const size_t smem = (resident_bytes(plan) + 15) / 16 * 16;
+  if (plan->mode == SCK_MODE_INT8) return launch_resident_t<1, int8_t>(p, threads, smem, s);
+  switch (c.g.n) {
+    case 1: return launch_resident_t<1, float>(p, threads, smem, s);
+    case 2: return launch_resident_t<2, float>(p, threads, smem, s);
+    default: return launch_resident_t<3, float>(p, threads, smem, s);
   }
 }
 

@@ -133,16 +133,20 @@ class Sampler:
         self._obs_ws = {}
         self._workspace(self.B)
 
-    def tune(self, specialised: bool = True, l2_budget: int = 72 << 20):
-        """Execution choices of sweep (specialised lattice kernels, L2 group-pipeline budget in bytes)."""
-        L.check(L.lib().sck_plan_tune(self._plan, int(bool(specialised)), int(l2_budget)))
+    def tune(self, specialised=True, l2_budget: int = 72 << 20, resident_limit: int = 200 << 10):
+        """Execution choices of sweep: specialised kernels (2 or True: lattice and row kernels, 1: lattice
+        kernels only, 0 or False: generic), L2 group-pipeline budget (bytes), largest replica (bytes) whose sweeps
+        run resident in shared memory. The chain does not depend on them."""
+        level = 2 if specialised is True else int(specialised)
+        L.check(L.lib().sck_plan_tune(self._plan, level, int(l2_budget), int(resident_limit)))
         return self.path()
 
     def path(self) -> dict:
-        """The sweep path the plan will take: specialised table id (0 = generic), budget, pipeline group."""
-        sp, bud, grp = ctypes.c_int32(), ctypes.c_int64(), ctypes.c_int32()
-        L.check(L.lib().sck_plan_path(self._plan, ctypes.byref(sp), ctypes.byref(bud), ctypes.byref(grp)))
-        return {"specialised": sp.value, "l2_budget": bud.value, "group": grp.value}
+        """The sweep path: specialised table id (0 = generic), budget, pipeline group, resident or not."""
+        sp, bud, grp, res = ctypes.c_int32(), ctypes.c_int64(), ctypes.c_int32(), ctypes.c_int32()
+        L.check(L.lib().sck_plan_path(self._plan, ctypes.byref(sp), ctypes.byref(bud), ctypes.byref(grp),
+                                      ctypes.byref(res)))
+        return {"specialised": sp.value, "l2_budget": bud.value, "group": grp.value, "resident": bool(res.value)}
 
     def __del__(self):
         h = getattr(self, "_plan", None)

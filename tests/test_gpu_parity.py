@@ -113,6 +113,7 @@ def test_parallel_equals_sequential_chain_on_gpu(name):
     case = C.CASES[name]
     s = case["build"](sy, cr)
     A, R = _sampler(case, s), _sampler(case, s)
+    A.tune(False, 0, 0)                 # generic class launches: the same site update as the sequential kernel
     for X in (A, R):
         X.set_temperature(1.5)
     S1 = A.init_spins(seed=2)
@@ -168,9 +169,9 @@ def test_l2_group_pipeline_equals_class_by_class(build):
     B = 24
     A, R = Sampler(s, B, device="cuda", seed=9, packed=False), Sampler(s, B, device="cuda", seed=9, packed=False)
     per_rep = s.nsite * s.n * (1 if s.n == 1 else 4)
-    pa = A.tune(True, 2 * len(A.classes) * per_rep)
-    assert pa["specialised"] > 0 and pa["group"] >= 1, pa
-    assert R.tune(True, 0)["group"] == 0
+    pa = A.tune(True, 2 * len(A.classes) * per_rep, 0)
+    assert pa["specialised"] > 0 and pa["group"] >= 1 and not pa["resident"], pa
+    assert R.tune(True, 0, 0)["group"] == 0
     for X in (A, R):
         X.set_temperature(torch.linspace(0.5, 5.0, B))
     S1 = A.init_spins(seed=4)
@@ -195,8 +196,8 @@ def test_specialised_and_generic_kernels_agree(name):
     from spin_colour_kernel_b200.sampler import Sampler
     A = Sampler(s, case["B"], device="cuda", seed=case["seed"], **kw)
     G = Sampler(s, case["B"], device="cuda", seed=case["seed"], **kw)
-    assert A.path()["specialised"] > 0
-    assert G.tune(False, 0)["specialised"] == 0
+    assert A.tune(True, 0, 0)["specialised"] > 0
+    assert G.tune(False, 0, 0)["specialised"] == 0
     T = torch.from_numpy(C.temperatures(case["T"], case["B"]))
     for X in (A, G):
         X.set_temperature(T)
@@ -211,6 +212,66 @@ def test_specialised_and_generic_kernels_agree(name):
         frac = float((d > VEC_TOL).double().mean())
         print(f"{name}: specialised vs generic, fraction beyond tolerance {frac:.2e}")
         assert frac <= 0.02
+
+
+ROW_SYSTEMS = {
+    "heis_bcc_j1j2_64x8x6": lambda: sy.System("Heisenberg bcc J1-J2", 3, cr.make("bcc", (1, 2)), (64, 8, 6),
+                                              (True,) * 3, {1: 1.0, 2: 0.3}, h=(0.0, 0.0, 0.1),
+                                              cubic_k1=np.full((2, 6, 8, 64), 0.05, np.float32)),
+    "heis_bcc_128x4x4": lambda: sy.System("Heisenberg bcc", 3, cr.make("bcc"), (128, 4, 4), (True,) * 3, {1: -1.0}),
+    "heis_sc_64x6x4": lambda: sy.System("Heisenberg sc", 3, cr.make("sc"), (64, 6, 4), (True,) * 3, {1: 1.0},
+                                        h=(0.2, 0.0, 0.0)),
+    "xy_square_128x10": lambda: sy.System("XY square", 2, cr.make("square"), (128, 10), (True, True), {1: 1.0},
+                                          h=(0.05, 0.0)),
+}
+
+
+@pytest.mark.parametrize("name", sorted(ROW_SYSTEMS))
+def test_row_kernels_equal_lattice_kernels(name):
+    """Row kernels (contiguous row pairs, shuffles for x-neighbours, one and two segments per row) run the same
+    float32x2 arithmetic as the lattice kernels: spins bit-identical, odd replica count included."""
+    from spin_colour_kernel_b200.sampler import Sampler
+    s = ROW_SYSTEMS[name]()
+    B = 5
+    A, R = Sampler(s, B, device="cuda", seed=3), Sampler(s, B, device="cuda", seed=3)
+    pa, pr = A.tune(2, 0, 0), R.tune(1, 0, 0)
+    assert pa["specialised"] // 100 == 2 and pr["specialised"] // 100 == 1, (pa, pr)
+    for X in (A, R):
+        X.set_temperature(torch.linspace(0.4, 3.0, B))
+    S1 = A.init_spins(seed=7)
+    S2 = S1.clone()
+    A.sweep(S1, 3)
+    R.sweep(S2, 3)
+    assert torch.equal(S1, S2)
+    assert not torch.equal(S1, A.init_spins(seed=7))
+
+
+@pytest.mark.parametrize("name", ["ising_square8", "nanodot_small", "w3_heis_bcc4_j1j2", "w4_xy_triangular12_disk",
+                                  "ising_masked_field_barker", "heis_kagome3_afm"])
+def test_resident_sweeps_equal_class_launches(name):
+    """Whole sweeps resident in shared memory run the generic site update: bit-identical to the generic class
+    launches, for every storage type, masks, extra matrices and multi-sublattice crystals."""
+    if not _have(name):
+        pytest.skip("fixture not generated")
+    case = C.CASES[name]
+    s = case["build"](sy, cr)
+    kw = dict(C.sampler_kwargs(case))
+    kw["packed"] = False
+    from spin_colour_kernel_b200.sampler import Sampler
+    A = Sampler(s, case["B"], device="cuda", seed=case["seed"], **kw)
+    G = Sampler(s, case["B"], device="cuda", seed=case["seed"], **kw)
+    assert A.path()["resident"]
+    assert not G.tune(False, 0, 0)["resident"]
+    T = torch.from_numpy(C.temperatures(case["T"], case["B"]))
+    for X in (A, G):
+        X.set_temperature(T)
+    S1 = A.init_spins(seed=case["init"])
+    S2 = S1.clone()
+    A.sweep(S1, case["sweeps"])
+    for _ in range(case["sweeps"]):
+        G.sweep(S2, 1)
+    assert torch.equal(S1, S2)
+    assert int(A.state[1]) == case["sweeps"]
 
 
 def test_graph_replay_equals_plain_sweeps():
