@@ -179,6 +179,24 @@ int sck_observables(const sck_plan* plan, const sck_buffers* buf, const void* sp
 int sck_pack(const sck_plan* plan, const int8_t* spins, int32_t* words, void* stream);
 int sck_unpack(const sck_plan* plan, const int32_t* words, const int8_t* mask, int8_t* spins, void* stream);
 
+/* Ragged batches (no counterpart in the reference, which runs one Sampler per system): several plans with one
+ * storage mode (int8 or float32) and one spin dimension, of different crystal, size, mask, colouring and
+ * temperatures, swept together. Systems whose replica takes at most resident_limit_bytes of shared memory run
+ * every sweep of a call in one resident launch; the others run one launch per colour step for all of them.
+ *   sck_batch_workspace_size  device bytes of the per-system descriptors (caller-owned workspace);
+ *   sck_batch_bind            write the descriptors for these per-system buffers (a host-to-device copy on
+ *                             `stream`: call it outside stream capture, again when a buffer moves);
+ *   sck_batch_sweep           n sweeps of every system, kernel launches only (capturable); each system's
+ *                             state[1] advances by n;
+ *   sck_batch_info            systems and blocks of the resident launch, blocks of the colour-step launches. */
+typedef struct sck_batch sck_batch;
+int sck_batch_create(const sck_plan* const* plans, int32_t n_plans, int64_t resident_limit_bytes, sck_batch** out);
+int sck_batch_destroy(sck_batch* batch);
+int sck_batch_workspace_size(const sck_batch* batch, int64_t* bytes);
+int sck_batch_bind(sck_batch* batch, const sck_buffers* buffers, void* workspace, void* stream);
+int sck_batch_sweep(sck_batch* batch, void* workspace, int32_t n_sweeps, void* stream);
+int sck_batch_info(const sck_batch* batch, int32_t* resident_systems, int32_t* resident_blocks, int64_t* step_blocks);
+
 /* Advance state[1] by `n` on the device (what a sweep does after its class launches). */
 int sck_advance(int64_t* state, int32_t n, void* stream);
 

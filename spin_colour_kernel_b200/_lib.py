@@ -63,6 +63,12 @@ _SIGNATURES = {
     "sck_pack": ([_vp, _vp, _vp, _vp], _i32),
     "sck_unpack": ([_vp, _vp, _vp, _vp, _vp], _i32),
     "sck_advance": ([_vp, _i32, _vp], _i32),
+    "sck_batch_create": ([ctypes.POINTER(_vp), _i32, _i64, ctypes.POINTER(_vp)], _i32),
+    "sck_batch_destroy": ([_vp], _i32),
+    "sck_batch_workspace_size": ([_vp, ctypes.POINTER(_i64)], _i32),
+    "sck_batch_bind": ([_vp, ctypes.POINTER(Buffers), _vp, _vp], _i32),
+    "sck_batch_sweep": ([_vp, _vp, _i32, _vp], _i32),
+    "sck_batch_info": ([_vp, ctypes.POINTER(_i32), ctypes.POINTER(_i32), ctypes.POINTER(_i64)], _i32),
 }
 
 EXPORTS = tuple(_SIGNATURES)

@@ -69,6 +69,8 @@ static Common make_common(const sck_plan* plan, const sck_buffers* buf, const vo
   return c;
 }
 
+Common make_common_public(const sck_plan* plan, const sck_buffers* buf) { return make_common(plan, buf, buf->spins); }
+
 static bool is_bitwise(int mode) { return mode == SCK_MODE_BITWISE || mode == SCK_MODE_BITWISE_INDEP; }
 
 constexpr long long kResidentDefault = 200ll << 10;

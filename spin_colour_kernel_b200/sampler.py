@@ -400,3 +400,75 @@ class Sampler:
     def magnetization(self, S: torch.Tensor) -> torch.Tensor:
         """Per-sublattice magnetization M_alpha, shape (B, b, n), float64."""
         return self.observables(S)[1]
+
+
+class SamplerBatch:
+    """Several samplers (different systems, sizes, masks, colourings, temperatures) swept together.
+
+    All samplers need the same storage (int8 Ising or float32 components of one spin dimension). Systems whose
+    replica fits `resident_limit` bytes of shared memory run every sweep of a call in one resident launch; the
+    rest run one launch per colour step for all of them (include/sck.h, sck_batch_*). Each sampler keeps its own
+    spins, temperatures, tables and counter; `sweep(n)` advances every sampler's counter by n.
+    """
+
+    def __init__(self, samplers: list, spins: list, resident_limit: int = 200 << 10):
+        if len(samplers) != len(spins) or not samplers:
+            raise ValueError("one spins tensor per sampler")
+        self.samplers = list(samplers)
+        self.spins = list(spins)
+        self.device = samplers[0].device
+        arr = (ctypes.c_void_p * len(samplers))(*[s._plan.value for s in samplers])
+        h = ctypes.c_void_p()
+        L.check(L.lib().sck_batch_create(arr, len(samplers), int(resident_limit), ctypes.byref(h)))
+        self._batch = h
+        nbytes = ctypes.c_int64()
+        L.check(L.lib().sck_batch_workspace_size(self._batch, ctypes.byref(nbytes)))
+        self._ws = torch.empty(max(256, nbytes.value), dtype=torch.uint8, device=self.device)
+        self.bind(spins)
+
+    def bind(self, spins: list):
+        """Point the batch at these spins tensors (and each sampler's current buffers); call outside capture."""
+        for s, S in zip(self.samplers, spins):
+            s._check(S)
+        self.spins = list(spins)
+        bufs = (L.Buffers * len(self.samplers))(*[s._buffers(S) for s, S in zip(self.samplers, spins)])
+        with torch.cuda.device(self.device):
+            L.check(L.lib().sck_batch_bind(self._batch, bufs, _ptr(self._ws), self.samplers[0]._stream()))
+
+    def info(self) -> dict:
+        rs, rb, sb = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int64()
+        L.check(L.lib().sck_batch_info(self._batch, ctypes.byref(rs), ctypes.byref(rb), ctypes.byref(sb)))
+        return {"resident_systems": rs.value, "resident_blocks": rb.value, "step_blocks": sb.value}
+
+    def sweep(self, n: int = 1):
+        with torch.cuda.device(self.device):
+            L.check(L.lib().sck_batch_sweep(self._batch, _ptr(self._ws), int(n), self.samplers[0]._stream()))
+
+    def graph(self, k: int):
+        """Capture k sweeps of the whole batch in a CUDA graph; returns its replay."""
+        with torch.cuda.device(self.device):
+            s = torch.cuda.Stream(device=self.device)
+            s.wait_stream(torch.cuda.current_stream(self.device))
+            with torch.cuda.stream(s):
+                self.sweep(1)
+            torch.cuda.current_stream(self.device).wait_stream(s)
+            torch.cuda.synchronize(self.device)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self.sweep(k)
+        dev = self.device
+
+        def replay():
+            with torch.cuda.device(dev):
+                g.replay()
+        replay.keep = (self, g)
+        return replay
+
+    def __del__(self):
+        h = getattr(self, "_batch", None)
+        if h is not None and h.value:
+            try:
+                L.lib().sck_batch_destroy(h)
+            except Exception:
+                pass
+            self._batch = None
