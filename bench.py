@@ -326,10 +326,15 @@ def main():
     path = A.path()
     C = len(classes)
     groups = -(-A.Bp // path["group"]) if path["group"] else 0
+    # the K timed steps are one call sweep(S, K): the library sees the whole sequence (a resident launch runs all
+    # K sweeps on-chip, the L2 pipeline overlaps consecutive sweeps), as a user running K sweeps would call it
+    K = args.steps
     if path["resident"]:
-        launches_per_sweep = 1
+        launches = 1
+    elif groups:
+        launches = K * groups + C - 1
     else:
-        launches_per_sweep = (groups + C - 1) if groups else C * (-(-A.Bp // (65535 * (2 if s.n > 1 else 1))))
+        launches = K * C * (-(-A.Bp // (65535 * (2 if s.n > 1 else 1))))
 
     for _ in range(args.warmup):
         A.sweep(S, 1)
@@ -339,15 +344,14 @@ def main():
     clocks = ClockSampler(device.index)
     clocks.start()
     time.sleep(0.25)
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     ev[0].record(stream)
-    for k in range(args.steps):
-        A.sweep(S, 1)
-        ev[k + 1].record(stream)
+    A.sweep(S, K)
+    ev[1].record(stream)
     torch.cuda.synchronize(device)
     clk = clocks.stop()
-    ms = ev[0].elapsed_time(ev[-1])
-    step_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
+    ms = ev[0].elapsed_time(ev[1])
+    step_ms = [ms / K]
     if dist:
         x = torch.tensor([ms], device=device)
         tdist.all_reduce(x, op=tdist.ReduceOp.MAX)
@@ -384,10 +388,11 @@ def main():
     value = world * attempts_per_step * args.steps / (ms * 1e6)
     e2e = world * attempts_per_step * e2e_steps / (e2e_ms * 1e6)
     bpa = BYTES_PER_ATTEMPT[args.workload]
-    # the sweep's launches run back to back on one stream: their mean duration is the step time over the launches
-    # (inter-launch gaps and the counter update included, so this is a lower bound on the kernel's rate)
-    bytes_per_launch = attempts_per_step * bpa / launches_per_sweep
-    mean_launch_ms = float(np.median(step_ms)) / launches_per_sweep
+    # the timed launches run back to back on one stream: their mean duration is the timed region over the launches
+    # (inter-launch gaps and the counter updates included, so this is a lower bound on the kernel's rate)
+    launches_per_sweep = launches / K
+    bytes_per_launch = attempts_per_step * K * bpa / launches
+    mean_launch_ms = ms / launches
     achieved = bytes_per_launch / (mean_launch_ms * 1e-3) / 1e9
     peak, peak_kind = hbm_peak()
     traffic = traffic_per_launch(f"{args.workload}")
@@ -404,7 +409,7 @@ def main():
                              f"step times from CUDA events"},
         "e2e": {"value": e2e, "unit": "attempts/ns", "h2d_bytes_per_step": int(beta_h.numel() * 4),
                 "d2h_bytes_per_step": int((E_h.numel() + M_h.numel()) * 8)},
-        "gpu_launches": (launches_per_sweep + 1) * args.steps,
+        "gpu_launches": int(launches + (1 if path["resident"] or groups else K)),
         "clocks": clk,
     }
     if rank == 0 and not args.no_cpu_baseline:

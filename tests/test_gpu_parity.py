@@ -218,7 +218,7 @@ ROW_SYSTEMS = {
     "heis_bcc_j1j2_64x8x6": lambda: sy.System("Heisenberg bcc J1-J2", 3, cr.make("bcc", (1, 2)), (64, 8, 6),
                                               (True,) * 3, {1: 1.0, 2: 0.3}, h=(0.0, 0.0, 0.1),
                                               cubic_k1=np.full((2, 6, 8, 64), 0.05, np.float32)),
-    "heis_bcc_128x4x4": lambda: sy.System("Heisenberg bcc", 3, cr.make("bcc"), (128, 4, 4), (True,) * 3, {1: -1.0}),
+    "heis_sc_128x4x4": lambda: sy.System("Heisenberg sc", 3, cr.make("sc"), (128, 4, 4), (True,) * 3, {1: -1.0}),
     "heis_sc_64x6x4": lambda: sy.System("Heisenberg sc", 3, cr.make("sc"), (64, 6, 4), (True,) * 3, {1: 1.0},
                                         h=(0.2, 0.0, 0.0)),
     "xy_square_128x10": lambda: sy.System("XY square", 2, cr.make("square"), (128, 10), (True, True), {1: 1.0},
