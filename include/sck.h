@@ -173,6 +173,19 @@ int sck_observables_workspace_size(const sck_plan* plan, int32_t batch, int64_t*
 int sck_observables(const sck_plan* plan, const sck_buffers* buf, const void* spins, int32_t storage,
                     int32_t batch, double* E, double* M, void* workspace, void* stream);
 
+/* sck_observables without a caller workspace — no counterpart in the reference (added for callers that cannot
+ * allocate device memory: a host whose device memory all belongs to its own pool or caching allocator, a loop
+ * that cannot afford the synchronisation an allocation may bring, an FFI binding that cannot own a device
+ * buffer). The partial sums go to a fixed 2 MiB array compiled into the library, which every GPU that loads the
+ * library keeps until the process exits; a request needing more (batch x blocks per replica x 16 doubles) fails
+ * with SCK_ERR_INVALID — use sck_observables then. The entry point allocates nothing. Its first call on a device
+ * looks up the array's device address (make that first call before any stream capture). Every call shares the
+ * one array and leaves its partial sums there; no part needs clearing, since each slot the final sum reads is
+ * written earlier in the same call, but calls that overlap on the GPU (other streams, other threads) race on it:
+ * keep them ordered. */
+int sck_observables_noalloc(const sck_plan* plan, const sck_buffers* buf, const void* spins, int32_t storage,
+                            int32_t batch, double* E, double* M, void* stream);
+
 /* Storage conversion (Sampler.pack / unpack, sampler.py:169-188). pack: int8 spins [B, 1, b, L3, L2, L1]
  * (+-1, 0 masked) -> int32 words [W, 1, b, L3, L2, L1] (padding replicas 0). unpack: words -> int8 spins,
  * masked sites 0. */

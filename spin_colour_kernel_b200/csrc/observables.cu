@@ -6,6 +6,9 @@
 // + k2 (sx sy sz)^2 and its contribution to M[alpha][k]. Warp shuffles, then shared memory, reduce a block to one
 // partial per value; a second kernel sums the partials of a replica in block order, so results do not depend
 // on scheduling.
+#include <mutex>
+#include <string>
+
 #include "internal.h"
 
 namespace sck {
@@ -157,3 +160,73 @@ int launch_observables(const sck_plan* plan, const void* spins, int storage, int
 }
 
 }  // namespace sck
+
+// ------------------------------------------------------------------------------------ allocation-free entry
+// Some callers cannot allocate device memory: a host that hands every device byte to its own pool or caching
+// allocator (a cudaMalloc behind its back breaks its accounting or its budget), a latency-critical loop that
+// cannot pay the device-wide synchronisation cudaMalloc / cudaFree may imply, or an FFI binding with no way to
+// own a device buffer. For them the per-block partial sums of the observables live in this fixed array, which
+// every GPU that loads the library keeps for the life of the process.
+namespace sck {
+
+constexpr size_t kScratchDoubles = (size_t)1 << 18;   // 2 MiB of FP64 partial sums
+static __device__ __align__(256) double g_observables_scratch[kScratchDoubles];
+
+constexpr int kScratchDevices = 256;
+static std::mutex g_scratch_lock;
+static double* g_scratch_addr[kScratchDevices] = {};
+
+// Device address of the scratch array on the current device, looked up once per device. In host code the
+// array's name is only a host-side handle, so the address must come from the runtime.
+static int scratch_address(double** out) {
+  int dev = 0;
+  int rc = cuda_status(cudaGetDevice(&dev), "no-alloc observables: current device");
+  if (rc != SCK_OK) return rc;
+  if (dev < 0 || dev >= kScratchDevices) return cuda_status(cudaErrorInvalidDevice, "no-alloc observables: device");
+  std::lock_guard<std::mutex> guard(g_scratch_lock);
+  if (g_scratch_addr[dev] == nullptr) {
+    void* p = nullptr;
+    rc = cuda_status(cudaGetSymbolAddress(&p, g_observables_scratch), "no-alloc observables: scratch address");
+    if (rc != SCK_OK) return rc;
+    g_scratch_addr[dev] = (double*)p;
+  }
+  *out = g_scratch_addr[dev];
+  return SCK_OK;
+}
+
+}  // namespace sck
+
+extern "C" int sck_observables_noalloc(const sck_plan* plan, const sck_buffers* buf, const void* spins,
+                                       int32_t storage, int32_t batch, double* E, double* M, void* stream) {
+  using namespace sck;
+  if (plan == nullptr || buf == nullptr || spins == nullptr) {
+    set_error("null plan, buffers or spins");
+    return SCK_ERR_INVALID;
+  }
+  if (batch < 1 || batch > 65535) {
+    set_error("batch must be within 1 .. 65535");
+    return SCK_ERR_INVALID;
+  }
+  if (storage != SCK_MODE_INT8 && storage != SCK_MODE_F32 && storage != SCK_MODE_PACKED) {
+    set_error("observables read int8, float32 or packed storage");
+    return SCK_ERR_INVALID;
+  }
+  if (storage != SCK_MODE_F32 && plan->geom.n != 1) {
+    set_error("vector models use float32 storage");
+    return SCK_ERR_INVALID;
+  }
+  if ((plan->geom.has_mask && buf->mask == nullptr) || (plan->geom.has_cubic && buf->k1 == nullptr)) {
+    set_error("the system needs its mask / k1 buffers");
+    return SCK_ERR_INVALID;
+  }
+  const size_t need = (size_t)batch * obs_blocks_per_rep(plan, batch) * OBS_VALUES;
+  if (need > kScratchDoubles) {
+    set_error("no-alloc observables: " + std::to_string(need * sizeof(double)) + " bytes of partial sums exceed the " +
+              std::to_string(kScratchDoubles * sizeof(double)) + "-byte scratch; use sck_observables with a workspace");
+    return SCK_ERR_INVALID;
+  }
+  double* scratch = nullptr;
+  const int rc = scratch_address(&scratch);
+  if (rc != SCK_OK) return rc;
+  return launch_observables(plan, spins, storage, batch, buf->mask, buf->k1, E, M, scratch, (cudaStream_t)stream);
+}
