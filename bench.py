@@ -39,6 +39,7 @@ import torch
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
+RESIDENT_LIMIT = 200 << 10        # the plan's default: replicas up to 200 KiB sweep resident in shared memory
 BYTES_PER_ATTEMPT = {"heisenberg-bcc": 24, "ising-sc-bitwise": 0.25, "ising-square": 2, "xy-ragged": 16}
 FALLBACK_HBM_GBS = 6650.0
 
@@ -280,10 +281,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--L", type=int, default=64, help="heisenberg-bcc cells per axis (profiling runs use less)")
     ap.add_argument("--replicas", type=int, default=1536, help="heisenberg-bcc replicas")
-    ap.add_argument("--path", default="auto", choices=["auto", "autotune", "classwise", "lattice", "generic"],
-                    help="sweep path: plan default, autotuned, row/lattice kernels class by class, lattice kernels "
-                         "only, or generic kernels")
-    ap.add_argument("--l2-mb", type=float, default=None, help="L2 budget of the group pipeline (MiB)")
+    ap.add_argument("--path", default="auto", choices=["auto", "autotune", "row", "lattice", "generic"],
+                    help="sweep path: plan default, autotuned, row and lattice kernels, lattice kernels only, or "
+                         "generic kernels")
+    ap.add_argument("--l2-mb", type=float, default=None,
+                    help="L2 budget of the group pipeline (MiB); with an explicit --path, 0 (class by class) "
+                         "unless given")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -309,17 +312,14 @@ def main():
             tdist.destroy_process_group()
         return
     s, A, S, T, cfg = make_workload(args.workload, rank, device, args.L, args.replicas)
-    if args.path == "classwise":
-        A.tune(2, 0, 0)
-    elif args.path == "lattice":
-        A.tune(1, 0, 0)
-    elif args.path == "generic":
-        A.tune(0, 0, 0)
+    budget = int((args.l2_mb or 0) * (1 << 20))
+    if args.path in ("row", "lattice", "generic"):
+        A.tune({"row": 2, "lattice": 1, "generic": 0}[args.path], budget, RESIDENT_LIMIT)
     elif args.path == "autotune":
         from spin_colour_kernel_b200.autotune import autotune
         cfg["autotune"] = autotune(A, S, use_cache=False)
     elif args.l2_mb is not None:
-        A.tune(2, int(args.l2_mb * (1 << 20)), 0)
+        A.tune(1, budget, RESIDENT_LIMIT)
     attempts_per_step = A.B * s.n_active
     stream = torch.cuda.current_stream(device)
     classes = list(A.classes)

@@ -70,6 +70,14 @@ _SIGNATURES = {
     "sck_batch_bind": ([_vp, ctypes.POINTER(Buffers), _vp, _vp], _i32),
     "sck_batch_sweep": ([_vp, _vp, _i32, _vp], _i32),
     "sck_batch_info": ([_vp, ctypes.POINTER(_i32), ctypes.POINTER(_i32), ctypes.POINTER(_i64)], _i32),
+    # learned block proposal (include/sck_made.h)
+    "sck_made_sizes": ([_i32, _i32, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64)], _i32),
+    "sck_made_prepare": ([_vp, _i32, _vp], _i32),
+    "sck_made_gather": ([_vp, _i32, _i32, _vp, _vp], _i32),
+    "sck_made_forward": ([_vp, _i32, _vp, _i32, _vp, _vp, _vp, _vp], _i32),
+    "sck_made_grads": ([_vp, _i32, _vp, _i32, _vp, _vp, _vp, _vp], _i32),
+    "sck_made_train_step": ([_vp, _vp, _i32, _vp, _i32, _f32, _f32, _f32, _f32, _i32, _vp, _vp, _vp], _i32),
+    "sck_made_colour_step": ([_vp, _i32, _vp, _i32, _i32, _vp, _i32, _i64, _i32, _vp, _vp, _vp], _i32),
 }
 
 EXPORTS = tuple(_SIGNATURES)

@@ -67,7 +67,7 @@ def autotune(sampler, S: torch.Tensor, sweeps: int = 3, use_cache: bool = True) 
     cache = _load() if use_cache else {}
     if key in cache:
         c = cache[key]
-        sampler.tune(c["specialised"] > 0, c["l2_budget"], c["resident_limit"])
+        sampler.tune(c["level"], c["l2_budget"], c["resident_limit"])
         return dict(c, cached=True)
     saved = sampler.state.clone()
     work = S.clone()
@@ -91,7 +91,7 @@ def autotune(sampler, S: torch.Tensor, sweeps: int = 3, use_cache: bool = True) 
     del work
     ms, spec, budget, resident, p = min(results, key=lambda r: r[0])
     sampler.tune(spec, budget, resident)
-    choice = {"specialised": p["specialised"], "l2_budget": budget, "resident_limit": resident, "group": p["group"],
+    choice = {"level": spec, "specialised": p["specialised"], "l2_budget": budget, "resident_limit": resident, "group": p["group"],
               "resident": p["resident"], "ms_per_sweep": ms,
               "tried": [{"specialised": r[4]["specialised"], "group": r[4]["group"], "resident": r[4]["resident"],
                          "ms": r[0]} for r in results]}

@@ -35,7 +35,7 @@ def nvcc() -> str:
 
 
 def _headers() -> list[Path]:
-    return sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + [ROOT / "include" / "sck.h"]
+    return sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + [ROOT / "include" / "sck.h", ROOT / "include" / "sck_made.h"]
 
 
 def _stale(target: Path, deps: list[Path]) -> bool:

@@ -342,8 +342,8 @@ int sck_plan_create(const sck_system_desc* d, int32_t batch, int32_t mode, sck_p
   p->NP = np < 1 ? 1 : np;
   p->field = (d->n == 1 && d->h64[0] != 0.0) ? 1 : 0;
   p->spec = find_spec(p);
-  p->row_kernels = 1;
-  p->l2_budget = 72ll << 20;
+  p->row_kernels = 0;
+  p->l2_budget = 0;
   p->resident_limit = kResidentDefault;
   *out = p;
   return SCK_OK;

@@ -133,11 +133,12 @@ class Sampler:
         self._obs_ws = {}
         self._workspace(self.B)
 
-    def tune(self, specialised=True, l2_budget: int = 72 << 20, resident_limit: int = 200 << 10):
-        """Execution choices of sweep: specialised kernels (2 or True: lattice and row kernels, 1: lattice
-        kernels only, 0 or False: generic), L2 group-pipeline budget (bytes), largest replica (bytes) whose sweeps
-        run resident in shared memory. The chain does not depend on them."""
-        level = 2 if specialised is True else int(specialised)
+    def tune(self, specialised=True, l2_budget: int = 0, resident_limit: int = 200 << 10):
+        """Execution choices of sweep: specialised kernels (1 or True: lattice kernels, the default; 2: row
+        kernels where the system allows them, else lattice kernels; 0 or False: generic), L2 group-pipeline budget
+        (bytes), largest replica (bytes) whose sweeps run resident in shared memory. The chain does not depend on
+        them."""
+        level = int(specialised)
         L.check(L.lib().sck_plan_tune(self._plan, level, int(l2_budget), int(resident_limit)))
         return self.path()
 

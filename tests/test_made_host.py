@@ -1,0 +1,53 @@
+"""Host-side checks of the learned block proposal's C ABI (no device work): sizes, layout and refusals."""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from oracle import made as MD
+from spin_colour_kernel_b200 import _lib as L
+from spin_colour_kernel_b200 import learned as LP
+
+
+def _sizes(groups, batch):
+    p, a, t = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+    rc = L.lib().sck_made_sizes(groups, batch, ctypes.byref(p), ctypes.byref(a), ctypes.byref(t))
+    return rc, p.value, a.value, t.value
+
+
+def test_sizes_and_refusals():
+    rc, p, a, t = _sizes(16, 8192)
+    assert rc == 0
+    assert p >= LP.NPARAM * 4 + 2 * (264 * (160 + 512) + 72 * 256) and p % 256 == 0
+    assert a == 2 * LP.NPARAM * 4
+    assert t > 8192 * 256 * 2 * 6
+    assert _sizes(17, 64)[0] == L.ERR_INVALID
+    assert _sizes(64, 100)[0] == L.ERR_INVALID
+    assert b"batch" in L.lib().sck_last_error()
+
+
+def test_colour_step_refusals_before_any_launch():
+    lib = L.lib()
+    fake = ctypes.c_void_p(256)
+    beta = ctypes.c_void_p(512)
+    assert lib.sck_made_colour_step(None, 16, fake, 4, 16, beta, 0, 1, 0, None, None, None) == L.ERR_INVALID
+    assert lib.sck_made_colour_step(fake, 16, fake, 4, 12, beta, 0, 1, 0, None, None, None) == L.ERR_INVALID
+    assert lib.sck_made_colour_step(fake, 16, fake, 4, 16, beta, 8, 1, 0, None, None, None) == L.ERR_INVALID
+    assert lib.sck_made_colour_step(fake, 32, fake, 4, 16, beta, 0, 1, 0, None, None, None) == L.ERR_INVALID
+    # 17 x replicas x blocks must fit the int32 Philox counter
+    assert lib.sck_made_colour_step(fake, 16, fake, 100000, 64, beta, 0, 1, 0, None, None, None) == L.ERR_COUNTER
+
+
+def test_parameter_flattening_round_trips_and_matches_the_oracle_shapes():
+    params = LP.kaiming_params(3)
+    ref = MD.init_params(96, 64, 256, seed=3)
+    for (W, b), (Wr, br) in zip(params, ref):
+        assert W.shape == Wr.shape and b.shape == br.shape
+        np.testing.assert_array_equal(W, Wr)
+    flat = LP.flatten(params)
+    assert flat.size == LP.NPARAM
+    for (W, b), (W2, b2) in zip(params, LP.unflatten(flat)):
+        np.testing.assert_array_equal(W, W2)
+        np.testing.assert_array_equal(b, b2)
