@@ -40,7 +40,8 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 RESIDENT_LIMIT = 200 << 10        # the plan's default: replicas up to 200 KiB sweep resident in shared memory
-BYTES_PER_ATTEMPT = {"heisenberg-bcc": 24, "ising-sc-bitwise": 0.25, "ising-square": 2, "xy-ragged": 16}
+BYTES_PER_ATTEMPT = {"heisenberg-bcc": 24, "ising-sc-bitwise": 0.25, "ising-square": 2, "xy-ragged": 16,
+                     "learned-ising-sc": 2}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -270,6 +271,105 @@ def ragged(args, rank, world, device):
         print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------------------ learned block proposal
+def learned(args, rank, world, device):
+    """3D Ising sc L=64 periodic at T = 4.5115, 256 replicas: plain colour sweeps against block rounds of the
+    learned proposal (8 colour steps of 4x4x4 blocks, MADE 160-256-256-256-64) plus one plain sweep. The network
+    is trained on the 2^20 blocks of a plain-chain configuration of all replicas. Reports tau_int of |M| and E
+    (Sokal window over the (time, replica) series) and effective independent samples per second of each arm."""
+    from spin_colour_kernel_b200 import stats
+    from spin_colour_kernel_b200 import system as sy
+    from spin_colour_kernel_b200.learned import BlockProposal
+    from spin_colour_kernel_b200.sampler import Sampler
+    L, R, T = 64, 256, 4.5115
+    K_plain, K_learned = args.learned_plain_sweeps, args.learned_rounds
+    s = sy.ising("sc", L)
+    A = Sampler(s, R, device=device, seed=5 + 1000 * rank, packed=False)
+    A.set_temperature(torch.full((R,), T))
+    S = A.init_spins(seed=1)
+    A.sweep(S, args.learned_therm)
+    beta = torch.full((R,), 1.0 / T, dtype=torch.float32, device=device)
+    P = BlockProposal(L, R, groups=args.learned_groups, seed=7, device=device)
+    ev = lambda: torch.cuda.Event(enable_timing=True)          # noqa: E731
+    t0, t1 = ev(), ev()
+    t0.record()
+    data = P.gather(S)
+    losses = P.train(data, steps=args.learned_train_steps, batch=8192, lr=1e-3)
+    t1.record()
+    torch.cuda.synchronize(device)
+    train_ms = t0.elapsed_time(t1)
+    del data
+
+    def series(step, K):
+        X = S.clone()
+        E_all = torch.empty((K, R), dtype=torch.float64, device=device)
+        M_all = torch.empty((K, R), dtype=torch.float64, device=device)
+        E = torch.empty(R, dtype=torch.float64, device=device)
+        M = torch.empty((R, 1, 1), dtype=torch.float64, device=device)
+        for k in range(K):
+            step(X, k)
+            A.observables(X, E, M)
+            E_all[k].copy_(E)
+            M_all[k].copy_(M.reshape(R).abs())
+        return E_all.cpu().numpy() / L ** 3, M_all.cpu().numpy() / L ** 3, X
+
+    def timed(step, K):
+        X = S.clone()
+        for k in range(3):
+            step(X, k)
+        torch.cuda.synchronize(device)
+        a, b = ev(), ev()
+        a.record()
+        for k in range(K):
+            step(X, k)
+        b.record()
+        torch.cuda.synchronize(device)
+        return a.elapsed_time(b) / K
+
+    acc = torch.zeros(R, dtype=torch.int32, device=device)
+
+    def plain_step(X, k):
+        A.sweep(X, 1)
+
+    def learned_step(X, k):
+        P.round(X, beta, seed=11, rnd=k, accepted=acc)
+        A.sweep(X, 1)
+
+    clocks = ClockSampler(device.index)
+    clocks.start()
+    ms_plain = timed(plain_step, 200)
+    ms_learned = timed(learned_step, 50)
+    clk = clocks.stop()
+    acc.zero_()
+    Ep, Mp, _ = series(plain_step, K_plain)
+    El, Ml, _ = series(learned_step, K_learned)
+    acceptance = float(acc.sum().item()) / (K_learned * R * (L // 4) ** 3)
+    out = {}
+    for name, (E_, M_, ms) in {"plain": (Ep, Mp, ms_plain), "learned": (El, Ml, ms_learned)}.items():
+        tm, te = stats.integrated_tau(M_), stats.integrated_tau(E_)
+        rate = R / (ms * 1e-3)                     # configurations (replica steps) per second
+        out[name] = {"ms_per_step": ms, "tau_int_absM": tm, "tau_int_E": te, "steps": int(E_.shape[0]),
+                     "eff_samples_per_s_absM": stats.effective_rate(rate, tm),
+                     "eff_samples_per_s_E": stats.effective_rate(rate, te),
+                     "absM": [float(M_.mean()), float(M_.std() * np.sqrt(2 * tm / M_.size))],
+                     "E": [float(E_.mean()), float(E_.std() * np.sqrt(2 * te / E_.size))]}
+    agree = {k: abs(out["plain"][k][0] - out["learned"][k][0]) /
+             max(np.hypot(out["plain"][k][1], out["learned"][k][1]), 1e-300) for k in ("absM", "E")}
+    gain = out["learned"]["eff_samples_per_s_absM"] / out["plain"]["eff_samples_per_s_absM"]
+    line = {"metric": "effective independent samples/s of |M| (learned block proposal)",
+            "value": out["learned"]["eff_samples_per_s_absM"], "unit": "samples/s", "n_gpus": world,
+            "higher_is_better": True, "vs_plain": gain, "dtype": "bf16/f32", "data": "synthetic",
+            "config": {"workload": "learned-ising-sc-64 (T=4.5115, 256 replicas, 4x4x4 blocks, 8 colours)",
+                       "groups": args.learned_groups, "therm_sweeps": args.learned_therm,
+                       "train_steps": args.learned_train_steps, "train_batch": 8192, "train_blocks": R * 4096,
+                       "train_ms": train_ms, "loss_first": float(losses[:10].mean()),
+                       "loss_last": float(losses[-10:].mean())},
+            "acceptance": acceptance, "plain": out["plain"], "learned": out["learned"],
+            "agreement_sigma": agree, "clocks": clk}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 # ------------------------------------------------------------------------------------------------- main
 def main():
     ap = argparse.ArgumentParser()
@@ -284,6 +384,11 @@ def main():
     ap.add_argument("--path", default="auto", choices=["auto", "autotune", "row", "lattice", "generic"],
                     help="sweep path: plan default, autotuned, row and lattice kernels, lattice kernels only, or "
                          "generic kernels")
+    ap.add_argument("--learned-groups", type=int, default=16, choices=[16, 64])
+    ap.add_argument("--learned-therm", type=int, default=2000)
+    ap.add_argument("--learned-train-steps", type=int, default=1000)
+    ap.add_argument("--learned-plain-sweeps", type=int, default=6000)
+    ap.add_argument("--learned-rounds", type=int, default=1500)
     ap.add_argument("--l2-mb", type=float, default=None,
                     help="L2 budget of the group pipeline (MiB); with an explicit --path, 0 (class by class) "
                          "unless given")
@@ -305,8 +410,8 @@ def main():
     torch.cuda.set_device(device)
     from spin_colour_kernel_b200 import build as bld
     bld.build()
-    if args.workload == "xy-ragged":
-        ragged(args, rank, world, device)
+    if args.workload in ("xy-ragged", "learned-ising-sc"):
+        (ragged if args.workload == "xy-ragged" else learned)(args, rank, world, device)
         if dist:
             tdist.barrier()
             tdist.destroy_process_group()

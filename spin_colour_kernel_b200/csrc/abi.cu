@@ -363,7 +363,7 @@ int sck_plan_tune(sck_plan* plan, int32_t specialised, int64_t l2_budget_bytes, 
 int sck_plan_path(const sck_plan* plan, int32_t* specialised, int64_t* l2_budget_bytes, int32_t* group,
                   int32_t* resident) {
   if (plan == nullptr) return fail(SCK_ERR_INVALID, "null plan");
-  if (specialised) *specialised = plan->spec ? (row_kernel_ok(plan) ? 2 : 1) * 100 + plan->spec : 0;
+  if (specialised) *specialised = plan->spec ? (seg_kernel_ok(plan) ? 2 : 1) * 100 + plan->spec : 0;
   if (l2_budget_bytes) *l2_budget_bytes = plan->l2_budget;
   if (group) *group = pipeline_group(plan);
   if (resident) *resident = use_resident(plan) ? 1 : 0;

@@ -6,8 +6,9 @@
 // one add and one load per component. Ising keeps the integer key and the host table (bit-exact); vector models
 // run two replicas per thread in packed float32x2 arithmetic (add.rn.f32x2 / mul.rn.f32x2, round-to-nearest
 // per lane, same operation order as the generic kernel), with proposal trigonometry and exp on the SFU
-// (__sinf / __cosf on [-pi, pi], __expf): per-spin differences from the reference stay ~1e-6. Lattices whose
-// classes alternate along x run the row kernels of rowpair.cu instead when their box allows it.
+// (__sinf / __cosf on [-pi, pi], __expf): per-spin differences from the reference stay ~1e-6. Vector models on
+// lattices whose classes alternate along x run the segment kernels of segment.cu instead when the tuning level
+// asks for them and their box allows it.
 //
 // Group pipeline. A sweep visits its C classes in order, and each class launch reads the whole state. When the
 // state is larger than L2, the replicas are cut into groups whose C-group working set fits in L2, and launch k
@@ -240,8 +241,11 @@ static void launch_lat(const sck_plan* plan, const SpecParams& p, dim3 grid, cud
     launch_lat_per<Lat, false>(plan, p, grid, s);
 }
 
+// replicas per grid y-slot: vector models pair two replicas per thread in the lattice kernels
+static int slot_replicas(const sck_plan* plan) { return plan->geom.n == 1 || seg_kernel_ok(plan) ? 1 : 2; }
+
 static int launch_tasks(const sck_plan* plan, SpecParams& p, cudaStream_t s) {
-  const int per_unit = plan->geom.n == 1 ? 1 : 2;
+  const int per_unit = slot_replicas(plan);
   int most = 1;
   for (int i = 0; i < p.n_tasks; ++i) {
     const int n = p.tasks[i].rep_end - p.tasks[i].rep_begin;
@@ -250,7 +254,7 @@ static int launch_tasks(const sck_plan* plan, SpecParams& p, cudaStream_t s) {
   p.units_per_task = (most + per_unit - 1) / per_unit;
   const long long ys = (long long)p.units_per_task * p.n_tasks;
   if (ys > 65535) return cuda_status(cudaErrorInvalidConfiguration, "task launch: too many replicas per launch");
-  if (row_kernel_ok(plan)) return launch_row_tasks(plan, p, (int)ys, s);
+  if (seg_kernel_ok(plan)) return launch_seg_tasks(plan, p, (int)ys, s);
   const uint32_t per = (uint32_t)p.c.rows * (uint32_t)p.c.bx;
   const dim3 grid((per + 255) / 256, (unsigned)ys);
   switch (plan->spec) {
@@ -270,15 +274,13 @@ static SpecParams spec_params(const sck_plan* plan, const Common& c) {
   p.c = c;
   for (int a = 0; a < SCK_MAX_BASIS; ++a)
     for (int gi = 0; gi < SCK_MAX_GROUPS; ++gi) p.J[a][gi] = plan->sub[a].J[gi];
-  p.segs_per_row = plan->geom.L1 / 64;
   return p;
 }
 
 // One class over all replicas, in chunks of at most 65535 grid rows.
 int launch_spec_class(const sck_plan* plan, const Common& c, int colour, int alpha, cudaStream_t s) {
   SpecParams p = spec_params(plan, c);
-  const int per_unit = plan->geom.n == 1 ? 1 : 2;
-  const int chunk = 65535 * per_unit;
+  const int chunk = 65535 * slot_replicas(plan);
   for (int r0 = 0; r0 < c.B; r0 += chunk) {
     p.n_tasks = 1;
     p.tasks[0] = Task{colour, alpha, r0, r0 + chunk < c.B ? r0 + chunk : c.B, 0};

@@ -1,6 +1,6 @@
-// Shared pieces of the specialised class kernels (fast_sweep.cu, rowpair.cu): task lists of the L2 group
+// Shared pieces of the specialised class kernels (fast_sweep.cu, segment.cu): task lists of the L2 group
 // pipeline, compile-time loops over the lattice tables, and the second half of a vector-model update (proposal,
-// energy change, anisotropy, acceptance) for two replicas in packed float32x2 arithmetic.
+// energy change, anisotropy, acceptance) for two attempts in packed float32x2 arithmetic.
 #pragma once
 
 #include <type_traits>
@@ -21,7 +21,7 @@ struct SpecParams {
   float J[SCK_MAX_BASIS][SCK_MAX_GROUPS];
   int n_tasks;
   int units_per_task;     // grid.y slots per task (replicas, or replica pairs for vector models)
-  int segs_per_row;       // row kernels: 64-cell segments per row
+  FastDiv fd_segs;        // segment kernels: 8-site segments per row
   Task tasks[kMaxTasks];
 };
 
@@ -56,17 +56,18 @@ __device__ __forceinline__ void sincos_2pi(float phi, float& sn, float& cs) {
   cs = -__cosf(red);
 }
 
-// Proposal, energy change with cubic anisotropy, and Metropolis / Barker decision of two replicas (lane .x =
-// rep0, lane .y = rep1) of site `own`, given their spins s and local fields v (field included). Returns the
-// proposals in t and the decisions in acc0 / acc1. Same operation order as the reference's kernel
-// (generator.py:275-305); packed float32x2 operations round each lane to nearest.
+// Proposal, energy change with cubic anisotropy, and Metropolis / Barker decision of two attempts (lane .x, lane
+// .y) with Philox counters cnt0 / cnt1, anisotropy sites k1_0 / k1_1 and inverse temperatures beta, given their
+// spins s and local fields v (field included). Returns the proposals in t and the decisions in acc0 / acc1. Same
+// operation order as the reference's kernel (generator.py:275-305); packed float32x2 operations round each lane
+// to nearest. With two == false lane .y repeats lane .x's draws and its result is ignored.
 template <int N>
-__device__ __forceinline__ void finish_pair(const Common& c, int own, int rep0, int rep1, bool two, int32_t key,
-                                            const float2 (&s)[N], const float2 (&v)[N], float2 (&t)[N], bool& acc0,
-                                            bool& acc1) {
+__device__ __forceinline__ void finish_core(const Common& c, uint32_t cnt0, uint32_t cnt1, bool two, int k1_0,
+                                            int k1_1, float2 beta, int32_t key, const float2 (&s)[N],
+                                            const float2 (&v)[N], float2 (&t)[N], bool& acc0, bool& acc1) {
   const Geometry& g = c.g;
-  const Philox4 ra = philox4x32_10(counter_of(rep0, g.nsite, own), 0u, key_lo(key), key_hi(key));
-  const Philox4 rb = two ? philox4x32_10(counter_of(rep1, g.nsite, own), 0u, key_lo(key), key_hi(key)) : ra;
+  const Philox4 ra = philox4x32_10(cnt0, 0u, key_lo(key), key_hi(key));
+  const Philox4 rb = two ? philox4x32_10(cnt1, 0u, key_lo(key), key_hi(key)) : ra;
   const float2 u0 = make_float2(to_uniform(ra.x0), to_uniform(rb.x0));
   const float TWO_PI = 6.2831855f;
   if constexpr (N == 2) {
@@ -94,7 +95,7 @@ __device__ __forceinline__ void finish_pair(const Common& c, int own, int rep0, 
   float2 dE = __fmul2_rn(m1, d);
   if constexpr (N == 3) {
     if (g.has_cubic) {
-      const float2 k1 = f2(c.k1[own]);
+      const float2 k1 = make_float2(c.k1[k1_0], c.k1[k1_1]);
       const float2 k2 = f2(c.k2);
       auto aniso = [&](const float2* p) {
         const float2 q01 = __fmul2_rn(p[0], p[1]), q02 = __fmul2_rn(p[0], p[2]), q12 = __fmul2_rn(p[1], p[2]);
@@ -105,7 +106,6 @@ __device__ __forceinline__ void finish_pair(const Common& c, int own, int rep0, 
       dE = __fadd2_rn(dE, __fadd2_rn(aniso(t), __fmul2_rn(m1, aniso(s))));
     }
   }
-  const float2 beta = make_float2(c.beta[rep0], c.beta[rep1]);
   if (g.acceptance == SCK_BARKER) {
     const float2 xb = __fmul2_rn(beta, dE);
     acc0 = __fmul_rn(u0.x, __fadd_rn(1.0f, __expf(xb.x))) < 1.0f;
@@ -117,8 +117,17 @@ __device__ __forceinline__ void finish_pair(const Common& c, int own, int rep0, 
   }
 }
 
-// Row kernels (rowpair.cu): eligibility and the task launch.
-bool row_kernel_ok(const sck_plan* plan);
-int launch_row_tasks(const sck_plan* plan, const SpecParams& p, int ys, cudaStream_t s);
+// Two replicas rep0 / rep1 of site `own`.
+template <int N>
+__device__ __forceinline__ void finish_pair(const Common& c, int own, int rep0, int rep1, bool two, int32_t key,
+                                            const float2 (&s)[N], const float2 (&v)[N], float2 (&t)[N], bool& acc0,
+                                            bool& acc1) {
+  finish_core<N>(c, counter_of(rep0, c.g.nsite, own), counter_of(rep1, c.g.nsite, own), two, own, own,
+                 make_float2(c.beta[rep0], c.beta[rep1]), key, s, v, t, acc0, acc1);
+}
+
+// Segment kernels (segment.cu): eligibility and the task launch.
+bool seg_kernel_ok(const sck_plan* plan);
+int launch_seg_tasks(const sck_plan* plan, SpecParams& p, int ys, cudaStream_t s);
 
 }  // namespace sck

@@ -19,7 +19,7 @@ import ctypes
 import numpy as np
 import torch
 
-from . import _lib as L
+from . import _lib as abi
 
 IN, HIDDEN, SPINS, BOUNDARY = 160, 256, 64, 96
 NPARAM = 256 * 160 + 256 + 2 * (256 * 256 + 256) + 64 * 256 + 64
@@ -71,7 +71,7 @@ class BlockProposal:
         self.L, self.R, self.groups = int(L), int(R), int(groups)
         self.nb = self.L // 4
         pb, ab = ctypes.c_int64(), ctypes.c_int64()
-        L.check(L.lib().sck_made_sizes(self.groups, 64, ctypes.byref(pb), ctypes.byref(ab), None))
+        abi.check(abi.lib().sck_made_sizes(self.groups, 64, ctypes.byref(pb), ctypes.byref(ab), None))
         self.params = torch.zeros(pb.value, dtype=torch.uint8, device=self.device)
         self.adam = torch.zeros(ab.value // 4, dtype=torch.float32, device=self.device)
         self.t = 0
@@ -92,7 +92,7 @@ class BlockProposal:
         self.adam.zero_()
         self.t = 0
         with torch.cuda.device(self.device):
-            L.check(L.lib().sck_made_prepare(_ptr(self.params), self.groups, self._stream()))
+            abi.check(abi.lib().sck_made_prepare(_ptr(self.params), self.groups, self._stream()))
 
     def get_params(self):
         return unflatten(self.masters().cpu().numpy())
@@ -100,7 +100,7 @@ class BlockProposal:
     def _workspace(self, batch: int) -> torch.Tensor:
         if batch not in self._ws:
             tb = ctypes.c_int64()
-            L.check(L.lib().sck_made_sizes(self.groups, batch, None, None, ctypes.byref(tb)))
+            abi.check(abi.lib().sck_made_sizes(self.groups, batch, None, None, ctypes.byref(tb)))
             self._ws[batch] = torch.empty(tb.value, dtype=torch.uint8, device=self.device)
         return self._ws[batch]
 
@@ -113,7 +113,7 @@ class BlockProposal:
             raise ValueError(f"spins must be int8 with {self.L}^3 sites per replica on {self.device}")
         out = torch.empty((R * self.nb ** 3, IN), dtype=torch.bfloat16, device=self.device)
         with torch.cuda.device(self.device):
-            L.check(L.lib().sck_made_gather(_ptr(S), R, self.L, _ptr(out), self._stream()))
+            abi.check(abi.lib().sck_made_gather(_ptr(S), R, self.L, _ptr(out), self._stream()))
         return out
 
     def forward(self, x: torch.Tensor):
@@ -122,8 +122,8 @@ class BlockProposal:
         logits = torch.empty((n, SPINS), dtype=torch.float32, device=self.device)
         logq = torch.empty(n, dtype=torch.float32, device=self.device)
         with torch.cuda.device(self.device):
-            L.check(L.lib().sck_made_forward(_ptr(self.params), self.groups, _ptr(x.contiguous()), n, _ptr(logits),
-                                             _ptr(logq), _ptr(self._workspace(n)), self._stream()))
+            abi.check(abi.lib().sck_made_forward(_ptr(self.params), self.groups, _ptr(x.contiguous()), n,
+                                                 _ptr(logits), _ptr(logq), _ptr(self._workspace(n)), self._stream()))
         return logits, logq
 
     def grads(self, x: torch.Tensor):
@@ -132,12 +132,12 @@ class BlockProposal:
         g = torch.empty(NPARAM, dtype=torch.float32, device=self.device)
         loss = torch.empty(1, dtype=torch.float32, device=self.device)
         with torch.cuda.device(self.device):
-            L.check(L.lib().sck_made_grads(_ptr(self.params), self.groups, _ptr(x.contiguous()), n, _ptr(g), _ptr(loss),
-                                           _ptr(self._workspace(n)), self._stream()))
+            abi.check(abi.lib().sck_made_grads(_ptr(self.params), self.groups, _ptr(x.contiguous()), n, _ptr(g),
+                                               _ptr(loss), _ptr(self._workspace(n)), self._stream()))
         return float(loss.item()), unflatten(g.cpu().numpy())
 
     def train(self, data: torch.Tensor, steps: int, batch: int = 8192, lr: float = 1e-3, betas=(0.9, 0.999),
-              eps: float = 1e-8, seed: int = 0, log_every: int = 0):
+              eps: float = 1e-8, seed: int = 0):
         """Adam on minibatches drawn (without replacement within an epoch) from `data` rows; returns the loss of
         every step (one device-to-host read at the end)."""
         n = data.shape[0]
@@ -158,9 +158,9 @@ class BlockProposal:
                 torch.index_select(data, 0, perm[pos:pos + batch], out=xb)
                 pos += batch
                 self.t += 1
-                L.check(L.lib().sck_made_train_step(_ptr(self.params), _ptr(self.adam), self.groups, _ptr(xb), batch,
-                                                    lr, betas[0], betas[1], eps, self.t, _ptr(losses[i:i + 1]),
-                                                    _ptr(ws), self._stream()))
+                abi.check(abi.lib().sck_made_train_step(_ptr(self.params), _ptr(self.adam), self.groups, _ptr(xb),
+                                                        batch, lr, betas[0], betas[1], eps, self.t,
+                                                        _ptr(losses[i:i + 1]), _ptr(ws), self._stream()))
         return losses.cpu().numpy()
 
     # ------------------------------------------------------------------ sampling
@@ -168,9 +168,9 @@ class BlockProposal:
                     accepted: torch.Tensor | None = None, record: torch.Tensor | None = None) -> None:
         """One colour step in place on int8 spins of this proposal's R replicas (beta: FP32 per replica)."""
         with torch.cuda.device(self.device):
-            L.check(L.lib().sck_made_colour_step(_ptr(self.params), self.groups, _ptr(spins), self.R, self.L,
-                                                 _ptr(beta), int(colour), int(seed), int(rnd), _ptr(accepted),
-                                                 _ptr(record), self._stream()))
+            abi.check(abi.lib().sck_made_colour_step(_ptr(self.params), self.groups, _ptr(spins), self.R, self.L,
+                                                     _ptr(beta), int(colour), int(seed), int(rnd), _ptr(accepted),
+                                                     _ptr(record), self._stream()))
 
     def round(self, spins: torch.Tensor, beta: torch.Tensor, seed: int, rnd: int,
               accepted: torch.Tensor | None = None) -> None:

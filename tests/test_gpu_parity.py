@@ -214,24 +214,29 @@ def test_specialised_and_generic_kernels_agree(name):
         assert frac <= 0.02
 
 
-ROW_SYSTEMS = {
+SEG_SYSTEMS = {
     "heis_bcc_j1j2_64x8x6": lambda: sy.System("Heisenberg bcc J1-J2", 3, cr.make("bcc", (1, 2)), (64, 8, 6),
                                               (True,) * 3, {1: 1.0, 2: 0.3}, h=(0.0, 0.0, 0.1),
                                               cubic_k1=np.full((2, 6, 8, 64), 0.05, np.float32)),
     "heis_sc_128x4x4": lambda: sy.System("Heisenberg sc", 3, cr.make("sc"), (128, 4, 4), (True,) * 3, {1: -1.0}),
     "heis_sc_64x6x4": lambda: sy.System("Heisenberg sc", 3, cr.make("sc"), (64, 6, 4), (True,) * 3, {1: 1.0},
                                         h=(0.2, 0.0, 0.0)),
+    # odd L2: ten colours, two per row, warps mixing both class offsets
+    "heis_sc_64x5x4": lambda: sy.System("Heisenberg sc", 3, cr.make("sc"), (64, 5, 4), (True,) * 3, {1: 1.0}),
     "xy_square_128x10": lambda: sy.System("XY square", 2, cr.make("square"), (128, 10), (True, True), {1: 1.0},
                                           h=(0.05, 0.0)),
+    "xy_square_24x7": lambda: sy.System("XY square", 2, cr.make("square"), (24, 7), (True, True), {1: 1.0}),
 }
 
 
-@pytest.mark.parametrize("name", sorted(ROW_SYSTEMS))
-def test_row_kernels_equal_lattice_kernels(name):
-    """Row kernels (contiguous row pairs, shuffles for x-neighbours, one and two segments per row) run the same
-    float32x2 arithmetic as the lattice kernels: spins bit-identical, odd replica count included."""
+@pytest.mark.parametrize("name", sorted(SEG_SYSTEMS))
+def test_segment_kernels_agree_with_lattice_kernels(name):
+    """Segment kernels (four sites of an 8-site x-segment per thread, 128-bit row loads) sum the local field in
+    row order instead of bond order, so spins agree with the lattice kernels to float32 rounding: per-spin
+    |delta| <= 1e-5 except on the rare attempts whose accept decision flips (at most 0.1 %), odd replica count
+    included."""
     from spin_colour_kernel_b200.sampler import Sampler
-    s = ROW_SYSTEMS[name]()
+    s = SEG_SYSTEMS[name]()
     B = 5
     A, R = Sampler(s, B, device="cuda", seed=3), Sampler(s, B, device="cuda", seed=3)
     pa, pr = A.tune(2, 0, 0), R.tune(1, 0, 0)
@@ -242,7 +247,8 @@ def test_row_kernels_equal_lattice_kernels(name):
     S2 = S1.clone()
     A.sweep(S1, 3)
     R.sweep(S2, 3)
-    assert torch.equal(S1, S2)
+    d = (S1 - S2).abs().amax(dim=1).cpu().numpy()       # per site and replica, over components
+    assert np.mean(d > 1e-5) <= 1e-3, np.mean(d > 1e-5)
     assert not torch.equal(S1, A.init_spins(seed=7))
 
 
