@@ -439,7 +439,19 @@ __global__ void gather_kernel(const int8_t* __restrict__ spins, int R, int L, __
 constexpr int XS = IN + 8;     // shared row strides (bfloat16): conflict-free ldmatrix rows
 constexpr int HS = H + 8;
 constexpr int WARP_SMEM = 16 * XS * 2 + 3 * 16 * HS * 2;
-constexpr int STEP_WARPS = 7;
+constexpr int STEP_WARPS = 5;
+
+// The weights one autoregressive step reads, staged per block of threads: rows [u0, u0 + 8 NT) of W1 (all 160
+// columns) and of W2, W3 (the 16 nkt columns of degree <= g), rows [S g, S g + 8) of W4.
+template <int G>
+struct Slice {
+  static constexpr int U = H / G, S = NSP / G, NT = U >= 8 ? U / 8 : 1, NR = 8 * NT;
+  static constexpr int W1 = 0, W2 = NR * XS, W3 = W2 + NR * HS, W4 = W3 + NR * HS, ELEMS = W4 + 8 * HS;
+  static constexpr int BYTES = ELEMS * 2;
+};
+
+template <int G>
+constexpr int step_smem() { return STEP_WARPS * WARP_SMEM + 2 * Slice<G>::BYTES; }
 
 struct StepParams {
   const __nv_bfloat16* W[4];
@@ -454,52 +466,106 @@ struct StepParams {
 
 __device__ __forceinline__ float log_sigmoid(float t) { return -(fmaxf(-t, 0.f) + __logf(1.f + __expf(-fabsf(t)))); }
 
-// one layer's new units [u0, u0 + 8 NT) over input k-tiles [0, nkt): acc = bias + A[16 x 16 nkt] W^T
+__device__ __forceinline__ void ldsm_x2(uint32_t& r0, uint32_t& r1, const void* p) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0,%1}, [%2];\n" : "=r"(r0), "=r"(r1) : "r"(smem_u32(p)));
+}
+
+// all threads of the block: copy step g's weight slice into `dst` (cp.async, committed as one group)
+template <int G>
+__device__ __forceinline__ void load_slice(__nv_bfloat16* dst, const StepParams& p, int g) {
+  using SL = Slice<G>;
+  const int u0 = g * SL::U;
+  const int nkt = (SL::U * (g + 1) + 15) / 16;
+  const int c1 = IN / 8, ch = 2 * nkt;
+  const int n1 = SL::NR * c1, n2 = SL::NR * ch, n4 = 8 * ch;
+  const int total = n1 + 2 * n2 + n4;
+  for (int i = threadIdx.x; i < total; i += blockDim.x) {
+    const __nv_bfloat16* src;
+    __nv_bfloat16* d;
+    if (i < n1) {
+      const int r = i / c1, c = i - r * c1;
+      src = p.W[0] + (long long)(u0 + r) * IN + c * 8;
+      d = dst + SL::W1 + r * XS + c * 8;
+    } else if (i < n1 + 2 * n2) {
+      const int j = i - n1, l = j < n2 ? 1 : 2, jj = j - (l - 1) * n2;
+      const int r = jj / ch, c = jj - r * ch;
+      src = (l == 1 ? p.W[1] : p.W[2]) + (long long)(u0 + r) * H + c * 8;
+      d = dst + (l == 1 ? SL::W2 : SL::W3) + r * HS + c * 8;
+    } else {
+      const int j = i - n1 - 2 * n2, r = j / ch, c = j - r * ch;
+      src = p.W[3] + (long long)(g * SL::S + r) * H + c * 8;
+      d = dst + SL::W4 + r * HS + c * 8;
+    }
+    cp_async16(d, src, 16);
+  }
+  cp_async_commit();
+}
+
 template <int NT>
-__device__ __forceinline__ void step_units(float (&acc)[NT][4], const __nv_bfloat16* A, int lda,
-                                           const __nv_bfloat16* __restrict__ W, int K, const float* __restrict__ bias,
-                                           int nbias, int u0, int nkt, int lane) {
-  const int gr = lane >> 2, q = lane & 3;
+__device__ __forceinline__ void stage_tile(float (&c)[NT][4], const __nv_bfloat16* arow, const __nv_bfloat16* B,
+                                           int ldb, int k, int lane) {
+  uint32_t a[4];
+  ldsm_x4(a, arow + k * 16);
+  if constexpr (NT == 2) {
+    uint32_t b[4];
+    ldsm_x4(b, B + ((lane >> 4) * 8 + (lane & 7)) * ldb + k * 16 + ((lane >> 3) & 1) * 8);
+    mma_bf16(c[0], a, b[0], b[1]);
+    mma_bf16(c[1], a, b[2], b[3]);
+  } else {
+    uint32_t b0, b1;
+    ldsm_x2(b0, b1, B + (lane & 7) * ldb + k * 16 + ((lane >> 3) & 1) * 8);
+    mma_bf16(c[0], a, b0, b1);
+  }
+}
+
+// one layer's new units of a 16-row tile: acc = bias + A[16 x 16 nkt] B^T, B rows in shared memory (row-major
+// [unit][k]); even and odd k-tiles accumulate separately to halve the MMA chain
+template <int NT>
+__device__ __forceinline__ void stage(float (&acc)[NT][4], const __nv_bfloat16* A, int lda, const __nv_bfloat16* B,
+                                      int ldb, const float* __restrict__ bias, int nbias, int u0, int nkt, int lane) {
+  const int q = lane & 3;
+  float acc2[NT][4];
 #pragma unroll
   for (int t = 0; t < NT; ++t) {
     const int n = u0 + t * 8 + 2 * q;   // columns past the layer (last tiles of small U) are computed and dropped
     const float b0 = n < nbias ? bias[n] : 0.f, b1 = n + 1 < nbias ? bias[n + 1] : 0.f;
-    acc[t][0] = b0;
-    acc[t][1] = b1;
-    acc[t][2] = b0;
-    acc[t][3] = b1;
-  }
-  for (int kt = 0; kt < nkt; ++kt) {
-    uint32_t a[4];
-    ldsm_x4(a, A + ((lane & 7) + ((lane >> 3) & 1) * 8) * lda + kt * 16 + (lane >> 4) * 8);
+    acc[t][0] = acc[t][2] = b0;
+    acc[t][1] = acc[t][3] = b1;
 #pragma unroll
-    for (int t = 0; t < NT; ++t) {
-      const __nv_bfloat16* w = W + (long long)(u0 + t * 8 + gr) * K + kt * 16 + 2 * q;
-      const uint32_t b0 = __ldg((const unsigned int*)w), b1 = __ldg((const unsigned int*)(w + 8));
-      mma_bf16(acc[t], a, b0, b1);
-    }
+    for (int e = 0; e < 4; ++e) acc2[t][e] = 0.f;
   }
+  const __nv_bfloat16* arow = A + ((lane & 7) + ((lane >> 3) & 1) * 8) * lda + (lane >> 4) * 8;
+  for (int kt = 0; kt < nkt; kt += 2) {
+    stage_tile<NT>(acc, arow, B, ldb, kt, lane);
+    if (kt + 1 < nkt) stage_tile<NT>(acc2, arow, B, ldb, kt + 1, lane);
+  }
+#pragma unroll
+  for (int t = 0; t < NT; ++t)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) acc[t][e] += acc2[t][e];
 }
+
+__device__ __forceinline__ int wrap_block(int v, int L) { return v < 0 ? v + L : (v >= L ? v - L : v); }
 
 template <int G>
 __global__ void __launch_bounds__(32 * STEP_WARPS) step_kernel(StepParams p) {
-  constexpr int U = H / G;                  // hidden units of one degree
-  constexpr int S = NSP / G;                // spins of one group
-  constexpr int NT = U >= 8 ? U / 8 : 1;    // n8 tiles per hidden stage
+  using SL = Slice<G>;
+  constexpr int U = SL::U, S = SL::S, NT = SL::NT;
   extern __shared__ __align__(16) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, gr = lane >> 2, q = lane & 3;
   __nv_bfloat16* X = (__nv_bfloat16*)(smem + warp * WARP_SMEM);
-  __nv_bfloat16* Hs[3];
-  for (int l = 0; l < 3; ++l) Hs[l] = X + 16 * XS + l * 16 * HS;
+  __nv_bfloat16* const H0 = X + 16 * XS;       // layer l's activations at H0 + l * 16 * HS
+  __nv_bfloat16* const slices = (__nv_bfloat16*)(smem + STEP_WARPS * WARP_SMEM);   // two buffers of ELEMS
   for (int i = lane; i < WARP_SMEM / 16; i += 32) ((uint4*)X)[i] = make_uint4(0, 0, 0, 0);
   __syncwarp();
 
   const long long tasks = (long long)p.R * p.nc;
-  const long long wtasks = (tasks + 7) / 8;
+  const long long ctasks = (tasks + 8 * STEP_WARPS - 1) / (8 * STEP_WARPS);   // 8 blocks per warp
   const int half = p.nb >> 1, L = p.L;
-  for (long long wt = (long long)blockIdx.x * STEP_WARPS + warp; wt < wtasks; wt += (long long)gridDim.x * STEP_WARPS) {
+  if ((long long)blockIdx.x < ctasks) load_slice<G>(slices, p, 0);
+  for (long long ct = blockIdx.x; ct < ctasks; ct += gridDim.x) {
     // ---- block r = gr of this warp (lanes 4r..4r+3): rows r (proposal) and r + 8 (current spins)
-    const long long task = wt * 8 + gr;
+    const long long task = (ct * STEP_WARPS + warp) * 8 + gr;
     const bool valid = task < tasks;
     const int rep = valid ? (int)(task / p.nc) : 0;
     const int k = valid ? (int)(task % p.nc) : 0;
@@ -511,8 +577,8 @@ __global__ void __launch_bounds__(32 * STEP_WARPS) step_kernel(StepParams p) {
     for (int col = q; col < IN; col += 4) {
       float s = 0.f;
       if (valid) {
-        const int x = (x0 + c_tab.in_off[col][0] + L) % L, y = (y0 + c_tab.in_off[col][1] + L) % L,
-                  z = (z0 + c_tab.in_off[col][2] + L) % L;
+        const int x = wrap_block(x0 + c_tab.in_off[col][0], L), y = wrap_block(y0 + c_tab.in_off[col][1], L),
+                  z = wrap_block(z0 + c_tab.in_off[col][2], L);
         s = (float)base[((long long)z * L + y) * L + x];
       }
       const __nv_bfloat16 v = __float2bfloat16_rn(s);
@@ -525,38 +591,47 @@ __global__ void __launch_bounds__(32 * STEP_WARPS) step_kernel(StepParams p) {
     Philox4 rnd{0, 0, 0, 0};
     int rnd_w = -1;
     for (int g = 0; g < G; ++g) {
+      cp_async_wait<0>();
+      __syncthreads();   // slice g has landed; every warp is done with the other buffer
+      const bool more = ct + gridDim.x < ctasks;
+      __nv_bfloat16* const next = slices + ((g + 1) & 1) * SL::ELEMS;
+      if (g + 1 < G) load_slice<G>(next, p, g + 1);
+      else if (more) load_slice<G>(next, p, 0);
+      const __nv_bfloat16* sl = slices + (g & 1) * SL::ELEMS;
+      const int nkt = (U * (g + 1) + 15) / 16;    // hidden units of degree <= g
       // layer 1: inputs of degree <= g are the boundary and the spins of groups < g
       {
         float acc[NT][4];
-        step_units<NT>(acc, X, XS, p.W[0], IN, p.bias[0], H, g * U, (NBD + S * g + 15) / 16, lane);
+        stage<NT>(acc, X, XS, sl + SL::W1, XS, p.bias[0], H, g * U, (NBD + S * g + 15) / 16, lane);
 #pragma unroll
         for (int t = 0; t < NT; ++t) {
           const int c = g * U + t * 8 + 2 * q;
           if (2 * q < U) {
-            *(uint32_t*)(Hs[0] + gr * HS + c) = pack_bf16(fmaxf(acc[t][0], 0.f), fmaxf(acc[t][1], 0.f));
-            *(uint32_t*)(Hs[0] + (gr + 8) * HS + c) = pack_bf16(fmaxf(acc[t][2], 0.f), fmaxf(acc[t][3], 0.f));
+            *(uint32_t*)(H0 + gr * HS + c) = pack_bf16(fmaxf(acc[t][0], 0.f), fmaxf(acc[t][1], 0.f));
+            *(uint32_t*)(H0 + (gr + 8) * HS + c) = pack_bf16(fmaxf(acc[t][2], 0.f), fmaxf(acc[t][3], 0.f));
           }
         }
       }
       __syncwarp();
-      const int nkt = (U * (g + 1) + 15) / 16;    // hidden units of degree <= g
 #pragma unroll
       for (int l = 1; l < 3; ++l) {
         float acc[NT][4];
-        step_units<NT>(acc, Hs[l - 1], HS, p.W[l], H, p.bias[l], H, g * U, nkt, lane);
+        stage<NT>(acc, H0 + (l - 1) * 16 * HS, HS, sl + (l == 1 ? SL::W2 : SL::W3), HS, p.bias[l], H, g * U, nkt,
+                  lane);
 #pragma unroll
         for (int t = 0; t < NT; ++t) {
           const int c = g * U + t * 8 + 2 * q;
           if (2 * q < U) {
-            *(uint32_t*)(Hs[l] + gr * HS + c) = pack_bf16(fmaxf(acc[t][0], 0.f), fmaxf(acc[t][1], 0.f));
-            *(uint32_t*)(Hs[l] + (gr + 8) * HS + c) = pack_bf16(fmaxf(acc[t][2], 0.f), fmaxf(acc[t][3], 0.f));
+            *(uint32_t*)(H0 + l * 16 * HS + gr * HS + c) = pack_bf16(fmaxf(acc[t][0], 0.f), fmaxf(acc[t][1], 0.f));
+            *(uint32_t*)(H0 + l * 16 * HS + (gr + 8) * HS + c) =
+                pack_bf16(fmaxf(acc[t][2], 0.f), fmaxf(acc[t][3], 0.f));
           }
         }
         __syncwarp();
       }
       // logits of group g (positions S g .. S g + S - 1 in the first columns of one n8 tile)
       float lo[1][4];
-      step_units<1>(lo, Hs[2], HS, p.W[3], H, p.bias[3], NSP, g * S, nkt, lane);
+      stage<1>(lo, H0 + 2 * 16 * HS, HS, sl + SL::W4, HS, p.bias[3], NSP, g * S, nkt, lane);
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         const int j = 2 * q + e;
@@ -567,7 +642,8 @@ __global__ void __launch_bounds__(32 * STEP_WARPS) step_kernel(StepParams p) {
             rnd = philox4x32_10((uint32_t)(int32_t)(17 * uid + w), 0u, p.k0, p.k1);
             rnd_w = w;
           }
-          const uint32_t bits = (pos & 3) == 0 ? rnd.x0 : (pos & 3) == 1 ? rnd.x1 : (pos & 3) == 2 ? rnd.x2 : rnd.x3;
+          const int o = pos & 3;
+          const uint32_t bits = o == 0 ? rnd.x0 : (o == 1 ? rnd.x1 : (o == 2 ? rnd.x2 : rnd.x3));
           const float u = to_uniform(bits);
           const float ln = lo[0][e], lc = lo[0][2 + e];
           const float xn = u < 1.f / (1.f + __expf(-ln)) ? 1.f : -1.f;
@@ -638,6 +714,7 @@ __global__ void __launch_bounds__(32 * STEP_WARPS) step_kernel(StepParams p) {
     }
     __syncwarp();
   }
+  cp_async_wait<0>();
 }
 
 // ======================================================================================= workspace layout
@@ -919,23 +996,21 @@ int sck_made_colour_step(const void* params, int32_t groups, int8_t* spins, int3
   p.accepted = accepted;
   p.record = (unsigned char*)record;
   cudaStream_t s = (cudaStream_t)stream;
-  const long long wtasks = ((long long)R * p.nc + 7) / 8;
+  const long long ctasks = ((long long)R * p.nc + 8 * STEP_WARPS - 1) / (8 * STEP_WARPS);
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  long long grid = (wtasks + STEP_WARPS - 1) / STEP_WARPS;
-  if (grid > sms) grid = sms;
-  const int smem = STEP_WARPS * WARP_SMEM;
+  const long long grid = ctasks < sms ? ctasks : sms;
   if (groups == 16) {
-    rc = cuda_status(cudaFuncSetAttribute(step_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
-                     "made step smem");
+    rc = cuda_status(cudaFuncSetAttribute(step_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          step_smem<16>()), "made step smem");
     if (rc) return rc;
-    step_kernel<16><<<(unsigned)grid, 32 * STEP_WARPS, smem, s>>>(p);
+    step_kernel<16><<<(unsigned)grid, 32 * STEP_WARPS, step_smem<16>(), s>>>(p);
   } else {
-    rc = cuda_status(cudaFuncSetAttribute(step_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
-                     "made step smem");
+    rc = cuda_status(cudaFuncSetAttribute(step_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          step_smem<64>()), "made step smem");
     if (rc) return rc;
-    step_kernel<64><<<(unsigned)grid, 32 * STEP_WARPS, smem, s>>>(p);
+    step_kernel<64><<<(unsigned)grid, 32 * STEP_WARPS, step_smem<64>(), s>>>(p);
   }
   return cuda_status(cudaGetLastError(), "made colour step");
 }

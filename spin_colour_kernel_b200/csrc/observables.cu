@@ -10,6 +10,7 @@
 #include <string>
 
 #include "internal.h"
+#include "spec.cuh"
 
 namespace sck {
 
@@ -102,6 +103,137 @@ __global__ void __launch_bounds__(256) observables_kernel(const __grid_constant_
   }
 }
 
+// Systems with a compile-time bond table (lattices.h): every neighbour offset is a constant and each bond is
+// visited once, from the end for which it points "forward" (to a higher sublattice, or within a sublattice to a
+// positive offset in z, then y, then x); its reverse sits in the partner's table with the same coupling, so
+// E = -sum_bonds J s_i . s_j - h . sum s + anisotropy equals -1/2 sum_i s_i . v_i of the generic kernel up to
+// FP64 rounding, at half the neighbour reads. Still FP64 throughout.
+template <class Lat, int A>
+__host__ __device__ constexpr bool forward_bond(int i) {
+  const BondC b = Lat::bond(A, i);
+  if (b.a2 != A) return b.a2 > A;
+  if (b.dz != 0) return b.dz > 0;
+  if (b.dy != 0) return b.dy > 0;
+  return b.dx > 0;
+}
+
+template <class Lat>
+__host__ __device__ constexpr bool bonds_paired() {
+  for (int a = 0; a < Lat::b; ++a)
+    for (int i = 0; i < Lat::n_bonds(a); ++i) {
+      const BondC b = Lat::bond(a, i);
+      bool found = false;
+      for (int j = 0; j < Lat::n_bonds(b.a2); ++j) {
+        const BondC r = Lat::bond(b.a2, j);
+        if (r.a2 == a && r.dx == -b.dx && r.dy == -b.dy && r.dz == -b.dz) {
+          int gi = 0, gj = 0;
+          while (Lat::group_end(a, gi) <= i) ++gi;
+          while (Lat::group_end(b.a2, gj) <= j) ++gj;
+          found = found || gi == gj;
+        }
+      }
+      if (!found) return false;
+    }
+  return true;
+}
+
+__device__ __forceinline__ bool step_axis(int& v, int d, int L, int per) {
+  v += d;
+  if (v < 0) {
+    if (!per) return false;
+    v += L;
+  } else if (v >= L) {
+    if (!per) return false;
+    v -= L;
+  }
+  return true;
+}
+
+template <class Lat, int N, int STORE>
+__global__ void __launch_bounds__(256) observables_spec_kernel(const __grid_constant__ ObsParams p) {
+  static_assert(bonds_paired<Lat>(), "every bond needs its reverse in the partner's table");
+  const Geometry& g = p.g;
+  const int rep = blockIdx.y;
+  constexpr int NV = 1 + SCK_MAX_BASIS * N;
+  double acc[NV];
+#pragma unroll
+  for (int i = 0; i < NV; ++i) acc[i] = 0.0;
+  // four sites per iteration: their loads and FP64 chains overlap
+#pragma unroll 4
+  for (int site = blockIdx.x * blockDim.x + threadIdx.x; site < g.nsite; site += p.blocks_per_rep * blockDim.x) {
+    if (p.mask != nullptr && p.mask[site] == 0) continue;
+    const int alpha = (int)fdiv((uint32_t)site, p.fd_plane);
+    const int rem = site - alpha * g.plane;
+    const int row = (int)fdiv((uint32_t)rem, p.fd_L1);
+    const int x = rem - row * g.L1;
+    const int z = (int)fdiv((uint32_t)row, p.fd_L2);
+    const int y = row - z * g.L2;
+    double s[N];
+    load_spin<N, STORE>(p, rep, site, s);
+    double e = 0.0;
+    static_for<0, Lat::b>([&](auto ac) {
+      constexpr int a = decltype(ac)::value;
+      if (a != alpha) return;
+      const SubObs& ob = p.obs[a];
+      static_for<0, Lat::n_bonds(a)>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        if constexpr (forward_bond<Lat, a>(i)) {
+          constexpr BondC bd = Lat::bond(a, i);
+          int x2 = x, y2 = y, z2 = z;
+          if (!step_axis(x2, bd.dx, g.L1, g.per[0]) || !step_axis(y2, bd.dy, g.L2, g.per[1])) return;
+          if (Lat::dim == 3 && !step_axis(z2, bd.dz, g.L3, g.per[2])) return;
+          const int q = bd.a2 * g.plane + (z2 * g.L2 + y2) * g.L1 + x2;
+          double t[N];
+          load_spin<N, STORE>(p, rep, q, t);
+          double dot = 0.0;
+#pragma unroll
+          for (int k = 0; k < N; ++k) dot += s[k] * t[k];
+          e -= ob.J[i] * dot;
+        }
+      });
+    });
+#pragma unroll
+    for (int k = 0; k < N; ++k) e -= p.h64[k] * s[k];
+    if constexpr (N == 3) {
+      if (g.has_cubic) {
+        const double k1 = (double)p.k1[site];
+        const double xy = s[0] * s[1], xz = s[0] * s[2], yz = s[1] * s[2], xyz = s[0] * s[1] * s[2];
+        e += k1 * (xy * xy + xz * xz + yz * yz) + p.k2 * xyz * xyz;
+      }
+    }
+    acc[0] += e;
+#pragma unroll
+    for (int a = 0; a < SCK_MAX_BASIS; ++a)
+      if (a == alpha) {
+#pragma unroll
+        for (int k = 0; k < N; ++k) acc[1 + a * N + k] += s[k];
+      }
+  }
+  __shared__ double red[NV][8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    double v = acc[i];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, off);
+    if (lane == 0) red[i][warp] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    double v = 0.0;
+    for (int wi = 0; wi < (int)(blockDim.x >> 5); ++wi) v += red[threadIdx.x][wi];
+    p.partial[((size_t)rep * p.blocks_per_rep + blockIdx.x) * OBS_VALUES + threadIdx.x] = v;
+  }
+}
+
+template <class Lat>
+static void launch_obs_spec(const ObsParams& p, dim3 grid, cudaStream_t s) {
+  if (p.storage == 0) observables_spec_kernel<Lat, 1, 0><<<grid, 256, 0, s>>>(p);
+  else if (p.g.n == 1) observables_spec_kernel<Lat, 1, 1><<<grid, 256, 0, s>>>(p);
+  else if (p.g.n == 2) observables_spec_kernel<Lat, 2, 1><<<grid, 256, 0, s>>>(p);
+  else observables_spec_kernel<Lat, 3, 1><<<grid, 256, 0, s>>>(p);
+}
+
 // Sum the partials of every replica in block order; E[r] and M[r][alpha][k] (B x b x n).
 __global__ void observables_finish(const double* __restrict__ partial, int B, int blocks_per_rep, int b, int n,
                                    double* __restrict__ E, double* __restrict__ M) {
@@ -147,7 +279,18 @@ int launch_observables(const sck_plan* plan, const void* spins, int storage, int
   p.partial = (double*)workspace;
   dim3 grid(p.blocks_per_rep, p.B);
   const int n = plan->geom.n;
-  if (p.storage == 2) observables_kernel<1, 2><<<grid, 256, 0, s>>>(p);
+  // the lattice table fixes the bonds of int8 and float32 storage (packed storage reads the generic way)
+  const bool spec = plan->spec != 0 && p.storage != 2;
+  if (spec) {
+    switch (plan->spec) {
+      case Lat_square_1::id: launch_obs_spec<Lat_square_1>(p, grid, s); break;
+      case Lat_triangular_1::id: launch_obs_spec<Lat_triangular_1>(p, grid, s); break;
+      case Lat_sc_1::id: launch_obs_spec<Lat_sc_1>(p, grid, s); break;
+      case Lat_bcc_1::id: launch_obs_spec<Lat_bcc_1>(p, grid, s); break;
+      case Lat_bcc_1_2::id: launch_obs_spec<Lat_bcc_1_2>(p, grid, s); break;
+      default: launch_obs_spec<Lat_fcc_1>(p, grid, s); break;
+    }
+  } else if (p.storage == 2) observables_kernel<1, 2><<<grid, 256, 0, s>>>(p);
   else if (p.storage == 0) observables_kernel<1, 0><<<grid, 256, 0, s>>>(p);
   else if (n == 1) observables_kernel<1, 1><<<grid, 256, 0, s>>>(p);
   else if (n == 2) observables_kernel<2, 1><<<grid, 256, 0, s>>>(p);

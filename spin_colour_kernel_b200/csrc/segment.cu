@@ -1,15 +1,15 @@
 // Segment kernels: the class update of vector models (n = 2, 3) on a periodic box with a compile-time bond
 // table (lattices.h) and a colouring whose classes alternate along x (x-period 2).
 //
-// A thread owns an aligned 8-site x-segment of one row of one replica, whose four sites of the class sit at
-// x0 + d, x0 + d + 2, x0 + d + 4, x0 + d + 6 (d = 0 or 1 by row). For every distinct neighbour row of the
-// sublattice's bond table (own row first) it loads the segment of each component with two 128-bit loads, plus
-// the one site past either end that an x-offset of -1 or +1 reaches, and adds each bond's neighbour to the
-// coupling-group sum of all four sites in packed float32x2 arithmetic. Compared with one site per thread this
-// cuts load instructions about 2.5x, reads whole 32-byte sectors, and shares the row addressing between four
-// sites. The group sums run in row order rather than the reference's bond order, so local fields differ from
-// the reference's by float32 rounding only; the proposal, energy change and acceptance keep the reference's
-// operation order (finish_core in spec.cuh). Lanes are mapped to rows so that the rows of a warp share d
+// A thread owns an aligned 4-site x-segment of one row of one replica, whose two sites of the class sit at
+// x0 + d and x0 + d + 2 (d = 0 or 1 by row). For every distinct neighbour row of the sublattice's bond table
+// (own row first) it loads the segment of each component with one 128-bit load (the lanes of a warp read
+// consecutive 16-byte pieces of a row, so every sector fetched is used whole), plus the one site past either
+// end that an x-offset of -1 or +1 reaches, and adds each bond's neighbour to the coupling-group sums of both
+// sites in packed float32x2 arithmetic. Compared with one site and two replicas per thread this halves the load
+// instructions and shares the row addressing between the two sites. The group sums run in row order rather than
+// the reference's bond order, so local fields differ from the reference's by float32 rounding only; the
+// proposal, energy change and acceptance keep the reference's operation order (finish_core in spec.cuh). Lanes are mapped to rows so that the rows of a warp share d
 // (rows of one y parity are consecutive), which keeps the two compile-time variants of a warp from diverging.
 #include "spec.cuh"
 
@@ -71,7 +71,7 @@ struct SegRows {
 
 __device__ __forceinline__ int wrap1(int v, int L) { return v < 0 ? v + L : (v >= L ? v - L : v); }
 
-// the four class sites x0 + D + 2j of row (y, z), sublattice A, replica rep
+// the two class sites x0 + D and x0 + D + 2 of row (y, z), sublattice A, replica rep
 template <class Lat, int A, int N, int D>
 __device__ __forceinline__ void seg_sites(const Common& c, const float (&J)[SCK_MAX_GROUPS], int rep, int y, int z,
                                           int x0, int32_t key) {
@@ -80,12 +80,14 @@ __device__ __forceinline__ void seg_sites(const Common& c, const float (&J)[SCK_
   const size_t NS = (size_t)g.nsite;
   const float* base = (const float*)c.src + (size_t)rep * N * NS;
   float* obase = (float*)c.dst + (size_t)rep * N * NS;
-  float2 gs[Lat::groups][N][2];
+  float2 gs[Lat::groups][N];
 #pragma unroll
   for (int gi = 0; gi < Lat::groups; ++gi)
 #pragma unroll
-    for (int k = 0; k < N; ++k) gs[gi][k][0] = gs[gi][k][1] = f2(0.0f);
-  float2 s[N][2];
+    for (int k = 0; k < N; ++k) gs[gi][k] = f2(0.0f);
+  float2 s[N];
+  const int xl = x0 == 0 ? g.L1 - 1 : x0 - 1;
+  const int xr = x0 + 4 == g.L1 ? 0 : x0 + 4;
   static_for<0, R::count()>([&](auto rc) {
     constexpr int r = decltype(rc)::value;
     constexpr BondC row = R::row(r);
@@ -94,74 +96,56 @@ __device__ __forceinline__ void seg_sites(const Common& c, const float (&J)[SCK_
     const int yy = wrap1(y + row.dy, g.L2);
     const int zz = Lat::dim == 3 ? wrap1(z + row.dz, g.L3) : 0;
     const float* rp = base + (size_t)row.a2 * g.plane + ((size_t)zz * g.L2 + yy) * g.L1;
-    const int xl = x0 == 0 ? g.L1 - 1 : x0 - 1;
-    const int xr = x0 + 8 == g.L1 ? 0 : x0 + 8;
 #pragma unroll
     for (int k = 0; k < N; ++k) {
       const float* q = rp + k * NS;
-      const float4 lo = *(const float4*)(q + x0);
-      const float4 hi = *(const float4*)(q + x0 + 4);
-      float w[10] = {0.f, lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w, 0.f};
+      const float4 m = *(const float4*)(q + x0);
+      float w[6] = {0.f, m.x, m.y, m.z, m.w, 0.f};
       if (left) w[0] = q[xl];
-      if (right) w[9] = q[xr];
-      if constexpr (r == 0) {
-        s[k][0] = make_float2(w[1 + D], w[3 + D]);
-        s[k][1] = make_float2(w[5 + D], w[7 + D]);
-      }
+      if (right) w[5] = q[xr];
+      if constexpr (r == 0) s[k] = make_float2(w[1 + D], w[3 + D]);
       static_for<0, R::nb>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
         if constexpr (R::row_of_bond(i) == r) {
           constexpr int o = 1 + D + Lat::bond(A, i).dx;
           constexpr int gi = R::group_of(i);
-          gs[gi][k][0] = __fadd2_rn(gs[gi][k][0], make_float2(w[o], w[o + 2]));
-          gs[gi][k][1] = __fadd2_rn(gs[gi][k][1], make_float2(w[o + 4], w[o + 6]));
+          gs[gi][k] = __fadd2_rn(gs[gi][k], make_float2(w[o], w[o + 2]));
         }
       });
     }
   });
-  float2 v[N][2];
+  float2 v[N];
 #pragma unroll
-  for (int k = 0; k < N; ++k)
+  for (int k = 0; k < N; ++k) {
+    float2 acc = f2(0.0f);
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      float2 acc = f2(0.0f);
-#pragma unroll
-      for (int gi = 0; gi < Lat::groups; ++gi) acc = __fadd2_rn(acc, __fmul2_rn(f2(J[gi]), gs[gi][k][h]));
-      if (c.hnz[k]) acc = __fadd2_rn(acc, f2(c.h[k]));
-      v[k][h] = acc;
-    }
-  const int own0 = A * g.plane + (z * g.L2 + y) * g.L1 + x0 + D;
+    for (int gi = 0; gi < Lat::groups; ++gi) acc = __fadd2_rn(acc, __fmul2_rn(f2(J[gi]), gs[gi][k]));
+    if (c.hnz[k]) acc = __fadd2_rn(acc, f2(c.h[k]));
+    v[k] = acc;
+  }
+  const int oa = A * g.plane + (z * g.L2 + y) * g.L1 + x0 + D, ob = oa + 2;
   const float beta = c.beta[rep];
+  float2 t[N];
+  bool acc0, acc1;
+  finish_core<N>(c, counter_of(rep, g.nsite, oa), counter_of(rep, g.nsite, ob), true, oa, ob,
+                 make_float2(beta, beta), key, s, v, t, acc0, acc1);
+  float* po = obase + oa;
+  if (acc0) {
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const int oa = own0 + 4 * h, ob = oa + 2;
-    float2 sp[N], vp[N], tp[N];
+    for (int k = 0; k < N; ++k) po[k * NS] = t[k].x;
+  }
+  if (acc1) {
 #pragma unroll
-    for (int k = 0; k < N; ++k) {
-      sp[k] = s[k][h];
-      vp[k] = v[k][h];
-    }
-    bool acc0, acc1;
-    finish_core<N>(c, counter_of(rep, g.nsite, oa), counter_of(rep, g.nsite, ob), true, oa, ob,
-                   make_float2(beta, beta), key, sp, vp, tp, acc0, acc1);
-    float* po = obase + oa;
-    if (acc0) {
-#pragma unroll
-      for (int k = 0; k < N; ++k) po[k * NS] = tp[k].x;
-    }
-    if (acc1) {
-#pragma unroll
-      for (int k = 0; k < N; ++k) po[k * NS + 2] = tp[k].y;
-    }
+    for (int k = 0; k < N; ++k) po[k * NS + 2] = t[k].y;
   }
 }
 
-// Grid (ceil(rows * L1 / 8 / 256), n_tasks * units_per_task); block y-slot -> (task, replica).
+// Grid (ceil(rows * L1 / 4 / 256), n_tasks * units_per_task); block y-slot -> (task, replica).
 template <class Lat, int N>
 __global__ void __launch_bounds__(256) seg_kernel(const __grid_constant__ SpecParams p) {
   const Common& c = p.c;
   const Geometry& g = c.g;
-  const uint32_t segs = (uint32_t)(g.L1 >> 3);
+  const uint32_t segs = (uint32_t)(g.L1 >> 2);
   const uint32_t per = (uint32_t)g.L2 * (uint32_t)g.L3 * segs;
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= per) return;
@@ -170,7 +154,7 @@ __global__ void __launch_bounds__(256) seg_kernel(const __grid_constant__ SpecPa
   const int rep = task.rep_begin + (int)(blockIdx.y - ti * p.units_per_task);
   if (rep >= task.rep_end) return;
   const uint32_t rowi = fdiv(t, p.fd_segs);
-  const int x0 = (int)(t - rowi * segs) * 8;
+  const int x0 = (int)(t - rowi * segs) * 4;
   const int z = (int)fdiv(rowi, c.fd_L2);
   const int i = (int)rowi - z * g.L2;
   // rows of one y parity first (an even L2 keeps each half whole), so a warp's rows share the class offset
@@ -203,7 +187,7 @@ static constexpr bool lat_reach_one() {
 bool seg_kernel_ok(const sck_plan* plan) {
   const Geometry& g = plan->geom;
   if (!plan->row_kernels || plan->mode != SCK_MODE_F32 || g.n < 2 || g.has_mask || plan->P != 2) return false;
-  if (g.L1 % 8 != 0 || !g.per[0] || !g.per[1] || g.L2 < 3) return false;
+  if (g.L1 % 4 != 0 || !g.per[0] || !g.per[1] || g.L2 < 3) return false;
   if (g.dim == 3 && (!g.per[2] || g.L3 < 3)) return false;
   switch (plan->spec) {
     case Lat_square_1::id: return lat_reach_one<Lat_square_1>();
@@ -225,8 +209,8 @@ static void launch_seg_lat(const sck_plan* plan, const SpecParams& p, dim3 grid,
 
 int launch_seg_tasks(const sck_plan* plan, SpecParams& p, int ys, cudaStream_t s) {
   const Geometry& g = plan->geom;
-  const uint32_t per = (uint32_t)g.L2 * (uint32_t)g.L3 * (uint32_t)(g.L1 >> 3);
-  p.fd_segs = make_fastdiv((uint32_t)(g.L1 >> 3));
+  const uint32_t per = (uint32_t)g.L2 * (uint32_t)g.L3 * (uint32_t)(g.L1 >> 2);
+  p.fd_segs = make_fastdiv((uint32_t)(g.L1 >> 2));
   const dim3 grid((per + 255) / 256, (unsigned)ys);
   switch (plan->spec) {
     case Lat_square_1::id: launch_seg_lat<Lat_square_1>(plan, p, grid, s); break;

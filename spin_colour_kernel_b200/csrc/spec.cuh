@@ -21,7 +21,7 @@ struct SpecParams {
   float J[SCK_MAX_BASIS][SCK_MAX_GROUPS];
   int n_tasks;
   int units_per_task;     // grid.y slots per task (replicas, or replica pairs for vector models)
-  FastDiv fd_segs;        // segment kernels: 8-site segments per row
+  FastDiv fd_segs;        // segment kernels: 4-site segments per row
   Task tasks[kMaxTasks];
 };
 
