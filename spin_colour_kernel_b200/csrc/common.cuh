@@ -131,13 +131,12 @@ __device__ __forceinline__ Philox4 philox4x32_10(uint32_t c0, uint32_t c1, uint3
   uint32_t c2 = 0u, c3 = 0u;
 #pragma unroll
   for (int i = 0; i < 10; ++i) {
-    // one 32 x 32 -> 64-bit product per word gives both halves
-    const unsigned long long pa = (unsigned long long)0xD2511F53u * c0;
-    const unsigned long long pb = (unsigned long long)0xCD9E8D57u * c2;
-    c0 = (uint32_t)(pb >> 32) ^ c1 ^ k0;
-    c2 = (uint32_t)(pa >> 32) ^ c3 ^ k1;
-    c1 = (uint32_t)pb;
-    c3 = (uint32_t)pa;
+    const uint32_t lo_a = 0xD2511F53u * c0, hi_a = __umulhi(0xD2511F53u, c0);
+    const uint32_t lo_b = 0xCD9E8D57u * c2, hi_b = __umulhi(0xCD9E8D57u, c2);
+    c0 = hi_b ^ c1 ^ k0;
+    c2 = hi_a ^ c3 ^ k1;
+    c1 = lo_b;
+    c3 = lo_a;
     k0 += 0x9E3779B9u;
     k1 += 0xBB67AE85u;
   }

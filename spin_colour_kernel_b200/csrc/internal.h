@@ -33,42 +33,42 @@ struct Common {
   FastDiv fd_bx, fd_L1, fd_L2, fd_m[SCK_MAX_FACTORS];
 };
 
+// First x in [0, P) of row (y, z) whose site on sublattice `alpha` has colour `colour`, or L1 when the row holds
+// no site of the class. Along a row the colour has period P and each colour of the row appears at most once per
+// period, so stepping the per-factor residues through one period finds it.
+__device__ __forceinline__ int first_class_x(const Common& c, int colour, int alpha, int y, int z) {
+  int g[SCK_MAX_FACTORS];
+#pragma unroll
+  for (int r = 0; r < SCK_MAX_FACTORS; ++r) {
+    if (r < c.col.r) {
+      const uint32_t v = (uint32_t)(c.col.K[r][1] * y + c.col.K[r][2] * z + c.col.o[alpha][r]);
+      g[r] = (int)(v - fdiv(v, c.fd_m[r]) * (uint32_t)c.col.m[r]);
+    }
+  }
+  for (int q = 0; q < c.P; ++q) {
+    int idx = 0;
+#pragma unroll
+    for (int r = 0; r < SCK_MAX_FACTORS; ++r) {
+      if (r < c.col.r) {
+        idx = idx * c.col.m[r] + g[r];
+        g[r] += c.col.K[r][0];
+        if (g[r] >= c.col.m[r]) g[r] -= c.col.m[r];
+      }
+    }
+    if (idx == colour) return q;
+  }
+  return c.g.L1;
+}
+
 // (t = row * bx + j) -> class site (x, y, z) of class `colour` on sublattice `alpha`, false when the row holds
-// no site of the class. Along a row the colour has period P and each colour of the row appears at most once
-// per period, so the row's first site x0 is found by stepping the per-factor residues through one period.
+// no site of the class.
 __device__ __forceinline__ bool class_site(const Common& c, int colour, int alpha, uint32_t t, int& x, int& y,
                                            int& z) {
   const uint32_t row = fdiv(t, c.fd_bx);
   const int j = (int)(t - row * (uint32_t)c.bx);
   z = (int)fdiv(row, c.fd_L2);
   y = (int)row - z * c.g.L2;
-  int x0 = 0;
-  if (colour >= 0) {
-    int g[SCK_MAX_FACTORS];
-#pragma unroll
-    for (int r = 0; r < SCK_MAX_FACTORS; ++r) {
-      if (r < c.col.r) {
-        const uint32_t v = (uint32_t)(c.col.K[r][1] * y + c.col.K[r][2] * z + c.col.o[alpha][r]);
-        g[r] = (int)(v - fdiv(v, c.fd_m[r]) * (uint32_t)c.col.m[r]);
-      }
-    }
-    x0 = c.g.L1;
-    for (int q = 0; q < c.P; ++q) {
-      int idx = 0;
-#pragma unroll
-      for (int r = 0; r < SCK_MAX_FACTORS; ++r) {
-        if (r < c.col.r) {
-          idx = idx * c.col.m[r] + g[r];
-          g[r] += c.col.K[r][0];
-          if (g[r] >= c.col.m[r]) g[r] -= c.col.m[r];
-        }
-      }
-      if (idx == colour) {
-        x0 = q;
-        break;
-      }
-    }
-  }
+  const int x0 = colour >= 0 ? first_class_x(c, colour, alpha, y, z) : 0;
   x = x0 + c.P * j;
   return x < c.g.L1;
 }

@@ -6,11 +6,12 @@
 // (own row first) it loads the segment of each component with one 128-bit load (the lanes of a warp read
 // consecutive 16-byte pieces of a row, so every sector fetched is used whole), plus the one site past either
 // end that an x-offset of -1 or +1 reaches, and adds each bond's neighbour to the coupling-group sums of both
-// sites in packed float32x2 arithmetic. Compared with one site and two replicas per thread this halves the load
+// sites. Compared with one site and two replicas per thread this halves the load
 // instructions and shares the row addressing between the two sites. The group sums run in row order rather than
 // the reference's bond order, so local fields differ from the reference's by float32 rounding only; the
-// proposal, energy change and acceptance keep the reference's operation order (finish_core in spec.cuh). Lanes are mapped to rows so that the rows of a warp share d
-// (rows of one y parity are consecutive), which keeps the two compile-time variants of a warp from diverging.
+// proposal, energy change and acceptance keep the reference's operation order (finish_core in spec.cuh). Lanes
+// are mapped to rows so that the rows of a warp share d (rows of one y parity are consecutive), which keeps the
+// two compile-time variants of a warp from diverging.
 #include "spec.cuh"
 
 namespace sck {
@@ -80,11 +81,16 @@ __device__ __forceinline__ void seg_sites(const Common& c, const float (&J)[SCK_
   const size_t NS = (size_t)g.nsite;
   const float* base = (const float*)c.src + (size_t)rep * N * NS;
   float* obase = (float*)c.dst + (size_t)rep * N * NS;
-  float2 gs[Lat::groups][N];
+  const float* bk[N];   // component planes of the replica: each load is one 32-bit index off these
+#pragma unroll
+  for (int k = 0; k < N; ++k) bk[k] = base + k * NS;
+  // scalar group sums per site: the two sites of a pair sit two registers apart in a 128-bit load, so packing
+  // them for float32x2 adds would cost a move per add
+  float gs[Lat::groups][N][2];
 #pragma unroll
   for (int gi = 0; gi < Lat::groups; ++gi)
 #pragma unroll
-    for (int k = 0; k < N; ++k) gs[gi][k] = f2(0.0f);
+    for (int k = 0; k < N; ++k) gs[gi][k][0] = gs[gi][k][1] = 0.0f;
   float2 s[N];
   const int xl = x0 == 0 ? g.L1 - 1 : x0 - 1;
   const int xr = x0 + 4 == g.L1 ? 0 : x0 + 4;
@@ -95,21 +101,21 @@ __device__ __forceinline__ void seg_sites(const Common& c, const float (&J)[SCK_
     constexpr bool right = D == 1 && R::has_dx(r, 1);
     const int yy = wrap1(y + row.dy, g.L2);
     const int zz = Lat::dim == 3 ? wrap1(z + row.dz, g.L3) : 0;
-    const float* rp = base + (size_t)row.a2 * g.plane + ((size_t)zz * g.L2 + yy) * g.L1;
+    const int ro = row.a2 * g.plane + (zz * g.L2 + yy) * g.L1;
 #pragma unroll
     for (int k = 0; k < N; ++k) {
-      const float* q = rp + k * NS;
-      const float4 m = *(const float4*)(q + x0);
+      const float4 m = *(const float4*)(bk[k] + ro + x0);
       float w[6] = {0.f, m.x, m.y, m.z, m.w, 0.f};
-      if (left) w[0] = q[xl];
-      if (right) w[5] = q[xr];
+      if (left) w[0] = bk[k][ro + xl];
+      if (right) w[5] = bk[k][ro + xr];
       if constexpr (r == 0) s[k] = make_float2(w[1 + D], w[3 + D]);
       static_for<0, R::nb>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
         if constexpr (R::row_of_bond(i) == r) {
           constexpr int o = 1 + D + Lat::bond(A, i).dx;
           constexpr int gi = R::group_of(i);
-          gs[gi][k] = __fadd2_rn(gs[gi][k], make_float2(w[o], w[o + 2]));
+          gs[gi][k][0] = __fadd_rn(gs[gi][k][0], w[o]);
+          gs[gi][k][1] = __fadd_rn(gs[gi][k][1], w[o + 2]);
         }
       });
     }
@@ -119,7 +125,8 @@ __device__ __forceinline__ void seg_sites(const Common& c, const float (&J)[SCK_
   for (int k = 0; k < N; ++k) {
     float2 acc = f2(0.0f);
 #pragma unroll
-    for (int gi = 0; gi < Lat::groups; ++gi) acc = __fadd2_rn(acc, __fmul2_rn(f2(J[gi]), gs[gi][k]));
+    for (int gi = 0; gi < Lat::groups; ++gi)
+      acc = __fadd2_rn(acc, __fmul2_rn(f2(J[gi]), make_float2(gs[gi][k][0], gs[gi][k][1])));
     if (c.hnz[k]) acc = __fadd2_rn(acc, f2(c.h[k]));
     v[k] = acc;
   }
@@ -160,9 +167,8 @@ __global__ void __launch_bounds__(256) seg_kernel(const __grid_constant__ SpecPa
   // rows of one y parity first (an even L2 keeps each half whole), so a warp's rows share the class offset
   const int y = (g.L2 & 1) ? i : (i < (g.L2 >> 1) ? 2 * i : 2 * (i - (g.L2 >> 1)) + 1);
   const int alpha = task.alpha;
-  const int d = colour_of(c.col, alpha, 0, y, z) == task.colour ? 0
-              : (colour_of(c.col, alpha, 1, y, z) == task.colour ? 1 : -1);
-  if (d < 0) return;
+  const int d = first_class_x(c, task.colour, alpha, y, z);
+  if (d > 1) return;
   const int32_t key = sweep_key_at(c.state, task.sweep_offset);
   static_for<0, Lat::b>([&](auto ac) {
     constexpr int a = decltype(ac)::value;
