@@ -381,9 +381,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--L", type=int, default=64, help="heisenberg-bcc cells per axis (profiling runs use less)")
     ap.add_argument("--replicas", type=int, default=1536, help="heisenberg-bcc replicas")
-    ap.add_argument("--path", default="auto", choices=["auto", "autotune", "row", "lattice", "generic"],
-                    help="sweep path: plan default, autotuned, row and lattice kernels, lattice kernels only, or "
-                         "generic kernels")
+    ap.add_argument("--path", default="auto",
+                    choices=["auto", "autotune", "tile", "segment", "row", "lattice", "generic"],
+                    help="sweep path: plan default, autotuned, tile kernels, segment kernels ('row' is an alias), "
+                         "lattice kernels only, or generic kernels")
     ap.add_argument("--learned-groups", type=int, default=16, choices=[16, 64])
     ap.add_argument("--learned-therm", type=int, default=2000)
     ap.add_argument("--learned-train-steps", type=int, default=1000)
@@ -418,8 +419,8 @@ def main():
         return
     s, A, S, T, cfg = make_workload(args.workload, rank, device, args.L, args.replicas)
     budget = int((args.l2_mb or 0) * (1 << 20))
-    if args.path in ("row", "lattice", "generic"):
-        A.tune({"row": 2, "lattice": 1, "generic": 0}[args.path], budget, RESIDENT_LIMIT)
+    if args.path in ("tile", "segment", "row", "lattice", "generic"):
+        A.tune({"tile": 3, "segment": 2, "row": 2, "lattice": 1, "generic": 0}[args.path], budget, RESIDENT_LIMIT)
     elif args.path == "autotune":
         from spin_colour_kernel_b200.autotune import autotune
         cfg["autotune"] = autotune(A, S, use_cache=False)
@@ -509,7 +510,7 @@ def main():
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "note": f"algorithmic {bpa} B/attempt; peak {peak_kind}; kernel = "
-                             f"{['generic', 'lattice', 'row'][path['specialised'] // 100]} class update, "
+                             f"{['generic', 'lattice', 'segment', 'tile'][path['specialised'] // 100]} class update, "
                              f"{launches_per_sweep} launches per sweep (L2 group {path['group']}), "
                              f"step times from CUDA events"},
         "e2e": {"value": e2e, "unit": "attempts/ns", "h2d_bytes_per_step": int(beta_h.numel() * 4),

@@ -131,16 +131,19 @@ int sck_plan_table_size(const sck_plan* plan, int64_t* elements, int32_t* elemen
 int sck_plan_shape(const sck_plan* plan, int32_t* computed_replicas, int32_t* rows);
 
 /* Execution choices of sck_sweep (set by the autotuner; the chain does not depend on them):
- *   specialised           2: compile-time lattice kernels and, where eligible, the segment kernels
- *                         (vector models, periodic box, classes alternating along x);
+ *   specialised           3: compile-time lattice kernels and, where eligible, the tile kernels (vector
+ *                         models, periodic box, L1 of 32, 64 or 128, rows a multiple of 8: neighbours
+ *                         read from shared memory);
+ *                         2: lattice kernels and, where eligible, the segment kernels (vector models,
+ *                         periodic box, classes alternating along x);
  *                         1: compile-time lattice kernels only (default); 0: generic kernels;
  *   l2_budget_bytes       L2 bytes the group pipeline may fill; 0 disables it (the default: the class kernels
  *                         are issue-bound, and smaller launches lose more than the saved HBM traffic);
  *   resident_limit_bytes  replicas up to this size (int8 / float32 storage) run all sweeps of a call in shared
  *                         memory, one block per replica; 0 disables it (default 200 KiB, at most 220 KiB).
- * sck_plan_path reports the chosen path: specialised = 100 * kernel kind (1 lattice, 2 segment) + table id (0 =
- * generic), budget, pipeline group (replicas
- * per group; 0 = class by class over all replicas) and whether sweeps run resident. No counterpart in the
+ * sck_plan_path reports the chosen path: specialised = 100 * kernel kind (1 lattice, 2 segment, 3 tile) + table
+ * id (0 = generic), budget, pipeline group (replicas per group; 0 = class by class over all replicas) and whether
+ * sweeps run resident. No counterpart in the
  * reference, whose Triton launch geometry plays this role (Sampler.__init__,
  * sampler.py:84-115). */
 int sck_plan_tune(sck_plan* plan, int32_t specialised, int64_t l2_budget_bytes, int64_t resident_limit_bytes);

@@ -342,7 +342,7 @@ int sck_plan_create(const sck_system_desc* d, int32_t batch, int32_t mode, sck_p
   p->NP = np < 1 ? 1 : np;
   p->field = (d->n == 1 && d->h64[0] != 0.0) ? 1 : 0;
   p->spec = find_spec(p);
-  p->row_kernels = 0;
+  p->kernel_kind = 1;
   p->l2_budget = 0;
   p->resident_limit = kResidentDefault;
   *out = p;
@@ -354,7 +354,7 @@ int sck_plan_tune(sck_plan* plan, int32_t specialised, int64_t l2_budget_bytes, 
     return fail(SCK_ERR_INVALID, "null plan or negative budget");
   if (resident_limit_bytes > kResidentMax) return fail(SCK_ERR_INVALID, "resident limit above 220 KiB of shared memory");
   plan->spec = specialised ? find_spec(plan) : 0;
-  plan->row_kernels = specialised >= 2 ? 1 : 0;
+  plan->kernel_kind = specialised >= 3 ? 3 : (specialised >= 2 ? 2 : 1);
   plan->l2_budget = l2_budget_bytes;
   plan->resident_limit = resident_limit_bytes;
   return SCK_OK;
@@ -363,7 +363,7 @@ int sck_plan_tune(sck_plan* plan, int32_t specialised, int64_t l2_budget_bytes, 
 int sck_plan_path(const sck_plan* plan, int32_t* specialised, int64_t* l2_budget_bytes, int32_t* group,
                   int32_t* resident) {
   if (plan == nullptr) return fail(SCK_ERR_INVALID, "null plan");
-  if (specialised) *specialised = plan->spec ? (seg_kernel_ok(plan) ? 2 : 1) * 100 + plan->spec : 0;
+  if (specialised) *specialised = plan->spec ? (tile_kernel_ok(plan) ? 3 : (seg_kernel_ok(plan) ? 2 : 1)) * 100 + plan->spec : 0;
   if (l2_budget_bytes) *l2_budget_bytes = plan->l2_budget;
   if (group) *group = pipeline_group(plan);
   if (resident) *resident = use_resident(plan) ? 1 : 0;

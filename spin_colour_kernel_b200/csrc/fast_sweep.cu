@@ -279,6 +279,7 @@ static SpecParams spec_params(const sck_plan* plan, const Common& c) {
 
 // One class over all replicas, in chunks of at most 65535 grid rows.
 int launch_spec_class(const sck_plan* plan, const Common& c, int colour, int alpha, cudaStream_t s) {
+  if (tile_kernel_ok(plan)) return launch_tile_class(plan, c, colour, alpha, s);
   SpecParams p = spec_params(plan, c);
   const int chunk = 65535 * slot_replicas(plan);
   for (int r0 = 0; r0 < c.B; r0 += chunk) {

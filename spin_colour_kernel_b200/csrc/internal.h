@@ -118,7 +118,7 @@ struct sck_plan {
   int Z, Z1, NP, field;
   int ising_lut;   // Ising chain with the host-built exp table (INT8, F32 with n = 1, PACKED)
   int spec;        // id of the matching compile-time lattice table (lattices.h), 0 = generic kernels
-  int row_kernels; // segment kernels (segment.cu) allowed for eligible specialised systems
+  int kernel_kind; // specialised class kernels: 1 lattice, 2 segment (segment.cu), 3 tile (tile.cu) where eligible
   long long l2_budget;  // bytes of L2 the group pipeline may fill
   long long resident_limit;  // largest replica (bytes) whose sweeps run resident in shared memory; 0 = never
 };

@@ -234,6 +234,159 @@ static void launch_obs_spec(const ObsParams& p, dim3 grid, cudaStream_t s) {
   else observables_spec_kernel<Lat, 3, 1><<<grid, 256, 0, s>>>(p);
 }
 
+// Tiled variant for float32 storage on periodic boxes with a lattice table. The spins of one replica are read
+// in bands of OBS_TY rows: a block of threads marches along z keeping three planes of its band (plus one halo
+// row on each side) in shared memory, converted to FP64 once when they arrive. Every forward bond then reads
+// FP64 neighbours from shared memory, so each spin component is converted ~(OBS_TY + 2) / OBS_TY times instead
+// of once per bond that reaches it: the float32 -> float64 conversions, not the FP64 arithmetic or the HBM
+// reads, bound the per-site kernel above. Same bond-once energy and the same fixed-order partial sums.
+constexpr int OBS_TY = 8;
+constexpr size_t OBS_TILE_SMEM_MAX = 112 * 1024;
+
+static size_t obs_tile_smem(const sck_plan* plan) {
+  const Geometry& g = plan->geom;
+  return (size_t)3 * g.b * g.n * (OBS_TY + 2) * g.L1 * sizeof(double);
+}
+
+// geometry that the tiled kernel serves (its lattice table may still be switched off by tuning)
+static bool obs_tile_geometry(const sck_plan* plan) {
+  const Geometry& g = plan->geom;
+  if (plan->mode != SCK_MODE_F32 || find_spec(plan) == 0) return false;
+  if (!g.per[0] || !g.per[1] || g.L1 % 4 != 0 || g.L1 < 3 || g.L2 % OBS_TY != 0) return false;
+  if (g.dim == 3 && (!g.per[2] || g.L3 < 3)) return false;
+  return obs_tile_smem(plan) <= OBS_TILE_SMEM_MAX;
+}
+
+template <class Lat, int N>
+__global__ void __launch_bounds__(256) observables_tile_kernel(const __grid_constant__ ObsParams p) {
+  extern __shared__ double ring[];   // [3 planes][b][N][OBS_TY + 2 rows][L1]
+  const Geometry& g = p.g;
+  const int rep = blockIdx.y, y0 = blockIdx.x * OBS_TY, L1 = g.L1;
+  constexpr int R2 = OBS_TY + 2;
+  const int slot = Lat::b * N * R2 * L1;
+  const float* src = (const float*)p.spins + (size_t)rep * N * g.nsite;
+  const int q4 = L1 >> 2;
+  auto load_plane = [&](int zu) {   // unwrapped plane index -1 .. L3
+    const int zz = zu < 0 ? zu + g.L3 : (zu >= g.L3 ? zu - g.L3 : zu);
+    double* dst = ring + ((zu + 3) % 3) * slot;
+    const int total = Lat::b * N * R2 * q4;
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+      const int row = i / q4, x4 = i - row * q4;
+      const int r = row % R2, ak = row / R2, k = ak % N, a = ak / N;
+      int y = y0 - 1 + r;
+      y = y < 0 ? y + g.L2 : (y >= g.L2 ? y - g.L2 : y);
+      const float4 v = *(const float4*)(src + (size_t)k * g.nsite + (size_t)a * g.plane +
+                                        ((size_t)zz * g.L2 + y) * L1 + 4 * x4);
+      double* d = dst + row * L1 + 4 * x4;
+      d[0] = v.x;
+      d[1] = v.y;
+      d[2] = v.z;
+      d[3] = v.w;
+    }
+  };
+  load_plane(-1);
+  load_plane(0);
+  load_plane(1);
+  __syncthreads();
+  constexpr int NV = 1 + SCK_MAX_BASIS * N;
+  double acc[NV];
+#pragma unroll
+  for (int i = 0; i < NV; ++i) acc[i] = 0.0;
+  const int sites = Lat::b * OBS_TY * L1;
+  for (int zu = 0; zu < g.L3; ++zu) {
+    const double* const pl[3] = {ring + ((zu + 2) % 3) * slot, ring + (zu % 3) * slot, ring + ((zu + 1) % 3) * slot};
+#pragma unroll 4
+    for (int i = threadIdx.x; i < sites; i += blockDim.x) {
+      const int rest = (int)fdiv((uint32_t)i, p.fd_L1);
+      const int x = i - rest * L1, ty = rest % OBS_TY, alpha = rest / OBS_TY;
+      const int site = alpha * g.plane + (zu * g.L2 + y0 + ty) * L1 + x;
+      if (p.mask != nullptr && p.mask[site] == 0) continue;
+      const double* own = pl[1];
+      double s[N];
+#pragma unroll
+      for (int k = 0; k < N; ++k) s[k] = own[((alpha * N + k) * R2 + ty + 1) * L1 + x];
+      double e = 0.0;
+      static_for<0, Lat::b>([&](auto ac) {
+        constexpr int a = decltype(ac)::value;
+        if (a != alpha) return;
+        const SubObs& ob = p.obs[a];
+        static_for<0, Lat::n_bonds(a)>([&](auto ic) {
+          constexpr int bi = decltype(ic)::value;
+          if constexpr (forward_bond<Lat, a>(bi)) {
+            constexpr BondC bd = Lat::bond(a, bi);
+            int x2 = x + bd.dx;
+            x2 = x2 < 0 ? x2 + L1 : (x2 >= L1 ? x2 - L1 : x2);
+            const double* nb = pl[bd.dz + 1] + ((bd.a2 * N) * R2 + ty + 1 + bd.dy) * L1 + x2;
+            double dot = 0.0;
+#pragma unroll
+            for (int k = 0; k < N; ++k) dot += s[k] * nb[k * R2 * L1];
+            e -= ob.J[bi] * dot;
+          }
+        });
+      });
+#pragma unroll
+      for (int k = 0; k < N; ++k) e -= p.h64[k] * s[k];
+      if constexpr (N == 3) {
+        if (g.has_cubic) {
+          const double k1 = (double)p.k1[site];
+          const double xy = s[0] * s[1], xz = s[0] * s[2], yz = s[1] * s[2], xyz = s[0] * s[1] * s[2];
+          e += k1 * (xy * xy + xz * xz + yz * yz) + p.k2 * xyz * xyz;
+        }
+      }
+      acc[0] += e;
+#pragma unroll
+      for (int a = 0; a < SCK_MAX_BASIS; ++a)
+        if (a == alpha) {
+#pragma unroll
+          for (int k = 0; k < N; ++k) acc[1 + a * N + k] += s[k];
+        }
+    }
+    __syncthreads();                              // every thread is done with plane zu - 1
+    if (zu + 1 < g.L3) load_plane(zu + 2);        // into plane zu - 1's slot
+    __syncthreads();
+  }
+  __shared__ double red[NV][8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    double v = acc[i];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, off);
+    if (lane == 0) red[i][warp] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    double v = 0.0;
+    for (int wi = 0; wi < (int)(blockDim.x >> 5); ++wi) v += red[threadIdx.x][wi];
+    p.partial[((size_t)rep * p.blocks_per_rep + blockIdx.x) * OBS_VALUES + threadIdx.x] = v;
+  }
+}
+
+template <class Lat>
+static int launch_obs_tile(const sck_plan* plan, const ObsParams& p, cudaStream_t s) {
+  const size_t smem = obs_tile_smem(plan);
+  const dim3 grid(plan->geom.L2 / OBS_TY, p.B);
+  int rc;
+  switch (plan->geom.n) {
+    case 1:
+      rc = cuda_status(cudaFuncSetAttribute(observables_tile_kernel<Lat, 1>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "obs tile");
+      if (rc == SCK_OK) observables_tile_kernel<Lat, 1><<<grid, 256, smem, s>>>(p);
+      break;
+    case 2:
+      rc = cuda_status(cudaFuncSetAttribute(observables_tile_kernel<Lat, 2>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "obs tile");
+      if (rc == SCK_OK) observables_tile_kernel<Lat, 2><<<grid, 256, smem, s>>>(p);
+      break;
+    default:
+      rc = cuda_status(cudaFuncSetAttribute(observables_tile_kernel<Lat, 3>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "obs tile");
+      if (rc == SCK_OK) observables_tile_kernel<Lat, 3><<<grid, 256, smem, s>>>(p);
+      break;
+  }
+  return rc;
+}
+
 // Sum the partials of every replica in block order; E[r] and M[r][alpha][k] (B x b x n).
 __global__ void observables_finish(const double* __restrict__ partial, int B, int blocks_per_rep, int b, int n,
                                    double* __restrict__ E, double* __restrict__ M) {
@@ -250,10 +403,18 @@ __global__ void observables_finish(const double* __restrict__ partial, int B, in
 }
 
 // Enough blocks in flight to cover the GPU, never more than the sites of one replica need.
-int obs_blocks_per_rep(const sck_plan* plan, int batch) {
+static int obs_blocks_generic(const sck_plan* plan, int batch) {
   const int per_rep = (plan->geom.nsite + 255) / 256;
   const int want = (148 * 8 + batch - 1) / batch;
   return want < per_rep ? (want < 1 ? 1 : want) : per_rep;
+}
+
+// Partial sums per replica the workspace must hold: the larger of the two paths' counts, so that a workspace
+// stays valid whatever the plan's tuning selects later.
+int obs_blocks_per_rep(const sck_plan* plan, int batch) {
+  const int gen = obs_blocks_generic(plan, batch);
+  const int tile = obs_tile_geometry(plan) ? plan->geom.L2 / OBS_TY : 0;
+  return gen > tile ? gen : tile;
 }
 
 int launch_observables(const sck_plan* plan, const void* spins, int storage, int batch, const int8_t* mask,
@@ -268,7 +429,9 @@ int launch_observables(const sck_plan* plan, const void* spins, int storage, int
   }
   for (int k = 0; k < 3; ++k) p.h64[k] = plan->desc.h64[k];
   p.k2 = plan->desc.k2_64;
-  p.blocks_per_rep = obs_blocks_per_rep(plan, batch);
+  // float32 storage of a tiled-geometry system with its lattice table on: bands of OBS_TY rows
+  const bool tile = plan->spec != 0 && storage == SCK_MODE_F32 && obs_tile_geometry(plan);
+  p.blocks_per_rep = tile ? plan->geom.L2 / OBS_TY : obs_blocks_generic(plan, batch);
   p.fd_plane = make_fastdiv((uint32_t)plan->geom.plane);
   p.fd_L1 = make_fastdiv((uint32_t)plan->geom.L1);
   p.fd_L2 = make_fastdiv((uint32_t)plan->geom.L2);
@@ -281,7 +444,18 @@ int launch_observables(const sck_plan* plan, const void* spins, int storage, int
   const int n = plan->geom.n;
   // the lattice table fixes the bonds of int8 and float32 storage (packed storage reads the generic way)
   const bool spec = plan->spec != 0 && p.storage != 2;
-  if (spec) {
+  if (tile) {
+    int rc = SCK_OK;
+    switch (plan->spec) {
+      case Lat_square_1::id: rc = launch_obs_tile<Lat_square_1>(plan, p, s); break;
+      case Lat_triangular_1::id: rc = launch_obs_tile<Lat_triangular_1>(plan, p, s); break;
+      case Lat_sc_1::id: rc = launch_obs_tile<Lat_sc_1>(plan, p, s); break;
+      case Lat_bcc_1::id: rc = launch_obs_tile<Lat_bcc_1>(plan, p, s); break;
+      case Lat_bcc_1_2::id: rc = launch_obs_tile<Lat_bcc_1_2>(plan, p, s); break;
+      default: rc = launch_obs_tile<Lat_fcc_1>(plan, p, s); break;
+    }
+    if (rc != SCK_OK) return rc;
+  } else if (spec) {
     switch (plan->spec) {
       case Lat_square_1::id: launch_obs_spec<Lat_square_1>(p, grid, s); break;
       case Lat_triangular_1::id: launch_obs_spec<Lat_triangular_1>(p, grid, s); break;

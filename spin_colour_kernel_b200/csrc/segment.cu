@@ -6,9 +6,9 @@
 // (own row first) it loads the segment of each component with one 128-bit load (the lanes of a warp read
 // consecutive 16-byte pieces of a row, so every sector fetched is used whole), plus the one site past either
 // end that an x-offset of -1 or +1 reaches, and adds each bond's neighbour to the coupling-group sums of both
-// sites. Compared with one site and two replicas per thread this halves the load
-// instructions and shares the row addressing between the two sites. The group sums run in row order rather than
-// the reference's bond order, so local fields differ from the reference's by float32 rounding only; the
+// sites. Compared with one site and two replicas per thread this halves the load instructions and shares the
+// row addressing between the two sites. The group sums run in row order rather than the reference's bond
+// order, so local fields differ from the reference's by float32 rounding only; the
 // proposal, energy change and acceptance keep the reference's operation order (finish_core in spec.cuh). Lanes
 // are mapped to rows so that the rows of a warp share d (rows of one y parity are consecutive), which keeps the
 // two compile-time variants of a warp from diverging.
@@ -149,7 +149,7 @@ __device__ __forceinline__ void seg_sites(const Common& c, const float (&J)[SCK_
 
 // Grid (ceil(rows * L1 / 4 / 256), n_tasks * units_per_task); block y-slot -> (task, replica).
 template <class Lat, int N>
-__global__ void __launch_bounds__(256) seg_kernel(const __grid_constant__ SpecParams p) {
+__global__ void __launch_bounds__(256, 4) seg_kernel(const __grid_constant__ SpecParams p) {
   const Common& c = p.c;
   const Geometry& g = c.g;
   const uint32_t segs = (uint32_t)(g.L1 >> 2);
@@ -192,7 +192,7 @@ static constexpr bool lat_reach_one() {
 
 bool seg_kernel_ok(const sck_plan* plan) {
   const Geometry& g = plan->geom;
-  if (!plan->row_kernels || plan->mode != SCK_MODE_F32 || g.n < 2 || g.has_mask || plan->P != 2) return false;
+  if (plan->kernel_kind != 2 || plan->mode != SCK_MODE_F32 || g.n < 2 || g.has_mask || plan->P != 2) return false;
   if (g.L1 % 4 != 0 || !g.per[0] || !g.per[1] || g.L2 < 3) return false;
   if (g.dim == 3 && (!g.per[2] || g.L3 < 3)) return false;
   switch (plan->spec) {

@@ -83,16 +83,18 @@ __device__ __forceinline__ void finish_core(const Common& c, uint32_t cnt0, uint
     sincos_2pi(__fmul_rn(TWO_PI, to_uniform(ra.x2)), sa, ca);
     sincos_2pi(__fmul_rn(TWO_PI, to_uniform(rb.x2)), sb, cb);
     const float2 w = __fadd2_rn(f2(1.0f), __fmul2_rn(f2(-1.0f), __fmul2_rn(cz, cz)));
-    const float2 rr = make_float2(sqrtf(fmaxf(w.x, 0.0f)), sqrtf(fmaxf(w.y, 0.0f)));
+    // sqrt(w) as w * rsqrt(w) on the SFU (a few ulp, like the SFU sine and cosine above; w = 0 gives 0)
+    const float2 rr = make_float2(w.x > 0.0f ? w.x * rsqrtf(w.x) : 0.0f, w.y > 0.0f ? w.y * rsqrtf(w.y) : 0.0f);
     t[0] = __fmul2_rn(rr, make_float2(ca, cb));
     t[1] = __fmul2_rn(rr, make_float2(sa, sb));
     t[2] = cz;
   }
-  const float2 m1 = f2(-1.0f);
-  float2 d = __fmul2_rn(__fadd2_rn(t[0], __fmul2_rn(m1, s[0])), v[0]);
+  // -1 * x is exact, so the reference's t + (-1) s and (-1) d are written as a subtraction and a negation
+  auto neg = [](float2 a) { return make_float2(-a.x, -a.y); };
+  float2 d = __fmul2_rn(__fadd2_rn(t[0], neg(s[0])), v[0]);
 #pragma unroll
-  for (int k = 1; k < N; ++k) d = __fadd2_rn(d, __fmul2_rn(__fadd2_rn(t[k], __fmul2_rn(m1, s[k])), v[k]));
-  float2 dE = __fmul2_rn(m1, d);
+  for (int k = 1; k < N; ++k) d = __fadd2_rn(d, __fmul2_rn(__fadd2_rn(t[k], neg(s[k])), v[k]));
+  float2 dE = neg(d);
   if constexpr (N == 3) {
     if (g.has_cubic) {
       const float2 k1 = make_float2(c.k1[k1_0], c.k1[k1_1]);
@@ -103,7 +105,7 @@ __device__ __forceinline__ void finish_core(const Common& c, uint32_t cnt0, uint
         const float2 quad = __fadd2_rn(__fadd2_rn(__fmul2_rn(q01, q01), __fmul2_rn(q02, q02)), __fmul2_rn(q12, q12));
         return __fadd2_rn(__fmul2_rn(k1, quad), __fmul2_rn(__fmul2_rn(k2, tri), tri));
       };
-      dE = __fadd2_rn(dE, __fadd2_rn(aniso(t), __fmul2_rn(m1, aniso(s))));
+      dE = __fadd2_rn(dE, __fadd2_rn(aniso(t), neg(aniso(s))));
     }
   }
   if (g.acceptance == SCK_BARKER) {
@@ -111,7 +113,7 @@ __device__ __forceinline__ void finish_core(const Common& c, uint32_t cnt0, uint
     acc0 = __fmul_rn(u0.x, __fadd_rn(1.0f, __expf(xb.x))) < 1.0f;
     acc1 = __fmul_rn(u0.y, __fadd_rn(1.0f, __expf(xb.y))) < 1.0f;
   } else {
-    const float2 xm = __fmul2_rn(__fmul2_rn(m1, beta), dE);
+    const float2 xm = __fmul2_rn(neg(beta), dE);
     acc0 = u0.x < __expf(xm.x);
     acc1 = u0.y < __expf(xm.y);
   }
@@ -129,5 +131,9 @@ __device__ __forceinline__ void finish_pair(const Common& c, int own, int rep0, 
 // Segment kernels (segment.cu): eligibility and the task launch.
 bool seg_kernel_ok(const sck_plan* plan);
 int launch_seg_tasks(const sck_plan* plan, SpecParams& p, int ys, cudaStream_t s);
+
+// Tile kernels (tile.cu): eligibility and one class over all replicas.
+bool tile_kernel_ok(const sck_plan* plan);
+int launch_tile_class(const sck_plan* plan, const Common& c, int colour, int alpha, cudaStream_t s);
 
 }  // namespace sck

@@ -134,8 +134,9 @@ class Sampler:
         self._workspace(self.B)
 
     def tune(self, specialised=True, l2_budget: int = 0, resident_limit: int = 200 << 10):
-        """Execution choices of sweep: specialised kernels (1 or True: lattice kernels, the default; 2: row
-        kernels where the system allows them, else lattice kernels; 0 or False: generic), L2 group-pipeline budget
+        """Execution choices of sweep: specialised kernels (1 or True: lattice kernels, the default; 2: segment
+        kernels, 3: tile kernels, where the system allows them, else lattice kernels; 0 or False: generic),
+        L2 group-pipeline budget
         (bytes), largest replica (bytes) whose sweeps run resident in shared memory. The chain does not depend on
         them."""
         level = int(specialised)

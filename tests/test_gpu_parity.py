@@ -252,6 +252,43 @@ def test_segment_kernels_agree_with_lattice_kernels(name):
     assert not torch.equal(S1, A.init_spins(seed=7))
 
 
+TILE_SYSTEMS = {
+    "heis_bcc_j1j2_64x8x6": SEG_SYSTEMS["heis_bcc_j1j2_64x8x6"],
+    "heis_sc_32x16x4": lambda: sy.System("Heisenberg sc", 3, cr.make("sc"), (32, 16, 4), (True,) * 3, {1: -1.0},
+                                         h=(0.2, 0.0, 0.1)),
+    "heis_fcc_32x8x4": lambda: sy.System("Heisenberg fcc", 3, cr.make("fcc"), (32, 8, 4), (True,) * 3, {1: 1.0}),
+    "xy_square_128x16": lambda: sy.System("XY square", 2, cr.make("square"), (128, 16), (True, True), {1: 1.0},
+                                          h=(0.05, 0.0)),
+    "xy_triangular_64x24": lambda: sy.System("XY triangular", 2, cr.make("triangular"), (64, 24), (True, True),
+                                             {1: -1.0}),
+    "xy_square_64x16_masked": lambda: sy.System("XY square masked", 2, cr.make("square"), (64, 16), (True, True),
+                                                {1: 1.0}, mask=np.broadcast_to(
+                                                    (np.add.outer(np.arange(16), np.arange(64)) % 7 != 0),
+                                                    (1, 1, 16, 64)).copy()),
+}
+
+
+@pytest.mark.parametrize("name", sorted(TILE_SYSTEMS))
+def test_tile_kernels_equal_lattice_kernels(name):
+    """Tile kernels (bands of rows staged in shared memory, neighbours read at compile-time offsets) run the same
+    float32x2 arithmetic in the same bond order as the lattice kernels: spins bit-identical, odd replica count,
+    masks, 2D and 3D, one to four sublattices, colourings of any x-period."""
+    from spin_colour_kernel_b200.sampler import Sampler
+    s = TILE_SYSTEMS[name]()
+    B = 5
+    A, R = Sampler(s, B, device="cuda", seed=3), Sampler(s, B, device="cuda", seed=3)
+    pa, pr = A.tune(3, 0, 0), R.tune(1, 0, 0)
+    assert pa["specialised"] // 100 == 3 and pr["specialised"] // 100 == 1, (pa, pr)
+    for X in (A, R):
+        X.set_temperature(torch.linspace(0.4, 3.0, B))
+    S1 = A.init_spins(seed=7)
+    S2 = S1.clone()
+    A.sweep(S1, 3)
+    R.sweep(S2, 3)
+    assert torch.equal(S1, S2)
+    assert not torch.equal(S1, A.init_spins(seed=7))
+
+
 @pytest.mark.parametrize("name", ["ising_square8", "nanodot_small", "w3_heis_bcc4_j1j2", "w4_xy_triangular12_disk",
                                   "ising_masked_field_barker", "heis_kagome3_afm"])
 def test_resident_sweeps_equal_class_launches(name):
@@ -354,6 +391,37 @@ def test_observables_match_oracle_fp64():
         x = A.unpack(S).cpu().numpy()
         np.testing.assert_allclose(E.cpu().numpy(), obs.energy(s, x), rtol=1e-12, atol=1e-9)
         np.testing.assert_allclose(M.cpu().numpy(), obs.magnetization(x), rtol=1e-12, atol=1e-9)
+
+
+def test_tiled_observables_match_oracle_fp64():
+    """Float32 storage on periodic boxes whose row count is a multiple of 8 takes the tiled path (bands of rows
+    staged in shared memory as FP64): energies and magnetizations within 1e-12 of the FP64 oracle, masks,
+    fields, anisotropy, 2D and 3D, one to three components; a workspace sized before the tuning switches the
+    lattice tables off stays valid for the other path."""
+    from spin_colour_kernel_b200.sampler import Sampler
+    from spin_colour_kernel_b200 import workloads as W
+    sq = cr.make("square")
+    masked = sy.System("XY square periodic masked", 2, sq, (16, 16), (True, True), {1: 1.0}, h=(0.05, 0.0),
+                       mask=W.disk_mask(1, 16, 6.0))
+    cases = [
+        (C.heisenberg_bcc_j1j2(sy, cr, 8), {}),
+        (sy.System("Heisenberg sc", 3, cr.make("sc"), (12, 16, 8), (True,) * 3, {1: -1.0}, h=(0.1, 0.0, 0.2)), {}),
+        (C.xy_periodic_field(sy, cr, "square", 16), {}),
+        (masked, {}),
+        (sy.ising("sc", 8), {"spin_dtype": torch.float32, "packed": False}),
+    ]
+    for s, kw in cases:
+        A = Sampler(s, 3, device="cuda", seed=1, **kw)
+        S = A.init_spins(seed=3)
+        A.sweep(S, 2)
+        E, M = A.observables(S)
+        x = A.unpack(S).cpu().numpy()
+        np.testing.assert_allclose(E.cpu().numpy(), obs.energy(s, x), rtol=1e-12, atol=1e-9, err_msg=s.name)
+        np.testing.assert_allclose(M.cpu().numpy(), obs.magnetization(x), rtol=1e-12, atol=1e-9, err_msg=s.name)
+        A.tune(False, 0, 0)                    # generic path, same workspace
+        E2, M2 = A.observables(S)
+        np.testing.assert_allclose(E2.cpu().numpy(), E.cpu().numpy(), rtol=1e-12, atol=1e-9)
+        np.testing.assert_allclose(M2.cpu().numpy(), M.cpu().numpy(), rtol=1e-12, atol=1e-9)
 
 
 def test_sync_sweep_matches_oracle():
