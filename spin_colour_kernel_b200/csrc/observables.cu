@@ -234,54 +234,76 @@ static void launch_obs_spec(const ObsParams& p, dim3 grid, cudaStream_t s) {
   else observables_spec_kernel<Lat, 3, 1><<<grid, 256, 0, s>>>(p);
 }
 
-// Tiled variant for float32 storage on periodic boxes with a lattice table. The spins of one replica are read
-// in bands of OBS_TY rows: a block of threads marches along z keeping three planes of its band (plus one halo
-// row on each side) in shared memory, converted to FP64 once when they arrive. Every forward bond then reads
-// FP64 neighbours from shared memory, so each spin component is converted ~(OBS_TY + 2) / OBS_TY times instead
-// of once per bond that reaches it: the float32 -> float64 conversions, not the FP64 arithmetic or the HBM
-// reads, bound the per-site kernel above. Same bond-once energy and the same fixed-order partial sums.
-constexpr int OBS_TY = 8;
-constexpr size_t OBS_TILE_SMEM_MAX = 112 * 1024;
+// Tiled variant for float32 storage on periodic boxes with a lattice table and a row length of 16, 32, 64 or
+// 128. The spins of one replica are read in bands of OBS_TY rows: a block of threads marches along z keeping
+// three planes of its band (plus one halo row on each side and one halo site at each end of a row) in shared
+// memory, converted to FP64 once when they arrive. Every forward bond then reads FP64 neighbours from shared
+// memory at compile-time offsets from one address per plane, so each spin component is converted
+// ~(OBS_TY + 2) / OBS_TY times instead of once per bond that reaches it, and no per-bond index arithmetic is
+// left: the conversions and the index arithmetic, not the FP64 arithmetic or the HBM reads, bound the per-site
+// kernel above. Same bond-once energy and the same fixed-order partial sums.
+constexpr int OBS_TY = 4;                     // rows per band
+constexpr int OBS_PAD = 2;                    // doubles before x = 0 in a shared row: x = -1 sits at OBS_PAD - 1
+constexpr size_t OBS_TILE_SMEM_MAX = 110 * 1024;
+
+template <int L1T>
+struct ObsRow {
+  static constexpr int RS = L1T + 2 * OBS_PAD;   // doubles per shared row
+  static constexpr int R2 = OBS_TY + 2;          // band rows plus halo rows
+};
 
 static size_t obs_tile_smem(const sck_plan* plan) {
   const Geometry& g = plan->geom;
-  return (size_t)3 * g.b * g.n * (OBS_TY + 2) * g.L1 * sizeof(double);
+  return (size_t)3 * g.b * g.n * (OBS_TY + 2) * (g.L1 + 2 * OBS_PAD) * sizeof(double);
 }
 
 // geometry that the tiled kernel serves (its lattice table may still be switched off by tuning)
 static bool obs_tile_geometry(const sck_plan* plan) {
   const Geometry& g = plan->geom;
   if (plan->mode != SCK_MODE_F32 || find_spec(plan) == 0) return false;
-  if (!g.per[0] || !g.per[1] || g.L1 % 4 != 0 || g.L1 < 3 || g.L2 % OBS_TY != 0) return false;
+  if (g.L1 != 16 && g.L1 != 32 && g.L1 != 64 && g.L1 != 128) return false;
+  if (!g.per[0] || !g.per[1] || g.L2 % OBS_TY != 0 || g.L2 < 3) return false;
   if (g.dim == 3 && (!g.per[2] || g.L3 < 3)) return false;
   return obs_tile_smem(plan) <= OBS_TILE_SMEM_MAX;
 }
 
-template <class Lat, int N>
+// FP64 shared-memory load at a compile-time byte offset from a register address
+template <int OFF>
+__device__ __forceinline__ double ldsd(uint32_t addr) {
+  double v;
+  asm volatile("ld.shared.f64 %0, [%1+%2];\n" : "=d"(v) : "r"(addr), "n"(OFF));
+  return v;
+}
+
+template <class Lat, int N, int L1T>
 __global__ void __launch_bounds__(256) observables_tile_kernel(const __grid_constant__ ObsParams p) {
-  extern __shared__ double ring[];   // [3 planes][b][N][OBS_TY + 2 rows][L1]
+  extern __shared__ __align__(16) double ring[];   // [3 planes][b][N][R2 rows][RS]
+  using RW = ObsRow<L1T>;
+  constexpr int RS = RW::RS, R2 = RW::R2;
+  constexpr int COMP = R2 * RS;                    // doubles of one component of one sublattice
+  constexpr int SLOT = Lat::b * N * COMP;
   const Geometry& g = p.g;
-  const int rep = blockIdx.y, y0 = blockIdx.x * OBS_TY, L1 = g.L1;
-  constexpr int R2 = OBS_TY + 2;
-  const int slot = Lat::b * N * R2 * L1;
+  const int rep = blockIdx.y, y0 = blockIdx.x * OBS_TY;
   const float* src = (const float*)p.spins + (size_t)rep * N * g.nsite;
-  const int q4 = L1 >> 2;
+  constexpr int Q = L1T / 4;
+  constexpr int ROWS = Lat::b * N * R2;
   auto load_plane = [&](int zu) {   // unwrapped plane index -1 .. L3
     const int zz = zu < 0 ? zu + g.L3 : (zu >= g.L3 ? zu - g.L3 : zu);
-    double* dst = ring + ((zu + 3) % 3) * slot;
-    const int total = Lat::b * N * R2 * q4;
-    for (int i = threadIdx.x; i < total; i += blockDim.x) {
-      const int row = i / q4, x4 = i - row * q4;
+    double* dst = ring + ((zu + 3) % 3) * SLOT;
+    for (int i = threadIdx.x; i < ROWS * Q; i += blockDim.x) {
+      const int row = i / Q, q = i % Q;
       const int r = row % R2, ak = row / R2, k = ak % N, a = ak / N;
       int y = y0 - 1 + r;
       y = y < 0 ? y + g.L2 : (y >= g.L2 ? y - g.L2 : y);
       const float4 v = *(const float4*)(src + (size_t)k * g.nsite + (size_t)a * g.plane +
-                                        ((size_t)zz * g.L2 + y) * L1 + 4 * x4);
-      double* d = dst + row * L1 + 4 * x4;
+                                        ((size_t)zz * g.L2 + y) * L1T + 4 * q);
+      double* d = dst + row * RS + OBS_PAD + 4 * q;
       d[0] = v.x;
       d[1] = v.y;
       d[2] = v.z;
       d[3] = v.w;
+      if (q == 0) d[L1T] = v.x;            // x = L1 is x = 0
+      if (q == Q - 1) d[-L1T + 3] = v.w;   // x = -1 is x = L1 - 1
     }
   };
   load_plane(-1);
@@ -292,34 +314,38 @@ __global__ void __launch_bounds__(256) observables_tile_kernel(const __grid_cons
   double acc[NV];
 #pragma unroll
   for (int i = 0; i < NV; ++i) acc[i] = 0.0;
-  const int sites = Lat::b * OBS_TY * L1;
+  const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(ring);
+  constexpr uint32_t SLOT_BYTES = 8u * SLOT;
+  uint32_t pl[3] = {sbase + 2 * SLOT_BYTES, sbase, sbase + SLOT_BYTES};   // planes zu - 1, zu, zu + 1 at zu = 0
+  constexpr int SITES = Lat::b * OBS_TY * L1T;
   for (int zu = 0; zu < g.L3; ++zu) {
-    const double* const pl[3] = {ring + ((zu + 2) % 3) * slot, ring + (zu % 3) * slot, ring + ((zu + 1) % 3) * slot};
-#pragma unroll 4
-    for (int i = threadIdx.x; i < sites; i += blockDim.x) {
-      const int rest = (int)fdiv((uint32_t)i, p.fd_L1);
-      const int x = i - rest * L1, ty = rest % OBS_TY, alpha = rest / OBS_TY;
-      const int site = alpha * g.plane + (zu * g.L2 + y0 + ty) * L1 + x;
+#pragma unroll 2
+    for (int i = threadIdx.x; i < SITES; i += blockDim.x) {
+      const int x = i % L1T, ty = (i / L1T) % OBS_TY, alpha = i / (L1T * OBS_TY);
+      const int site = alpha * g.plane + (zu * g.L2 + y0 + ty) * L1T + x;
       if (p.mask != nullptr && p.mask[site] == 0) continue;
-      const double* own = pl[1];
+      const uint32_t so = 8u * (uint32_t)((ty + 1) * RS + OBS_PAD + x);
       double s[N];
-#pragma unroll
-      for (int k = 0; k < N; ++k) s[k] = own[((alpha * N + k) * R2 + ty + 1) * L1 + x];
       double e = 0.0;
       static_for<0, Lat::b>([&](auto ac) {
         constexpr int a = decltype(ac)::value;
         if (a != alpha) return;
+        static_for<0, N>([&](auto kc) {
+          constexpr int k = decltype(kc)::value;
+          s[k] = ldsd<8 * (a * N + k) * COMP>(pl[1] + so);
+        });
         const SubObs& ob = p.obs[a];
         static_for<0, Lat::n_bonds(a)>([&](auto ic) {
           constexpr int bi = decltype(ic)::value;
           if constexpr (forward_bond<Lat, a>(bi)) {
             constexpr BondC bd = Lat::bond(a, bi);
-            int x2 = x + bd.dx;
-            x2 = x2 < 0 ? x2 + L1 : (x2 >= L1 ? x2 - L1 : x2);
-            const double* nb = pl[bd.dz + 1] + ((bd.a2 * N) * R2 + ty + 1 + bd.dy) * L1 + x2;
+            constexpr int off = 8 * (bd.a2 * N * COMP + bd.dy * RS + bd.dx);
+            const uint32_t q = pl[bd.dz + 1] + so;
             double dot = 0.0;
-#pragma unroll
-            for (int k = 0; k < N; ++k) dot += s[k] * nb[k * R2 * L1];
+            static_for<0, N>([&](auto kc) {
+              constexpr int k = decltype(kc)::value;
+              dot += s[k] * ldsd<off + 8 * k * COMP>(q);
+            });
             e -= ob.J[bi] * dot;
           }
         });
@@ -342,8 +368,14 @@ __global__ void __launch_bounds__(256) observables_tile_kernel(const __grid_cons
         }
     }
     __syncthreads();                              // every thread is done with plane zu - 1
-    if (zu + 1 < g.L3) load_plane(zu + 2);        // into plane zu - 1's slot
-    __syncthreads();
+    const uint32_t rot = pl[0];                   // the ring turns
+    pl[0] = pl[1];
+    pl[1] = pl[2];
+    pl[2] = rot;
+    if (zu + 1 < g.L3) {
+      load_plane(zu + 2);                         // into plane zu - 1's slot
+      __syncthreads();
+    }
   }
   __shared__ double red[NV][8];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -362,29 +394,34 @@ __global__ void __launch_bounds__(256) observables_tile_kernel(const __grid_cons
   }
 }
 
-template <class Lat>
-static int launch_obs_tile(const sck_plan* plan, const ObsParams& p, cudaStream_t s) {
+template <class Lat, int N, int L1T>
+static int launch_obs_tile_t(const sck_plan* plan, const ObsParams& p, cudaStream_t s) {
   const size_t smem = obs_tile_smem(plan);
   const dim3 grid(plan->geom.L2 / OBS_TY, p.B);
-  int rc;
-  switch (plan->geom.n) {
-    case 1:
-      rc = cuda_status(cudaFuncSetAttribute(observables_tile_kernel<Lat, 1>,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "obs tile");
-      if (rc == SCK_OK) observables_tile_kernel<Lat, 1><<<grid, 256, smem, s>>>(p);
-      break;
-    case 2:
-      rc = cuda_status(cudaFuncSetAttribute(observables_tile_kernel<Lat, 2>,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "obs tile");
-      if (rc == SCK_OK) observables_tile_kernel<Lat, 2><<<grid, 256, smem, s>>>(p);
-      break;
-    default:
-      rc = cuda_status(cudaFuncSetAttribute(observables_tile_kernel<Lat, 3>,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "obs tile");
-      if (rc == SCK_OK) observables_tile_kernel<Lat, 3><<<grid, 256, smem, s>>>(p);
-      break;
-  }
+  const int rc = cuda_status(cudaFuncSetAttribute(observables_tile_kernel<Lat, N, L1T>,
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                             "obs tile");
+  if (rc == SCK_OK) observables_tile_kernel<Lat, N, L1T><<<grid, 256, smem, s>>>(p);
   return rc;
+}
+
+template <class Lat, int N>
+static int launch_obs_tile_n(const sck_plan* plan, const ObsParams& p, cudaStream_t s) {
+  switch (plan->geom.L1) {
+    case 16: return launch_obs_tile_t<Lat, N, 16>(plan, p, s);
+    case 32: return launch_obs_tile_t<Lat, N, 32>(plan, p, s);
+    case 64: return launch_obs_tile_t<Lat, N, 64>(plan, p, s);
+    default: return launch_obs_tile_t<Lat, N, 128>(plan, p, s);
+  }
+}
+
+template <class Lat>
+static int launch_obs_tile(const sck_plan* plan, const ObsParams& p, cudaStream_t s) {
+  switch (plan->geom.n) {
+    case 1: return launch_obs_tile_n<Lat, 1>(plan, p, s);
+    case 2: return launch_obs_tile_n<Lat, 2>(plan, p, s);
+    default: return launch_obs_tile_n<Lat, 3>(plan, p, s);
+  }
 }
 
 // Sum the partials of every replica in block order; E[r] and M[r][alpha][k] (B x b x n).

@@ -394,8 +394,8 @@ def test_observables_match_oracle_fp64():
 
 
 def test_tiled_observables_match_oracle_fp64():
-    """Float32 storage on periodic boxes whose row count is a multiple of 8 takes the tiled path (bands of rows
-    staged in shared memory as FP64): energies and magnetizations within 1e-12 of the FP64 oracle, masks,
+    """Float32 storage on periodic boxes with 16, 32, 64 or 128 sites per row and a row count that is a multiple
+    of 4 takes the tiled path (bands of rows staged in shared memory as FP64): energies and magnetizations within 1e-12 of the FP64 oracle, masks,
     fields, anisotropy, 2D and 3D, one to three components; a workspace sized before the tuning switches the
     lattice tables off stays valid for the other path."""
     from spin_colour_kernel_b200.sampler import Sampler
@@ -403,12 +403,13 @@ def test_tiled_observables_match_oracle_fp64():
     sq = cr.make("square")
     masked = sy.System("XY square periodic masked", 2, sq, (16, 16), (True, True), {1: 1.0}, h=(0.05, 0.0),
                        mask=W.disk_mask(1, 16, 6.0))
-    cases = [
-        (C.heisenberg_bcc_j1j2(sy, cr, 8), {}),
-        (sy.System("Heisenberg sc", 3, cr.make("sc"), (12, 16, 8), (True,) * 3, {1: -1.0}, h=(0.1, 0.0, 0.2)), {}),
+    cases = [   # row lengths 16, 32, 64, row counts multiples of 4: all take the tiled path
+        (C.heisenberg_bcc_j1j2(sy, cr, 16), {}),
+        (sy.System("Heisenberg sc", 3, cr.make("sc"), (32, 8, 4), (True,) * 3, {1: -1.0}, h=(0.1, 0.0, 0.2)), {}),
         (C.xy_periodic_field(sy, cr, "square", 16), {}),
+        (sy.System("XY triangular", 2, cr.make("triangular"), (64, 12), (True, True), {1: -1.0}), {}),
         (masked, {}),
-        (sy.ising("sc", 8), {"spin_dtype": torch.float32, "packed": False}),
+        (sy.ising("sc", 16), {"spin_dtype": torch.float32, "packed": False}),
     ]
     for s, kw in cases:
         A = Sampler(s, 3, device="cuda", seed=1, **kw)
