@@ -61,6 +61,7 @@ _SIGNATURES = {
     "sck_observables_workspace_size": ([_vp, _i32, ctypes.POINTER(_i64)], _i32),
     "sck_observables": ([_vp, ctypes.POINTER(Buffers), _vp, _i32, _i32, _vp, _vp, _vp, _vp], _i32),
     "sck_observables_noalloc": ([_vp, ctypes.POINTER(Buffers), _vp, _i32, _i32, _vp, _vp, _vp], _i32),
+    "sck_wait_timeouts": ([ctypes.POINTER(_i64)], _i32),
     "sck_pack": ([_vp, _vp, _vp, _vp], _i32),
     "sck_unpack": ([_vp, _vp, _vp, _vp, _vp], _i32),
     "sck_advance": ([_vp, _i32, _vp], _i32),

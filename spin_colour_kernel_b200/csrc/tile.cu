@@ -1,31 +1,36 @@
 // Tile kernels: the class update of vector models on a periodic box with a compile-time bond table, reading
 // every neighbour from shared memory.
 //
-// A block of threads owns a band of TILE_TY rows of two replicas and marches along z. It keeps three planes of
-// the band (z - 1, z, z + 1), each with one halo row on either side and one halo site at either end of every
-// row, in shared memory (both sublattices, every component, float32), filled with cp.async. The class sites of
-// plane z then read their neighbours with shared-memory loads at compile-time offsets from three per-site
-// pointers (one per plane): the 64-bit address arithmetic that the global-memory kernels spend on every
-// neighbour load disappears. Two replicas per thread share the addressing and run the proposal and acceptance in
-// packed float32x2 arithmetic (finish_core in spec.cuh). Neighbours are never sites of the class being
-// updated, so the shared copies never go stale within a launch. Group sums run in bond order, as in the lattice
-// kernels.
+// A block of threads owns a brick of one replica: BR_Z planes x BR_Y rows x the whole row length (one plane in
+// 2D). It copies the brick plus one halo plane and one halo row on every side (both sublattices, every
+// component, float32) into shared memory with one bulk asynchronous copy per row (the copy engine moves the
+// bytes; the threads issue one instruction per row and wait on one mbarrier, with a bounded wait), fills the
+// halo site at each end of every row from the row itself, and then updates the class sites of the brick. Every
+// neighbour is a shared-memory load at a compile-time offset from the site's own shared address: none of the
+// 64-bit address arithmetic that the global-memory kernels spend on each neighbour load is left. A thread takes
+// two class sites of one row and runs the proposal and acceptance of both in packed float32x2 arithmetic
+// (finish_core in spec.cuh). Neighbours are never sites of the class being updated, so the shared copy never
+// goes stale within a launch. Group sums run in bond order, so results are those of the lattice kernels.
 #include "spec.cuh"
 
 namespace sck {
 
-constexpr int TILE_TY = 8;    // rows per band
+constexpr int BR_Y = 4;       // rows per brick
 constexpr int TILE_PAD = 4;   // floats before x = 0 in a shared row: x = -1 sits at TILE_PAD - 1
+constexpr long long kBrickWaitLimit = 1ll << 22;   // mbarrier polls before a brick gives up
 
-template <class Lat, int N, int L1T>
-struct TileDims {
+template <class Lat, int N, int L1T, int BZ>
+struct BrickDims {
   static_assert(Lat::reach == 1, "tile kernels read neighbours at most one cell away");
-  static constexpr int R2 = TILE_TY + 2;               // band rows plus halo rows
-  static constexpr int RS = L1T + 2 * TILE_PAD;        // floats per shared row
-  static constexpr int COMP = R2 * RS;                 // one component of one sublattice
-  static constexpr int REP = Lat::b * N * COMP;        // one replica of one plane
-  static constexpr int SLOT = 2 * REP;                 // two replicas
-  static constexpr int BYTES = 3 * SLOT * 4;
+  static constexpr int R2 = BR_Y + 2;                   // rows with halo
+  static constexpr int P2 = BZ == 1 ? 1 : BZ + 2;       // planes with halo (2D: the one plane)
+  static constexpr int ZO = BZ == 1 ? 0 : 1;            // plane index of the brick's first plane
+  static constexpr int RS = L1T + 2 * TILE_PAD;         // floats per shared row
+  static constexpr int PLANE = R2 * RS;
+  static constexpr int COMP = P2 * PLANE;               // one component of one sublattice
+  static constexpr int FLOATS = Lat::b * N * COMP;
+  static constexpr int ROWS = Lat::b * N * P2 * R2;     // rows copied
+  static constexpr int BYTES = FLOATS * 4 + 16;         // + the mbarrier
 };
 
 struct TileParams {
@@ -34,68 +39,9 @@ struct TileParams {
   int colour, alpha;
 };
 
-__device__ __forceinline__ void tile_wait_all() {
-  asm volatile("cp.async.commit_group;\n" ::);
-  asm volatile("cp.async.wait_group 0;\n" ::);
-}
+static __device__ unsigned long long g_wait_timeouts;   // bounded waits that gave up (sck_wait_timeouts)
 
-// The rows one thread copies are the same on every plane: rows tid / Q + RSTEP i of the slot (replica,
-// sublattice, component, band row), 16-byte chunk tid % Q of each, plus the two halo sites of row tid. Their
-// global offsets within a plane and their shared addresses are worked out once; a plane adds its z offset.
-template <class Lat, int N, int L1T>
-struct TileLoader {
-  using D = TileDims<Lat, N, L1T>;
-  static constexpr int Q = L1T / 4;                       // 16-byte chunks per row
-  static constexpr int RSTEP = 256 / Q;                   // rows per pass of the block
-  static constexpr int ROWS = 2 * Lat::b * N * D::R2;     // rows of a slot
-  static constexpr int MAXR = (ROWS + RSTEP - 1) / RSTEP;
-  static_assert(ROWS <= 256, "one thread per row for the halo sites");
-  long long goff[MAXR];   // element offset of the chunk within the pair of replicas, without z
-  uint32_t soff[MAXR];    // byte offset of the chunk within a slot
-  long long hoff;         // halo sites of row tid: element offset of x = 0 of that row, without z
-  uint32_t hs;            // byte offset of x = 0 of that row within a slot
-  int nrow;
-  bool halo;
-
-  __device__ __forceinline__ TileLoader(const Geometry& g, bool two, int y0) {
-    const int q = threadIdx.x % Q;
-    nrow = 0;
-#pragma unroll
-    for (int i = 0; i < MAXR; ++i) {
-      const int row = threadIdx.x / Q + RSTEP * i;
-      goff[i] = 0;
-      soff[i] = 0;
-      if (row < ROWS) {
-        goff[i] = row_offset(g, two, y0, row) + 4 * q;
-        soff[i] = 4u * (uint32_t)(row * D::RS + TILE_PAD + 4 * q);
-        nrow = i + 1;
-      }
-    }
-    halo = threadIdx.x < ROWS;
-    hoff = halo ? row_offset(g, two, y0, threadIdx.x) : 0;
-    hs = 4u * (uint32_t)(threadIdx.x * D::RS + TILE_PAD);
-  }
-  __device__ __forceinline__ static long long row_offset(const Geometry& g, bool two, int y0, int row) {
-    const int r = row % D::R2, akj = row / D::R2, k = akj % N, aj = akj / N, a = aj % Lat::b, j = aj / Lat::b;
-    int y = y0 - 1 + r;
-    y = y < 0 ? y + g.L2 : (y >= g.L2 ? y - g.L2 : y);
-    return (long long)(two ? j : 0) * N * g.nsite + (long long)k * g.nsite + (long long)a * g.plane +
-           (long long)y * L1T;
-  }
-  // plane zu (-1 .. L3, wrapped) into the slot at shared address `slot`
-  __device__ __forceinline__ void load(const Geometry& g, const float* src, uint32_t slot, int zu) const {
-    const int zz = zu < 0 ? zu + g.L3 : (zu >= g.L3 ? zu - g.L3 : zu);
-    const float* base = src + (long long)zz * g.L2 * L1T;
-#pragma unroll
-    for (int i = 0; i < MAXR; ++i)
-      if (i < nrow)
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(slot + soff[i]), "l"(base + goff[i]));
-    if (halo) {
-      asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(slot + hs - 4), "l"(base + hoff + L1T - 1));
-      asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(slot + hs + 4 * L1T), "l"(base + hoff));
-    }
-  }
-};
+__device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 // 32-bit shared-memory load at a compile-time byte offset from a register address
 template <int OFF>
@@ -105,21 +51,34 @@ __device__ __forceinline__ float lds(uint32_t addr) {
   return v;
 }
 
-template <class Lat, int A, int N, int L1T>
-__device__ __forceinline__ void tile_site(const Common& c, const float (&J)[SCK_MAX_GROUPS], const uint32_t (&pl)[3],
-                                          int zu, int ty, int x, int y, int rep0, bool two, int32_t key) {
-  using D = TileDims<Lat, N, L1T>;
+__device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(mbar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// the two class sites xa and xa + P of row y0 + ty, plane z0 + tz (lane .y absent when !two)
+template <class Lat, int A, int N, int L1T, int BZ>
+__device__ __forceinline__ void brick_pair(const Common& c, const float (&J)[SCK_MAX_GROUPS], uint32_t sbase, int rep,
+                                           int tz, int ty, int xa, int y, int z, bool two, int32_t key) {
+  using D = BrickDims<Lat, N, L1T, BZ>;
   const Geometry& g = c.g;
-  const int own = A * g.plane + (zu * g.L2 + y) * L1T + x;
-  if (g.has_mask && c.mask[own] == 0) return;
-  const uint32_t site = 4u * (uint32_t)((ty + 1) * D::RS + TILE_PAD + x);
-  // one shared address per plane z - 1, z, z + 1; every neighbour is a compile-time offset from one of them
-  const uint32_t pz[3] = {pl[0] + site, pl[1] + site, pl[2] + site};
+  const int xb = two ? xa + c.P : xa;
+  const int own_a = A * g.plane + (z * g.L2 + y) * L1T + xa, own_b = own_a + (xb - xa);
+  const bool la = !g.has_mask || c.mask[own_a] != 0;
+  const bool lb = two && (!g.has_mask || c.mask[own_b] != 0);
+  if (!la && !lb) return;
+  const int row = (tz + D::ZO) * D::PLANE + (ty + 1) * D::RS + TILE_PAD;
+  const uint32_t qa = sbase + 4u * (uint32_t)(row + xa), qb = sbase + 4u * (uint32_t)(row + xb);
   float2 s[N], v[N];
   static_for<0, N>([&](auto kc) {
     constexpr int k = decltype(kc)::value;
     constexpr int o = 4 * (A * N + k) * D::COMP;
-    s[k] = make_float2(lds<o>(pz[1]), lds<o + 4 * D::REP>(pz[1]));
+    s[k] = make_float2(lds<o>(qa), lds<o>(qb));
     v[k] = f2(0.0f);
   });
   static_for<0, Lat::groups>([&](auto gc) {
@@ -130,11 +89,10 @@ __device__ __forceinline__ void tile_site(const Common& c, const float (&J)[SCK_
     for (int k = 0; k < N; ++k) gs[k] = f2(0.0f);
     static_for<R::begin, R::end>([&](auto ic) {
       constexpr BondC bd = Lat::bond(A, decltype(ic)::value);
-      constexpr int off = 4 * (bd.a2 * N * D::COMP + bd.dy * D::RS + bd.dx);
-      const uint32_t q = pz[bd.dz + 1];
+      constexpr int off = 4 * (bd.a2 * N * D::COMP + bd.dz * D::PLANE + bd.dy * D::RS + bd.dx);
       static_for<0, N>([&](auto kc) {
         constexpr int k = decltype(kc)::value;
-        gs[k] = __fadd2_rn(gs[k], make_float2(lds<off + 4 * k * D::COMP>(q), lds<off + 4 * (D::REP + k * D::COMP)>(q)));
+        gs[k] = __fadd2_rn(gs[k], make_float2(lds<off + 4 * k * D::COMP>(qa), lds<off + 4 * k * D::COMP>(qb)));
       });
     });
 #pragma unroll
@@ -145,76 +103,108 @@ __device__ __forceinline__ void tile_site(const Common& c, const float (&J)[SCK_
     if (c.hnz[k]) v[k] = __fadd2_rn(v[k], f2(c.h[k]));
   float2 t[N];
   bool acc0, acc1;
-  const int rep1 = two ? rep0 + 1 : rep0;
-  finish_pair<N>(c, own, rep0, rep1, two, key, s, v, t, acc0, acc1);
+  const float beta = c.beta[rep];
+  finish_core<N>(c, counter_of(rep, g.nsite, own_a), counter_of(rep, g.nsite, own_b), two, own_a, own_b,
+                 make_float2(beta, beta), key, s, v, t, acc0, acc1);
   const size_t NS = (size_t)g.nsite;
-  float* po = (float*)c.dst + (size_t)rep0 * N * NS + own;
-  if (acc0) {
+  float* po = (float*)c.dst + (size_t)rep * N * NS;
+  if (la && acc0) {
 #pragma unroll
-    for (int k = 0; k < N; ++k) po[k * NS] = t[k].x;
+    for (int k = 0; k < N; ++k) po[k * NS + own_a] = t[k].x;
   }
-  if (two && acc1) {
+  if (lb && acc1) {
 #pragma unroll
-    for (int k = 0; k < N; ++k) po[(N + k) * NS] = t[k].y;
+    for (int k = 0; k < N; ++k) po[k * NS + own_b] = t[k].y;
   }
 }
 
-// Grid (L2 / TILE_TY bands, ceil(B / 2) replica pairs), 256 threads.
-template <class Lat, int N, int L1T>
-__global__ void __launch_bounds__(256) tile_class_kernel(const __grid_constant__ TileParams p) {
-  extern __shared__ __align__(16) float sm[];
+// Grid ((L2 / BR_Y) x (L3 / BZ) bricks, B replicas), 256 threads.
+template <class Lat, int N, int L1T, int BZ>
+__global__ void __launch_bounds__(256) brick_class_kernel(const __grid_constant__ TileParams p) {
+  using D = BrickDims<Lat, N, L1T, BZ>;
+  extern __shared__ __align__(128) float sm[];
   const Common& c = p.c;
   const Geometry& g = c.g;
-  const int y0 = blockIdx.x * TILE_TY;
-  const int rep0 = 2 * blockIdx.y;
-  const bool two = rep0 + 1 < c.B;
-  const float* src0 = (const float*)c.src + (size_t)rep0 * N * g.nsite;
-  const TileLoader<Lat, N, L1T> ld(g, two, y0);
-  const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(sm);
-  constexpr uint32_t SLOT_BYTES = 4u * TileDims<Lat, N, L1T>::SLOT;
-  ld.load(g, src0, sbase + 2 * SLOT_BYTES, -1);
-  ld.load(g, src0, sbase, 0);
-  ld.load(g, src0, sbase + SLOT_BYTES, 1);
-  tile_wait_all();
+  const int nby = g.L2 / BR_Y;
+  const int y0 = (blockIdx.x % nby) * BR_Y, z0 = (blockIdx.x / nby) * BZ;
+  const int rep = blockIdx.y;
+  const uint32_t sbase = saddr(sm);
+  const uint32_t mbar = sbase + 4u * D::FLOATS;
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mbar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(mbar), "r"(D::ROWS * L1T * 4)
+                 : "memory");
+  }
+  __syncthreads();
+  const float* src = (const float*)c.src + (size_t)rep * N * g.nsite;
+  for (int row = threadIdx.x; row < D::ROWS; row += blockDim.x) {
+    const int ry = row % D::R2, rest = row / D::R2, pz = rest % D::P2, ak = rest / D::P2, k = ak % N, a = ak / N;
+    int y = y0 - 1 + ry;
+    y = y < 0 ? y + g.L2 : (y >= g.L2 ? y - g.L2 : y);
+    int z = z0 - D::ZO + pz;
+    z = z < 0 ? z + g.L3 : (z >= g.L3 ? z - g.L3 : z);
+    const float* gr = src + (size_t)k * g.nsite + (size_t)a * g.plane + ((size_t)z * g.L2 + y) * L1T;
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+            sbase + 4u * (uint32_t)(row * D::RS + TILE_PAD)),
+        "l"(gr), "r"(L1T * 4), "r"(mbar)
+        : "memory");
+  }
+  long long polls = 0;
+  bool ready = false;
+  while (!(ready = mbar_try_wait(mbar, 0)) && ++polls < kBrickWaitLimit) {
+  }
+  if (__syncthreads_or(!ready)) {
+    // gave up (every thread of the block agrees): count it, wait (bounded again) for the copies still in
+    // flight, leave the brick unchanged
+    if (threadIdx.x == 0) atomicAdd(&g_wait_timeouts, 1ull);
+    for (long long i = 0; i < kBrickWaitLimit && !mbar_try_wait(mbar, 0); ++i) {
+    }
+    return;
+  }
+  // halo sites: x = -1 is x = L1 - 1, x = L1 is x = 0
+  for (int row = threadIdx.x; row < D::ROWS; row += blockDim.x) {
+    float* r = sm + row * D::RS + TILE_PAD;
+    r[-1] = r[L1T - 1];
+    r[L1T] = r[0];
+  }
   __syncthreads();
   const int32_t key = sweep_key_at(c.state, 0);
-  const int spr = c.bx;                      // class sites per row at most
+  const int pairs = (c.bx + 1) >> 1;   // pairs of class sites per row
   const int alpha = p.alpha;
-  uint32_t pl[3] = {sbase + 2 * SLOT_BYTES, sbase, sbase + SLOT_BYTES};   // planes zu - 1, zu, zu + 1 at zu = 0
-  for (int zu = 0; zu < g.L3; ++zu) {
-    for (int t = threadIdx.x; t < TILE_TY * spr; t += blockDim.x) {
-      const int ty = t / spr, j = t - ty * spr;
-      const int y = y0 + ty;
-      const int x = first_class_x(c, p.colour, alpha, y, zu) + c.P * j;
-      if (x >= L1T) continue;
-      static_for<0, Lat::b>([&](auto ac) {
-        constexpr int a = decltype(ac)::value;
-        if (a == alpha) tile_site<Lat, a, N, L1T>(c, p.J[a], pl, zu, ty, x, y, rep0, two, key);
-      });
-    }
-    const uint32_t rot = pl[0];   // the ring turns: zu's slot becomes z - 1, zu + 1's becomes z
-    pl[0] = pl[1];
-    pl[1] = pl[2];
-    pl[2] = rot;
-    __syncthreads();   // every thread is done with plane zu - 1
-    if (zu + 1 < g.L3) {
-      ld.load(g, src0, pl[2], zu + 2);
-      tile_wait_all();
-      __syncthreads();
-    }
+  for (int t = threadIdx.x; t < BZ * BR_Y * pairs; t += blockDim.x) {
+    const int jp = t % pairs, r2 = t / pairs, ty = r2 % BR_Y, tz = r2 / BR_Y;
+    const int y = y0 + ty, z = z0 + tz;
+    const int xa = first_class_x(c, p.colour, alpha, y, z) + 2 * c.P * jp;
+    if (xa >= L1T) continue;
+    const bool two = xa + c.P < L1T;
+    static_for<0, Lat::b>([&](auto ac) {
+      constexpr int a = decltype(ac)::value;
+      if (a == alpha) brick_pair<Lat, a, N, L1T, BZ>(c, p.J[a], sbase, rep, tz, ty, xa, y, z, two, key);
+    });
   }
+}
+
+template <class Lat, int N, int L1T, int BZ>
+static int launch_brick(const TileParams& p, cudaStream_t s) {
+  using D = BrickDims<Lat, N, L1T, BZ>;
+  const dim3 grid((p.c.g.L2 / BR_Y) * (p.c.g.L3 / BZ), p.c.B);
+  const int rc = cuda_status(cudaFuncSetAttribute(brick_class_kernel<Lat, N, L1T, BZ>,
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, D::BYTES),
+                             "tile shared memory");
+  if (rc != SCK_OK) return rc;
+  brick_class_kernel<Lat, N, L1T, BZ><<<grid, 256, D::BYTES, s>>>(p);
+  return cuda_status(cudaGetLastError(), "tile class launch");
 }
 
 template <class Lat, int N, int L1T>
 static int launch_tile_lnt(const TileParams& p, cudaStream_t s) {
-  using D = TileDims<Lat, N, L1T>;
-  const dim3 grid(p.c.g.L2 / TILE_TY, (p.c.B + 1) / 2);
-  const int rc = cuda_status(cudaFuncSetAttribute(tile_class_kernel<Lat, N, L1T>,
-                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, D::BYTES),
-                             "tile shared memory");
-  if (rc != SCK_OK) return rc;
-  tile_class_kernel<Lat, N, L1T><<<grid, 256, D::BYTES, s>>>(p);
-  return cuda_status(cudaGetLastError(), "tile class launch");
+  if constexpr (Lat::dim == 3)
+    return launch_brick<Lat, N, L1T, 4>(p, s);
+  else
+    return launch_brick<Lat, N, L1T, 1>(p, s);
 }
 
 template <class Lat, int N>
@@ -231,12 +221,16 @@ static int launch_tile_l(const TileParams& p, cudaStream_t s) {
   return p.c.g.n == 2 ? launch_tile_ln<Lat, 2>(p, s) : launch_tile_ln<Lat, 3>(p, s);
 }
 
+template <class Lat, int N>
+static constexpr int tile_bytes_n(int L1) {
+  constexpr int BZ = Lat::dim == 3 ? 4 : 1;
+  return L1 == 32 ? BrickDims<Lat, N, 32, BZ>::BYTES
+                  : (L1 == 64 ? BrickDims<Lat, N, 64, BZ>::BYTES : BrickDims<Lat, N, 128, BZ>::BYTES);
+}
+
 template <class Lat>
 static constexpr int tile_bytes(int n, int L1) {
-  return n == 2 ? (L1 == 32 ? TileDims<Lat, 2, 32>::BYTES : L1 == 64 ? TileDims<Lat, 2, 64>::BYTES
-                                                                      : TileDims<Lat, 2, 128>::BYTES)
-                : (L1 == 32 ? TileDims<Lat, 3, 32>::BYTES : L1 == 64 ? TileDims<Lat, 3, 64>::BYTES
-                                                                      : TileDims<Lat, 3, 128>::BYTES);
+  return n == 2 ? tile_bytes_n<Lat, 2>(L1) : tile_bytes_n<Lat, 3>(L1);
 }
 
 static int tile_smem(const sck_plan* plan) {
@@ -254,9 +248,10 @@ static int tile_smem(const sck_plan* plan) {
 bool tile_kernel_ok(const sck_plan* plan) {
   const Geometry& g = plan->geom;
   if (plan->kernel_kind != 3 || plan->spec == 0 || plan->mode != SCK_MODE_F32 || g.n < 2) return false;
+  if (plan->Bp > 65535) return false;   // one grid row per replica
   if (g.L1 != 32 && g.L1 != 64 && g.L1 != 128) return false;
-  if (!g.per[0] || !g.per[1] || g.L2 % TILE_TY != 0) return false;
-  if (g.dim == 3 && (!g.per[2] || g.L3 < 3)) return false;
+  if (!g.per[0] || !g.per[1] || g.L2 % BR_Y != 0 || g.L2 < 3) return false;
+  if (g.dim == 3 && (!g.per[2] || g.L3 % 4 != 0 || g.L3 < 4)) return false;
   return tile_smem(plan) <= 220 * 1024;
 }
 
@@ -279,3 +274,15 @@ int launch_tile_class(const sck_plan* plan, const Common& c, int colour, int alp
 }
 
 }  // namespace sck
+
+extern "C" int sck_wait_timeouts(int64_t* count) {
+  if (count == nullptr) {
+    sck::set_error("null output");
+    return SCK_ERR_INVALID;
+  }
+  unsigned long long v = 0;
+  const int rc = sck::cuda_status(cudaMemcpyFromSymbol(&v, sck::g_wait_timeouts, sizeof(v)), "wait timeouts");
+  if (rc != SCK_OK) return rc;
+  *count = (int64_t)v;
+  return SCK_OK;
+}

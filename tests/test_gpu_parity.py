@@ -8,6 +8,7 @@ probability can flip. The tests report the fraction of spins outside the toleran
 
 from __future__ import annotations
 
+import ctypes
 from pathlib import Path
 
 import numpy as np
@@ -18,6 +19,7 @@ import cases as C
 from oracle import bitwise as obw
 from oracle import observables as obs
 from oracle import sweep as osw
+from spin_colour_kernel_b200 import _lib as L
 from spin_colour_kernel_b200 import crystals as cr
 from spin_colour_kernel_b200 import system as sy
 
@@ -253,7 +255,9 @@ def test_segment_kernels_agree_with_lattice_kernels(name):
 
 
 TILE_SYSTEMS = {
-    "heis_bcc_j1j2_64x8x6": SEG_SYSTEMS["heis_bcc_j1j2_64x8x6"],
+    "heis_bcc_j1j2_64x8x8": lambda: sy.System("Heisenberg bcc J1-J2", 3, cr.make("bcc", (1, 2)), (64, 8, 8),
+                                              (True,) * 3, {1: 1.0, 2: 0.3}, h=(0.0, 0.0, 0.1),
+                                              cubic_k1=np.full((2, 8, 8, 64), 0.05, np.float32)),
     "heis_sc_32x16x4": lambda: sy.System("Heisenberg sc", 3, cr.make("sc"), (32, 16, 4), (True,) * 3, {1: -1.0},
                                          h=(0.2, 0.0, 0.1)),
     "heis_fcc_32x8x4": lambda: sy.System("Heisenberg fcc", 3, cr.make("fcc"), (32, 8, 4), (True,) * 3, {1: 1.0}),
@@ -270,9 +274,9 @@ TILE_SYSTEMS = {
 
 @pytest.mark.parametrize("name", sorted(TILE_SYSTEMS))
 def test_tile_kernels_equal_lattice_kernels(name):
-    """Tile kernels (bands of rows staged in shared memory, neighbours read at compile-time offsets) run the same
-    float32x2 arithmetic in the same bond order as the lattice kernels: spins bit-identical, odd replica count,
-    masks, 2D and 3D, one to four sublattices, colourings of any x-period."""
+    """Tile kernels (bricks staged in shared memory by bulk copies, neighbours read at compile-time offsets) run
+    the same float32 arithmetic in the same bond order as the lattice kernels: spins bit-identical, odd replica
+    count, masks, 2D and 3D, one to four sublattices, colourings of any x-period; no bounded wait gave up."""
     from spin_colour_kernel_b200.sampler import Sampler
     s = TILE_SYSTEMS[name]()
     B = 5
@@ -283,10 +287,15 @@ def test_tile_kernels_equal_lattice_kernels(name):
         X.set_temperature(torch.linspace(0.4, 3.0, B))
     S1 = A.init_spins(seed=7)
     S2 = S1.clone()
+    before = ctypes.c_int64()
+    L.check(L.lib().sck_wait_timeouts(ctypes.byref(before)))
     A.sweep(S1, 3)
     R.sweep(S2, 3)
     assert torch.equal(S1, S2)
     assert not torch.equal(S1, A.init_spins(seed=7))
+    after = ctypes.c_int64()
+    L.check(L.lib().sck_wait_timeouts(ctypes.byref(after)))
+    assert after.value == before.value
 
 
 @pytest.mark.parametrize("name", ["ising_square8", "nanodot_small", "w3_heis_bcc4_j1j2", "w4_xy_triangular12_disk",
