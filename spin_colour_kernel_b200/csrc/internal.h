@@ -134,6 +134,7 @@ int launch_sequential(const sck_plan* plan, const Common& c, cudaStream_t s);
 int launch_bitwise_class(const sck_plan* plan, const Common& c, int colour, int alpha, cudaStream_t s);
 int launch_bitwise_sequential(const sck_plan* plan, const Common& c, cudaStream_t s);
 int obs_blocks_per_rep(const sck_plan* plan, int batch);
+int made_wait_timeouts(unsigned long long* count);   // bounded waits of the learned proposal's kernels that gave up
 int launch_observables(const sck_plan* plan, const void* spins, int storage, int batch, const int8_t* mask,
                        const float* k1, double* E, double* M, void* workspace, cudaStream_t s);
 int launch_pack(const sck_plan* plan, const int8_t* spins, int32_t* words, cudaStream_t s);

@@ -227,6 +227,163 @@ __global__ void __launch_bounds__(128) gemm_kernel(GemmArgs g) {
     }
 }
 
+// ================================================================================ tcgen05 forward GEMM
+// C[M x N] = epilogue(A[M x K] B[N x K]^T) for the forward layers (both operands K-major), on the fifth-generation
+// tensor cores: a block of 128 threads owns 128 rows and all N columns; per 32-wide K chunk the threads stage
+// A and B in shared memory in the canonical no-swizzle K-major layout (8-row x 16-byte core matrices: 128 bytes
+// apart along M or N, 16 x 128 bytes apart along K), one thread issues two tcgen05.mma (M 128, N, K 16, bf16
+// in, FP32 accumulating in tensor memory) and commits them to an mbarrier that all threads wait on (bounded)
+// before the next chunk overwrites the stage. The epilogue reads the accumulator with tcgen05.ld (warp w reads
+// rows 32 w .. 32 w + 31) and applies bias, ReLU and the bfloat16 conversion.
+constexpr int UM = 128;     // rows per block (MMA M)
+constexpr int UKC = 32;     // K per staged chunk (two K16 MMAs)
+constexpr long long kUmmaWaitLimit = 1ll << 22;
+
+static __device__ unsigned long long g_made_wait_timeouts;
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;   // descriptor version of sm100; base offset 0, no swizzle
+  return d;
+}
+
+__device__ __forceinline__ bool umma_try_wait(uint32_t mbar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(mbar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+template <int N, int EPI>
+__global__ void __launch_bounds__(128) umma_gemm_kernel(GemmArgs g) {
+  __shared__ __align__(1024) __nv_bfloat16 As[UM * UKC];
+  __shared__ __align__(1024) __nv_bfloat16 Bs[N * UKC];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tmem_slot;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.x * UM;
+  const uint32_t mb = smem_u32(&mbar);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_slot)),
+                 "r"(N < 32 ? 32 : N)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mb) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = tmem_slot;
+  constexpr uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
+                             ((uint32_t)(UM >> 4) << 24);   // FP32 accumulator, bf16 A and B, K-major
+  constexpr uint32_t A_LBO = (UM / 8) * 128, B_LBO = (N / 8) * 128;
+  const uint32_t a_s = smem_u32(As), b_s = smem_u32(Bs);
+  const int nch = g.K / UKC;
+  uint32_t phase = 0;
+  bool ok = true;
+  for (int ch = 0; ch < nch && ok; ++ch) {
+    const int k0 = ch * UKC;
+    for (int i = tid; i < UM * (UKC / 8); i += 128) {
+      const int r = i / (UKC / 8), c = i % (UKC / 8);
+      cp_async16(As + ((c * (UM / 8) + (r >> 3)) * 64 + (r & 7) * 8), g.A + (long long)(m0 + r) * g.lda + k0 + 8 * c, 16);
+    }
+    for (int i = tid; i < N * (UKC / 8); i += 128) {
+      const int n = i / (UKC / 8), c = i % (UKC / 8);
+      cp_async16(Bs + ((c * (N / 8) + (n >> 3)) * 64 + (n & 7) * 8), g.B + (long long)n * g.ldb + k0 + 8 * c, 16);
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");   // the tensor cores read what we wrote
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+#pragma unroll
+      for (int s = 0; s < UKC / 16; ++s) {
+        const uint64_t ad = umma_desc(a_s + s * 2 * A_LBO, A_LBO, 128);
+        const uint64_t bd = umma_desc(b_s + s * 2 * B_LBO, B_LBO, 128);
+        const uint32_t acc = (ch > 0 || s > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n}\n" ::"r"(tmem),
+            "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0u)
+            : "memory");
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(mb)
+                   : "memory");
+    }
+    long long polls = 0;
+    bool done = false;
+    while (!(done = umma_try_wait(mb, phase)) && ++polls < kUmmaWaitLimit) {
+    }
+    phase ^= 1u;
+    ok = !__syncthreads_or(!done);
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  if (ok) {
+    const int row = m0 + 32 * warp + lane;
+#pragma unroll 1
+    for (int col = 0; col < N; col += 8) {
+      uint32_t v[8];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+          : "r"(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)col));
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+      float f[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) f[e] = __uint_as_float(v[e]) + g.bias[col + e];
+      if (EPI == EPI_BIAS_RELU_BF16) {
+        uint4 o;
+        o.x = pack_bf16(fmaxf(f[0], 0.f), fmaxf(f[1], 0.f));
+        o.y = pack_bf16(fmaxf(f[2], 0.f), fmaxf(f[3], 0.f));
+        o.z = pack_bf16(fmaxf(f[4], 0.f), fmaxf(f[5], 0.f));
+        o.w = pack_bf16(fmaxf(f[6], 0.f), fmaxf(f[7], 0.f));
+        *(uint4*)((__nv_bfloat16*)g.C + (long long)row * g.ldc + col) = o;
+      } else {
+        float* o = (float*)g.C + (long long)row * g.ldc + col;
+        *(float4*)o = make_float4(f[0], f[1], f[2], f[3]);
+        *(float4*)(o + 4) = make_float4(f[4], f[5], f[6], f[7]);
+      }
+    }
+  } else if (tid == 0) {
+    atomicAdd(&g_made_wait_timeouts, 1ull);
+    // the MMAs of the chunk that timed out may still run: wait for them, bounded, before freeing their memory
+    for (long long i = 0; i < kUmmaWaitLimit && !umma_try_wait(mb, phase ^ 1u); ++i) {
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(N < 32 ? 32 : N)
+                 : "memory");
+}
+
+}  // namespace made
+
+int made_wait_timeouts(unsigned long long* v) {
+  return cuda_status(cudaMemcpyFromSymbol(v, made::g_made_wait_timeouts, sizeof(*v)), "learned wait timeouts");
+}
+
+namespace made {
+
+template <int EPI>
+int umma_gemm(const GemmArgs& g, cudaStream_t s) {
+  const dim3 grid(g.M / UM);
+  if (g.N == H)
+    umma_gemm_kernel<H, EPI><<<grid, 128, 0, s>>>(g);
+  else
+    umma_gemm_kernel<NSP, EPI><<<grid, 128, 0, s>>>(g);
+  return cuda_status(cudaGetLastError(), "made tcgen05 gemm");
+}
+
 template <bool A_K, bool B_K, int EPI>
 int gemm(const GemmArgs& g, int splits, cudaStream_t s) {
   dim3 grid((g.N + BN - 1) / BN, g.M / BM, splits);
@@ -762,16 +919,18 @@ int forward_layers(const void* params, const __nv_bfloat16* x, int M, char* ws, 
     g.kchunk = in_cols(l);
     g.bias = master + off_b(l);
     int rc;
+    // batches of whole 128-row tiles run on tcgen05; others on the mma.sync kernel
+    const bool umma = M % UM == 0;
     if (l < 3) {
       g.C = ws + t.h[l];
       g.ldc = H;
-      rc = gemm<true, true, EPI_BIAS_RELU_BF16>(g, 1, s);
+      rc = umma ? umma_gemm<EPI_BIAS_RELU_BF16>(g, s) : gemm<true, true, EPI_BIAS_RELU_BF16>(g, 1, s);
       in = (const __nv_bfloat16*)(ws + t.h[l]);
       ld = H;
     } else {
       g.C = ws + t.logits;
       g.ldc = NSP;
-      rc = gemm<true, true, EPI_BIAS_F32>(g, 1, s);
+      rc = umma ? umma_gemm<EPI_BIAS_F32>(g, s) : gemm<true, true, EPI_BIAS_F32>(g, 1, s);
     }
     if (rc) return rc;
   }

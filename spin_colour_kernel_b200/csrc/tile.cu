@@ -280,9 +280,10 @@ extern "C" int sck_wait_timeouts(int64_t* count) {
     sck::set_error("null output");
     return SCK_ERR_INVALID;
   }
-  unsigned long long v = 0;
-  const int rc = sck::cuda_status(cudaMemcpyFromSymbol(&v, sck::g_wait_timeouts, sizeof(v)), "wait timeouts");
+  unsigned long long v = 0, w = 0;
+  int rc = sck::cuda_status(cudaMemcpyFromSymbol(&v, sck::g_wait_timeouts, sizeof(v)), "wait timeouts");
+  if (rc == SCK_OK) rc = sck::made_wait_timeouts(&w);
   if (rc != SCK_OK) return rc;
-  *count = (int64_t)v;
+  *count = (int64_t)(v + w);
   return SCK_OK;
 }

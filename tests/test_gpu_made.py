@@ -62,6 +62,28 @@ def test_forward_matches_oracle(groups):
     assert np.abs(logq.cpu().numpy() - lq_ref).max() < 0.1
 
 
+def test_tcgen05_forward_matches_mma_sync_forward():
+    """Batches of whole 128-row tiles take the tcgen05 GEMMs (accumulator in tensor memory), others the mma.sync
+    kernel: the same rows give the same logits up to FP32 summation order (and the rare bfloat16 rounding tie of
+    an activation), and no bounded wait gives up."""
+    _need_gpu()
+    import ctypes
+    from spin_colour_kernel_b200 import _lib as L
+    from spin_colour_kernel_b200.learned import BlockProposal
+    P = BlockProposal(16, 1, groups=16, params=_random_params(11))
+    b, x = _inputs(256, 12)
+    X = _to_dev(b, x)
+    before = ctypes.c_int64()
+    L.check(L.lib().sck_wait_timeouts(ctypes.byref(before)))
+    l_umma, _ = P.forward(X)          # 256 rows: tcgen05
+    l_sync, _ = P.forward(X[:192])    # 192 rows: mma.sync
+    d = np.abs(l_umma[:192].cpu().numpy() - l_sync.cpu().numpy())
+    assert np.median(d) < 1e-5 and d.max() < 0.05, (np.median(d), d.max())
+    after = ctypes.c_int64()
+    L.check(L.lib().sck_wait_timeouts(ctypes.byref(after)))
+    assert after.value == before.value
+
+
 @pytest.mark.parametrize("groups", [16, 64])
 def test_gradients_match_oracle(groups):
     _need_gpu()
