@@ -261,50 +261,83 @@ __device__ __forceinline__ bool umma_try_wait(uint32_t mbar, uint32_t parity) {
 
 template <int N, int EPI>
 __global__ void __launch_bounds__(128) umma_gemm_kernel(GemmArgs g) {
-  __shared__ __align__(1024) __nv_bfloat16 As[UM * UKC];
-  __shared__ __align__(1024) __nv_bfloat16 Bs[N * UKC];
-  __shared__ __align__(8) uint64_t mbar;
-  __shared__ uint32_t tmem_slot;
+  // two stages: the copies of chunk ch + 1 run while the tensor cores multiply chunk ch
+  extern __shared__ __align__(1024) unsigned char usm[];
+  __nv_bfloat16* As = (__nv_bfloat16*)usm;                                    // [2][UM * UKC]
+  __nv_bfloat16* Bs = (__nv_bfloat16*)(usm + 2 * UM * UKC * 2);               // [2][N * UKC]
+  uint64_t* mbar = (uint64_t*)(usm + 2 * (UM + N) * UKC * 2);                 // [2]
+  uint32_t* tmem_slot = (uint32_t*)(mbar + 2);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.x * UM;
-  const uint32_t mb = smem_u32(&mbar);
+  const uint32_t mb0 = smem_u32(mbar), mb1 = smem_u32(mbar + 1);
   if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_slot)),
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)),
                  "r"(N < 32 ? 32 : N)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
   }
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mb) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mb0) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mb1) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-  const uint32_t tmem = tmem_slot;
+  const uint32_t tmem = *tmem_slot;
   constexpr uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
                              ((uint32_t)(UM >> 4) << 24);   // FP32 accumulator, bf16 A and B, K-major
   constexpr uint32_t A_LBO = (UM / 8) * 128, B_LBO = (N / 8) * 128;
-  const uint32_t a_s = smem_u32(As), b_s = smem_u32(Bs);
   const int nch = g.K / UKC;
-  uint32_t phase = 0;
-  bool ok = true;
-  for (int ch = 0; ch < nch && ok; ++ch) {
-    const int k0 = ch * UKC;
+  auto stage = [&](int ch) {
+    const int k0 = ch * UKC, b = ch & 1;
+    __nv_bfloat16* as = As + b * UM * UKC;
+    __nv_bfloat16* bs = Bs + b * N * UKC;
     for (int i = tid; i < UM * (UKC / 8); i += 128) {
       const int r = i / (UKC / 8), c = i % (UKC / 8);
-      cp_async16(As + ((c * (UM / 8) + (r >> 3)) * 64 + (r & 7) * 8), g.A + (long long)(m0 + r) * g.lda + k0 + 8 * c, 16);
+      cp_async16(as + ((c * (UM / 8) + (r >> 3)) * 64 + (r & 7) * 8), g.A + (long long)(m0 + r) * g.lda + k0 + 8 * c,
+                 16);
     }
     for (int i = tid; i < N * (UKC / 8); i += 128) {
       const int n = i / (UKC / 8), c = i % (UKC / 8);
-      cp_async16(Bs + ((c * (N / 8) + (n >> 3)) * 64 + (n & 7) * 8), g.B + (long long)n * g.ldb + k0 + 8 * c, 16);
+      cp_async16(bs + ((c * (N / 8) + (n >> 3)) * 64 + (n & 7) * 8), g.B + (long long)n * g.ldb + k0 + 8 * c, 16);
     }
     cp_async_commit();
-    cp_async_wait<0>();
+  };
+  // bounded wait of every thread on a stage's mbarrier; false (for the whole block) when it gave up
+  uint32_t ph[2] = {0u, 0u};
+  auto wait_stage = [&](int b) {
+    const uint32_t mb = b ? mb1 : mb0;
+    long long polls = 0;
+    bool done = false;
+    while (!(done = umma_try_wait(mb, ph[b])) && ++polls < kUmmaWaitLimit) {
+    }
+    ph[b] ^= 1u;
+    return !__syncthreads_or(!done);
+  };
+  bool ok = true;
+  int pending = -1;   // stage whose products the timeout path must still drain
+  stage(0);
+  for (int ch = 0; ch < nch && ok; ++ch) {
+    const int b = ch & 1;
+    if (ch + 1 < nch) {
+      if (ch >= 1) {   // chunk ch - 1 used the other stage: its products must be done before it is refilled
+        ok = wait_stage(b ^ 1);
+        if (!ok) {
+          pending = b ^ 1;
+          break;
+        }
+      }
+      stage(ch + 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");   // the tensor cores read what we wrote
     __syncthreads();
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      const uint32_t a_s = smem_u32(As + b * UM * UKC), b_s = smem_u32(Bs + b * N * UKC);
 #pragma unroll
       for (int s = 0; s < UKC / 16; ++s) {
         const uint64_t ad = umma_desc(a_s + s * 2 * A_LBO, A_LBO, 128);
@@ -316,15 +349,13 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(GemmArgs g) {
             "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0u)
             : "memory");
       }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(mb)
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(b ? mb1 : mb0)
                    : "memory");
     }
-    long long polls = 0;
-    bool done = false;
-    while (!(done = umma_try_wait(mb, phase)) && ++polls < kUmmaWaitLimit) {
-    }
-    phase ^= 1u;
-    ok = !__syncthreads_or(!done);
+  }
+  if (ok) {   // the last commit covers every product issued before it
+    ok = wait_stage((nch - 1) & 1);
+    if (!ok) pending = (nch - 1) & 1;
   }
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   if (ok) {
@@ -353,11 +384,13 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(GemmArgs g) {
         *(float4*)(o + 4) = make_float4(f[4], f[5], f[6], f[7]);
       }
     }
-  } else if (tid == 0) {
-    atomicAdd(&g_made_wait_timeouts, 1ull);
-    // the MMAs of the chunk that timed out may still run: wait for them, bounded, before freeing their memory
-    for (long long i = 0; i < kUmmaWaitLimit && !umma_try_wait(mb, phase ^ 1u); ++i) {
+  } else {
+    if (tid == 0) atomicAdd(&g_made_wait_timeouts, 1ull);
+    // products of the stage that timed out may still run: wait for them, bounded, before freeing their memory
+    const uint32_t mb = pending ? mb1 : mb0;
+    for (long long i = 0; i < kUmmaWaitLimit && !umma_try_wait(mb, ph[pending] ^ 1u); ++i) {
     }
+    cp_async_wait<0>();
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
@@ -365,6 +398,9 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(GemmArgs g) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(N < 32 ? 32 : N)
                  : "memory");
 }
+
+template <int N>
+constexpr int umma_smem() { return 2 * (UM + N) * UKC * 2 + 16 + 16; }
 
 }  // namespace made
 
@@ -374,14 +410,19 @@ int made_wait_timeouts(unsigned long long* v) {
 
 namespace made {
 
+template <int N, int EPI>
+int umma_gemm_n(const GemmArgs& g, cudaStream_t s) {
+  const int rc = cuda_status(cudaFuncSetAttribute(umma_gemm_kernel<N, EPI>,
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, umma_smem<N>()),
+                             "made tcgen05 gemm smem");
+  if (rc != SCK_OK) return rc;
+  umma_gemm_kernel<N, EPI><<<dim3(g.M / UM), 128, umma_smem<N>(), s>>>(g);
+  return cuda_status(cudaGetLastError(), "made tcgen05 gemm");
+}
+
 template <int EPI>
 int umma_gemm(const GemmArgs& g, cudaStream_t s) {
-  const dim3 grid(g.M / UM);
-  if (g.N == H)
-    umma_gemm_kernel<H, EPI><<<grid, 128, 0, s>>>(g);
-  else
-    umma_gemm_kernel<NSP, EPI><<<grid, 128, 0, s>>>(g);
-  return cuda_status(cudaGetLastError(), "made tcgen05 gemm");
+  return g.N == H ? umma_gemm_n<H, EPI>(g, s) : umma_gemm_n<NSP, EPI>(g, s);
 }
 
 template <bool A_K, bool B_K, int EPI>
