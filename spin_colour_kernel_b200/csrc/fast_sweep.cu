@@ -96,16 +96,20 @@ __device__ __forceinline__ void ising_spec_site(const Common& c, int rep, int x,
 // --------------------------------------------------------------------------------------------- vector models
 // Two replicas (lanes .x and .y) of one class site. `two` = false runs lane y as a copy of lane x and stores
 // lane x only (an odd replica count).
-template <class Lat, int A, int N, bool PER>
+// NSL > 0: the replica has 2^NSL sites, so component offsets are compile-time and every neighbour load of a
+// replica is one address plus an immediate offset (each replica of the pair gets its own base); NSL = 0: one
+// base for the pair, runtime offsets.
+template <class Lat, int A, int N, bool PER, int NSL>
 __device__ __forceinline__ void vec_spec_pair(const Common& c, const float (&J)[SCK_MAX_GROUPS], int rep0, bool two,
                                               int x, int y, int z, int32_t key) {
   const Geometry& g = c.g;
   const int own = A * g.plane + (z * g.L2 + y) * g.L1 + x;
   if (g.has_mask && c.mask[own] == 0) return;
-  // one base pointer for the pair: component k of replica rep0 + j sits at k * NS + j * RS (uniform offsets)
+  // component k of replica rep0 + j sits at k * NS + j * RS
   const float* base = (const float*)c.src + (size_t)rep0 * N * g.nsite;
   float* obase = (float*)c.dst + (size_t)rep0 * N * g.nsite;
-  const size_t NS = (size_t)g.nsite, RS = two ? (size_t)N * g.nsite : 0;
+  const size_t NS = NSL ? ((size_t)1 << NSL) : (size_t)g.nsite, RS = two ? (size_t)N * NS : 0;
+  const float* base1 = base + RS;
   const int rep1 = two ? rep0 + 1 : rep0;
   const Around<Lat::reach, PER> nb(g, x, y, z);
   float2 s[N], v[N];
@@ -125,11 +129,17 @@ __device__ __forceinline__ void vec_spec_pair(const Common& c, const float (&J)[
     for (int k = 0; k < N; ++k) gs[k] = f2(0.0f);
     static_for<R::begin, R::end>([&](auto ic) {
       constexpr BondC bd = Lat::bond(A, decltype(ic)::value);
-      const float* pq = base + nb.index(g, bd);
+      const int qi = nb.index(g, bd);
+      const float* pq = base + qi;
+      const float* pq1 = base1 + qi;
       const bool ok = nb.valid(bd);
 #pragma unroll
       for (int k = 0; k < N; ++k) {
-        const float2 t = ok ? make_float2(pq[k * NS], pq[k * NS + RS]) : f2(0.0f);
+        float2 t;
+        if constexpr (NSL > 0)
+          t = ok ? make_float2(pq[k * NS], pq1[k * NS]) : f2(0.0f);
+        else
+          t = ok ? make_float2(pq[k * NS], pq[k * NS + RS]) : f2(0.0f);
         gs[k] = __fadd2_rn(gs[k], t);
       }
     });
@@ -155,7 +165,7 @@ __device__ __forceinline__ void vec_spec_pair(const Common& c, const float (&J)[
 
 // ------------------------------------------------------------------------------------------------- kernels
 // Grid (ceil(rows * bx / 256), n_tasks * units_per_task). Block y-slot -> (task, replica or replica pair).
-template <class Lat, int N, typename ST, bool PER>
+template <class Lat, int N, typename ST, bool PER, int NSL>
 __global__ void __launch_bounds__(256) spec_task_kernel(const __grid_constant__ SpecParams p) {
   const uint32_t per = (uint32_t)p.c.rows * (uint32_t)p.c.bx;
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -175,7 +185,7 @@ __global__ void __launch_bounds__(256) spec_task_kernel(const __grid_constant__ 
     if constexpr (N == 1) {
       ising_spec_site<Lat, a, ST, PER>(p.c, rep, x, y, z, key);
     } else {
-      vec_spec_pair<Lat, a, N, PER>(p.c, p.J[a], rep, rep + 1 < task.rep_end, x, y, z, key);
+      vec_spec_pair<Lat, a, N, PER, NSL>(p.c, p.J[a], rep, rep + 1 < task.rep_end, x, y, z, key);
     }
   });
 }
@@ -211,17 +221,28 @@ int find_spec(const sck_plan* p) {
 }
 
 // ------------------------------------------------------------------------------------------- host: launches
+template <class Lat, int N, bool PER>
+static void launch_vec(const sck_plan* plan, const SpecParams& p, dim3 grid, cudaStream_t s) {
+  // replicas of 2^16 .. 2^19 sites on periodic boxes: component strides up to 2 MiB fit a load's immediate offset
+  const int64_t ns = plan->geom.nsite;
+  if (PER && ns == (1 << 16)) spec_task_kernel<Lat, N, float, PER, 16><<<grid, 256, 0, s>>>(p);
+  else if (PER && ns == (1 << 17)) spec_task_kernel<Lat, N, float, PER, 17><<<grid, 256, 0, s>>>(p);
+  else if (PER && ns == (1 << 18)) spec_task_kernel<Lat, N, float, PER, 18><<<grid, 256, 0, s>>>(p);
+  else if (PER && ns == (1 << 19)) spec_task_kernel<Lat, N, float, PER, 19><<<grid, 256, 0, s>>>(p);
+  else spec_task_kernel<Lat, N, float, PER, 0><<<grid, 256, 0, s>>>(p);
+}
+
 template <class Lat, bool PER>
 static void launch_lat_per(const sck_plan* plan, const SpecParams& p, dim3 grid, cudaStream_t s) {
   if (plan->geom.n == 1) {
     if (plan->mode == SCK_MODE_INT8)
-      spec_task_kernel<Lat, 1, int8_t, PER><<<grid, 256, 0, s>>>(p);
+      spec_task_kernel<Lat, 1, int8_t, PER, 0><<<grid, 256, 0, s>>>(p);
     else
-      spec_task_kernel<Lat, 1, float, PER><<<grid, 256, 0, s>>>(p);
+      spec_task_kernel<Lat, 1, float, PER, 0><<<grid, 256, 0, s>>>(p);
   } else if (plan->geom.n == 2) {
-    spec_task_kernel<Lat, 2, float, PER><<<grid, 256, 0, s>>>(p);
+    launch_vec<Lat, 2, PER>(plan, p, grid, s);
   } else {
-    spec_task_kernel<Lat, 3, float, PER><<<grid, 256, 0, s>>>(p);
+    launch_vec<Lat, 3, PER>(plan, p, grid, s);
   }
 }
 

@@ -462,6 +462,41 @@ def test_refusals_and_counter_limit():
         A.set_temperature(torch.linspace(2.0, 3.0, 64))
 
 
+POW2_SYSTEMS = {
+    # 2^16 sites each: the lattice kernels take their compile-time component strides
+    "xy_square_256x256": lambda: sy.System("XY square", 2, cr.make("square"), (256, 256), (True, True), {1: 1.0},
+                                           h=(0.05, 0.0)),
+    "heis_sc_64x32x32": lambda: sy.System("Heisenberg sc", 3, cr.make("sc"), (64, 32, 32), (True,) * 3, {1: -1.0},
+                                          h=(0.2, 0.0, 0.1)),
+    "heis_bcc_j1j2_32x16x64": lambda: sy.System("Heisenberg bcc J1-J2", 3, cr.make("bcc", (1, 2)), (32, 16, 64),
+                                                (True,) * 3, {1: 1.0, 2: 0.3}, h=(0.0, 0.0, 0.1)),
+}
+
+
+@pytest.mark.parametrize("name", sorted(POW2_SYSTEMS))
+def test_power_of_two_replicas_match_oracle(name):
+    """Replicas of 2^16 sites (component offsets fixed at compile time, one base address per replica of the
+    pair), odd replica count so the last pair has one replica: every replica against the oracle."""
+    from spin_colour_kernel_b200.sampler import Sampler
+    s = POW2_SYSTEMS[name]()
+    B = 3
+    A = Sampler(s, B, device="cuda", seed=11)
+    assert A.tune(1, 0, 0)["specialised"] // 100 == 1
+    T = torch.tensor([0.6, 1.3, 2.4])
+    A.set_temperature(T)
+    S = A.init_spins(seed=5)
+    x = S.cpu().numpy().copy()
+    A.sweep(S, 2)
+    got = S.cpu().numpy()
+    beta = (np.float32(1.0) / T.numpy()).astype(np.float32)
+    osw.sweep(s, x, beta, [11, 0], 2)
+    d = np.abs(got.astype(np.float64) - x)
+    frac = float((d > VEC_TOL).any(axis=1).mean())
+    print(f"{name}: fraction of spins beyond {VEC_TOL}: {frac:.2e}")
+    assert frac <= 1e-3
+    assert not np.array_equal(got, A.init_spins(seed=5).cpu().numpy())
+
+
 # ------------------------------------------------------------------ full-size workloads, checked on a few replicas
 def test_workload3_full_size_replicas_match_oracle():
     """Heisenberg bcc 64^3 cells (524,288 sites), J1 = 1, J2 = 0.3, K1 = 0.05, h = 0.1 z, 1536 replicas at
