@@ -93,8 +93,6 @@ static int pipeline_group(const sck_plan* p) {
   long long group = p->l2_budget / ((long long)C * per_rep);
   if (p->geom.n > 1) group &= ~1ll;
   if (group < 1) return 0;
-  const long long cap = (65535 / 8) * (p->geom.n > 1 ? 2 : 1);   // grid rows: tasks x units per task
-  if (group > cap) group = cap;
   if ((p->Bp + group - 1) / group < C) return 0;
   return (int)group;
 }
@@ -357,13 +355,36 @@ int sck_plan_tune(sck_plan* plan, int32_t specialised, int64_t l2_budget_bytes, 
   plan->kernel_kind = specialised >= 3 ? 3 : (specialised >= 2 ? 2 : 1);
   plan->l2_budget = l2_budget_bytes;
   plan->resident_limit = resident_limit_bytes;
+  // the group pipeline's counters live on the current device, allocated here (never inside a sweep)
+  const int group = pipeline_group(plan);
+  if (group > 0 && !use_resident(plan)) {
+    const size_t need = stream_counter_bytes(plan, group);
+    int dev = 0;
+    int rc = cuda_status(cudaGetDevice(&dev), "group pipeline counters");
+    if (rc != SCK_OK) return rc;
+    if (plan->pipe_counters == nullptr || plan->pipe_bytes < need || plan->pipe_device != dev) {
+      if (plan->pipe_counters != nullptr) cudaFree(plan->pipe_counters);
+      plan->pipe_counters = nullptr;
+      plan->pipe_bytes = 0;
+      rc = cuda_status(cudaMalloc(&plan->pipe_counters, need), "group pipeline counters");
+      if (rc != SCK_OK) {
+        plan->pipe_counters = nullptr;
+        return rc;
+      }
+      plan->pipe_bytes = need;
+      plan->pipe_device = dev;
+    }
+  }
   return SCK_OK;
 }
 
 int sck_plan_path(const sck_plan* plan, int32_t* specialised, int64_t* l2_budget_bytes, int32_t* group,
                   int32_t* resident) {
   if (plan == nullptr) return fail(SCK_ERR_INVALID, "null plan");
-  if (specialised) *specialised = plan->spec ? (tile_kernel_ok(plan) ? 3 : (seg_kernel_ok(plan) ? 2 : 1)) * 100 + plan->spec : 0;
+  if (specialised) {
+    const int kind = pipeline_group(plan) > 0 ? 1 : (tile_kernel_ok(plan) ? 3 : (seg_kernel_ok(plan) ? 2 : 1));
+    *specialised = plan->spec ? kind * 100 + plan->spec : 0;
+  }
   if (l2_budget_bytes) *l2_budget_bytes = plan->l2_budget;
   if (group) *group = pipeline_group(plan);
   if (resident) *resident = use_resident(plan) ? 1 : 0;
@@ -371,6 +392,7 @@ int sck_plan_path(const sck_plan* plan, int32_t* specialised, int64_t* l2_budget
 }
 
 int sck_plan_destroy(sck_plan* plan) {
+  if (plan != nullptr && plan->pipe_counters != nullptr) cudaFree(plan->pipe_counters);
   delete plan;
   return SCK_OK;
 }
@@ -432,7 +454,12 @@ int sck_sweep(const sck_plan* plan, const sck_buffers* buf, int32_t n_sweeps, vo
     const Common c = make_common(plan, buf, buf->spins);
     const int group = pipeline_group(plan);
     if (group > 0) {
-      rc = launch_spec_pipeline(plan, c, n_sweeps, group, s);
+      int dev = -1;
+      rc = cuda_status(cudaGetDevice(&dev), "group pipeline");
+      if (rc != SCK_OK) return rc;
+      if (plan->pipe_counters == nullptr || plan->pipe_device != dev || plan->pipe_bytes < stream_counter_bytes(plan, group))
+        return fail(SCK_ERR_INVALID, "the group pipeline's counters belong to another device: call sck_plan_tune on this one");
+      rc = launch_spec_pipeline(plan, c, n_sweeps, group, plan->pipe_counters, s);
       if (rc != SCK_OK) return rc;
       return launch_advance(buf->state, n_sweeps, s);
     }

@@ -190,6 +190,114 @@ __global__ void __launch_bounds__(256) spec_task_kernel(const __grid_constant__ 
   });
 }
 
+// ----------------------------------------------------------------------------------- the streamed pipeline
+// One launch runs the group pipeline of several sweeps. Tickets, taken from a counter in the order blocks start,
+// enumerate stages k = 0, 1, ...; stage k holds class ci of unit k - ci (unit = sweep-major group) for every ci,
+// each class task split into T tickets (slot of the group x chunk of site blocks). Before touching spins a
+// block waits until every ticket of the task it follows has finished: class ci - 1 of its unit, or, for class
+// 0, class C - 1 of the same group's previous sweep. That task holds smaller tickets, so its blocks started
+// before this one and are running or done: the wait ends. Tasks of one group are therefore serialised exactly
+// as class launches are, tasks of different groups overlap freely, and a group's state is read from HBM once
+// per sweep while its C classes pass over it from L2.
+constexpr int kStreamSiteBlocks = 1;                 // site blocks of 256 threads per ticket
+constexpr unsigned kStreamWaitLimit = 1u << 22;      // polls of a completion counter before giving up
+static __device__ unsigned long long g_stream_wait_timeouts;
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* a) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(a) : "memory");
+  return v;
+}
+
+struct StreamTask {
+  int go;            // 0: no task (pipeline fill / drain) or a wait that gave up
+  int rep, rep_end;  // first replica of this block's slot, end of its group
+  int colour, alpha, sweep;
+  int done;          // index of this task's completion counter
+  uint32_t t0;       // first class-site thread of this block
+};
+
+template <class Lat, int N, typename ST, bool PER, int NSL>
+__global__ void __launch_bounds__(256, 5) stream_kernel(const __grid_constant__ StreamParams p) {
+  __shared__ StreamTask s;
+  if (threadIdx.x == 0) {
+    const unsigned tk = atomicAdd(p.ticket, 1u);
+    const unsigned stage = (unsigned)p.C * (unsigned)p.T;
+    const unsigned k = tk / stage;
+    const unsigned r = tk - k * stage;
+    const int ci = (int)(r / (unsigned)p.T), j = (int)(r - (unsigned)ci * (unsigned)p.T);
+    const int u = (int)k - ci;
+    s.go = 0;
+    s.done = -1;
+    if (u >= 0 && u < p.units) {
+      const int sw = u / p.ngroups, g = u - sw * p.ngroups;
+      const int q = j / p.chunks, chunk = j - q * p.chunks;
+      constexpr int per_slot = N == 1 ? 1 : 2;
+      s.rep = g * p.group + q * per_slot;
+      s.rep_end = min(p.c.B, (g + 1) * p.group);
+      s.colour = p.cls[ci][0];
+      s.alpha = p.cls[ci][1];
+      s.sweep = p.sweep_base + sw;
+      s.done = g * p.C + ci;
+      s.t0 = (uint32_t)chunk * (kStreamSiteBlocks * 256u);
+      const unsigned* dep = nullptr;
+      unsigned need = 0;
+      if (ci > 0) {
+        dep = p.done + s.done - 1;
+        need = (unsigned)(sw + 1) * (unsigned)p.T;
+      } else if (sw > 0) {
+        dep = p.done + g * p.C + p.C - 1;
+        need = (unsigned)sw * (unsigned)p.T;
+      }
+      int go = 1;
+      if (dep != nullptr) {
+        unsigned polls = 0;
+        while (ld_acquire_u32(dep) < need) {
+          if (++polls > kStreamWaitLimit) {
+            go = 0;
+            atomicAdd(&g_stream_wait_timeouts, 1ull);
+            break;
+          }
+          __nanosleep(100);
+        }
+      }
+      s.go = go && s.rep < s.rep_end;
+    }
+  }
+  __syncthreads();
+  if (s.done < 0) return;                              // the pipeline's fill and drain: no task
+  if (s.go) {
+    const int rep = s.rep, rep_end = s.rep_end, alpha = s.alpha;
+    const int32_t key = sweep_key_at(p.c.state, s.sweep);
+    const uint32_t per = (uint32_t)p.c.rows * (uint32_t)p.c.bx;
+#pragma unroll 1
+    for (int sb = 0; sb < kStreamSiteBlocks; ++sb) {
+      const uint32_t t = s.t0 + sb * 256u + threadIdx.x;
+      int x, y, z;
+      if (t < per && class_site(p.c, s.colour, alpha, t, x, y, z)) {
+        static_for<0, Lat::b>([&](auto ac) {
+          constexpr int a = decltype(ac)::value;
+          if (a != alpha) return;
+          if constexpr (N == 1) {
+            ising_spec_site<Lat, a, ST, PER>(p.c, rep, x, y, z, key);
+          } else {
+            vec_spec_pair<Lat, a, N, PER, NSL>(p.c, p.J[a], rep, rep + 1 < rep_end, x, y, z, key);
+          }
+        });
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(p.done + s.done, 1u);   // finished (or given up): later tasks of this group may start
+  }
+}
+
+int stream_wait_timeouts(unsigned long long* count) {
+  return cuda_status(cudaMemcpyFromSymbol(count, g_stream_wait_timeouts, sizeof(*count)), "stream wait timeouts");
+}
+
 // ------------------------------------------------------------------------------------------ host: matching
 template <class Lat>
 static bool matches(const sck_plan* p) {
@@ -221,24 +329,34 @@ int find_spec(const sck_plan* p) {
 }
 
 // ------------------------------------------------------------------------------------------- host: launches
-template <class Lat, int N, bool PER>
-static void launch_vec(const sck_plan* plan, const SpecParams& p, dim3 grid, cudaStream_t s) {
-  // replicas of 2^16 .. 2^19 sites on periodic boxes: component strides up to 2 MiB fit a load's immediate offset
-  const int64_t ns = plan->geom.nsite;
-  if (PER && ns == (1 << 16)) spec_task_kernel<Lat, N, float, PER, 16><<<grid, 256, 0, s>>>(p);
-  else if (PER && ns == (1 << 17)) spec_task_kernel<Lat, N, float, PER, 17><<<grid, 256, 0, s>>>(p);
-  else if (PER && ns == (1 << 18)) spec_task_kernel<Lat, N, float, PER, 18><<<grid, 256, 0, s>>>(p);
-  else if (PER && ns == (1 << 19)) spec_task_kernel<Lat, N, float, PER, 19><<<grid, 256, 0, s>>>(p);
-  else spec_task_kernel<Lat, N, float, PER, 0><<<grid, 256, 0, s>>>(p);
+template <class Lat, int N, typename ST, bool PER, int NSL, class P>
+static void launch_one(const P& p, dim3 grid, cudaStream_t s) {
+  if constexpr (std::is_same_v<P, SpecParams>)
+    spec_task_kernel<Lat, N, ST, PER, NSL><<<grid, 256, 0, s>>>(p);
+  else
+    stream_kernel<Lat, N, ST, PER, NSL><<<grid, 256, 0, s>>>(p);
 }
 
-template <class Lat, bool PER>
-static void launch_lat_per(const sck_plan* plan, const SpecParams& p, dim3 grid, cudaStream_t s) {
+template <class Lat, int N, bool PER, class P>
+static void launch_vec(const sck_plan* plan, const P& p, dim3 grid, cudaStream_t s) {
+  // replicas of 2^16 .. 2^19 sites on periodic boxes: component strides up to 2 MiB fit a load's immediate offset
+  if constexpr (PER) {
+    const int64_t ns = plan->geom.nsite;
+    if (ns == (1 << 16)) return launch_one<Lat, N, float, PER, 16>(p, grid, s);
+    if (ns == (1 << 17)) return launch_one<Lat, N, float, PER, 17>(p, grid, s);
+    if (ns == (1 << 18)) return launch_one<Lat, N, float, PER, 18>(p, grid, s);
+    if (ns == (1 << 19)) return launch_one<Lat, N, float, PER, 19>(p, grid, s);
+  }
+  launch_one<Lat, N, float, PER, 0>(p, grid, s);
+}
+
+template <class Lat, bool PER, class P>
+static void launch_lat_per(const sck_plan* plan, const P& p, dim3 grid, cudaStream_t s) {
   if (plan->geom.n == 1) {
     if (plan->mode == SCK_MODE_INT8)
-      spec_task_kernel<Lat, 1, int8_t, PER, 0><<<grid, 256, 0, s>>>(p);
+      launch_one<Lat, 1, int8_t, PER, 0>(p, grid, s);
     else
-      spec_task_kernel<Lat, 1, float, PER, 0><<<grid, 256, 0, s>>>(p);
+      launch_one<Lat, 1, float, PER, 0>(p, grid, s);
   } else if (plan->geom.n == 2) {
     launch_vec<Lat, 2, PER>(plan, p, grid, s);
   } else {
@@ -254,8 +372,8 @@ static bool periodic_box(const sck_plan* plan) {
   return g.dim == 2 || (g.per[2] && g.L3 >= Lat::reach);
 }
 
-template <class Lat>
-static void launch_lat(const sck_plan* plan, const SpecParams& p, dim3 grid, cudaStream_t s) {
+template <class Lat, class P>
+static void launch_lat(const sck_plan* plan, const P& p, dim3 grid, cudaStream_t s) {
   if (periodic_box<Lat>(plan))
     launch_lat_per<Lat, true>(plan, p, grid, s);
   else
@@ -263,6 +381,18 @@ static void launch_lat(const sck_plan* plan, const SpecParams& p, dim3 grid, cud
 }
 
 // replicas per grid y-slot: vector models pair two replicas per thread in the lattice kernels
+template <class P>
+static void launch_spec_grid(const sck_plan* plan, const P& p, dim3 grid, cudaStream_t s) {
+  switch (plan->spec) {
+    case Lat_square_1::id: launch_lat<Lat_square_1>(plan, p, grid, s); break;
+    case Lat_triangular_1::id: launch_lat<Lat_triangular_1>(plan, p, grid, s); break;
+    case Lat_sc_1::id: launch_lat<Lat_sc_1>(plan, p, grid, s); break;
+    case Lat_bcc_1::id: launch_lat<Lat_bcc_1>(plan, p, grid, s); break;
+    case Lat_bcc_1_2::id: launch_lat<Lat_bcc_1_2>(plan, p, grid, s); break;
+    default: launch_lat<Lat_fcc_1>(plan, p, grid, s); break;
+  }
+}
+
 static int slot_replicas(const sck_plan* plan) { return plan->geom.n == 1 || seg_kernel_ok(plan) ? 1 : 2; }
 
 static int launch_tasks(const sck_plan* plan, SpecParams& p, cudaStream_t s) {
@@ -277,15 +407,7 @@ static int launch_tasks(const sck_plan* plan, SpecParams& p, cudaStream_t s) {
   if (ys > 65535) return cuda_status(cudaErrorInvalidConfiguration, "task launch: too many replicas per launch");
   if (seg_kernel_ok(plan)) return launch_seg_tasks(plan, p, (int)ys, s);
   const uint32_t per = (uint32_t)p.c.rows * (uint32_t)p.c.bx;
-  const dim3 grid((per + 255) / 256, (unsigned)ys);
-  switch (plan->spec) {
-    case Lat_square_1::id: launch_lat<Lat_square_1>(plan, p, grid, s); break;
-    case Lat_triangular_1::id: launch_lat<Lat_triangular_1>(plan, p, grid, s); break;
-    case Lat_sc_1::id: launch_lat<Lat_sc_1>(plan, p, grid, s); break;
-    case Lat_bcc_1::id: launch_lat<Lat_bcc_1>(plan, p, grid, s); break;
-    case Lat_bcc_1_2::id: launch_lat<Lat_bcc_1_2>(plan, p, grid, s); break;
-    default: launch_lat<Lat_fcc_1>(plan, p, grid, s); break;
-  }
+  launch_spec_grid(plan, p, dim3((per + 255) / 256, (unsigned)ys), s);
   return cuda_status(cudaGetLastError(), "specialised class launch");
 }
 
@@ -312,22 +434,53 @@ int launch_spec_class(const sck_plan* plan, const Common& c, int colour, int alp
   return SCK_OK;
 }
 
-// n sweeps as a diagonal over (sweep-major group unit, class); state[1] is advanced by the caller.
-int launch_spec_pipeline(const sck_plan* plan, const Common& c, int n_sweeps, int group, cudaStream_t s) {
+size_t stream_counter_bytes(const sck_plan* plan, int group) {
+  const int ngroups = (plan->Bp + group - 1) / group;
+  return (size_t)(1 + ngroups * plan->desc.n_classes) * sizeof(unsigned);
+}
+
+// n sweeps of the group pipeline (streamed kernel, one launch per chunk of sweeps); state[1] is advanced by
+// the caller. `counters` holds stream_counter_bytes(plan, group) bytes of device memory, zeroed here before
+// every launch.
+int launch_spec_pipeline(const sck_plan* plan, const Common& c, int n_sweeps, int group, void* counters,
+                         cudaStream_t s) {
+  if (counters == nullptr) {
+    set_error("the group pipeline has no completion counters (set an L2 budget with sck_plan_tune)");
+    return SCK_ERR_INVALID;
+  }
   const int C = plan->desc.n_classes;
-  const int ngroups = (c.B + group - 1) / group;
-  const long long units = (long long)n_sweeps * ngroups;
-  SpecParams p = spec_params(plan, c);
-  for (long long k = 0; k < units + C - 1; ++k) {
-    p.n_tasks = 0;
-    for (int ci = 0; ci < C; ++ci) {
-      const long long u = k - ci;
-      if (u < 0 || u >= units) continue;
-      const int sw = (int)(u / ngroups), gi = (int)(u - (long long)sw * ngroups);
-      const int r0 = gi * group, r1 = r0 + group < c.B ? r0 + group : c.B;
-      p.tasks[p.n_tasks++] = Task{plan->desc.classes[ci][0], plan->desc.classes[ci][1], r0, r1, sw};
-    }
-    const int rc = launch_tasks(plan, p, s);
+  StreamParams p;
+  memset(&p, 0, sizeof(p));
+  p.c = c;
+  for (int a = 0; a < SCK_MAX_BASIS; ++a)
+    for (int gi = 0; gi < SCK_MAX_GROUPS; ++gi) p.J[a][gi] = plan->sub[a].J[gi];
+  p.C = C;
+  for (int ci = 0; ci < C; ++ci) {
+    p.cls[ci][0] = plan->desc.classes[ci][0];
+    p.cls[ci][1] = plan->desc.classes[ci][1];
+  }
+  p.group = group;
+  p.ngroups = (c.B + group - 1) / group;
+  const int per_slot = plan->geom.n == 1 ? 1 : 2;
+  const long long site_blocks = ((long long)c.rows * c.bx + 255) / 256;
+  p.chunks = (int)((site_blocks + kStreamSiteBlocks - 1) / kStreamSiteBlocks);
+  p.T = ((group + per_slot - 1) / per_slot) * p.chunks;
+  p.ticket = (unsigned*)counters;
+  p.done = p.ticket + 1;
+  // tickets of a launch, (units + C - 1) x C x T, stay below 2^30
+  const long long stage = (long long)C * p.T;
+  const long long most_units = (1ll << 30) / stage - (C - 1);
+  const long long sweeps_per_launch = most_units / p.ngroups;
+  if (sweeps_per_launch < 1) return cuda_status(cudaErrorInvalidConfiguration, "group pipeline: too many tickets");
+  const size_t bytes = stream_counter_bytes(plan, group);
+  for (int sw0 = 0; sw0 < n_sweeps; sw0 += (int)sweeps_per_launch) {
+    const int n = (int)((long long)(n_sweeps - sw0) < sweeps_per_launch ? n_sweeps - sw0 : sweeps_per_launch);
+    p.units = n * p.ngroups;
+    p.sweep_base = sw0;
+    int rc = cuda_status(cudaMemsetAsync(counters, 0, bytes, s), "group pipeline counters");
+    if (rc != SCK_OK) return rc;
+    launch_spec_grid(plan, p, dim3((unsigned)((p.units + C - 1) * stage)), s);
+    rc = cuda_status(cudaGetLastError(), "group pipeline launch");
     if (rc != SCK_OK) return rc;
   }
   return SCK_OK;

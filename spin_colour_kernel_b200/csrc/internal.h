@@ -121,6 +121,9 @@ struct sck_plan {
   int kernel_kind; // specialised class kernels: 1 lattice, 2 segment (segment.cu), 3 tile (tile.cu) where eligible
   long long l2_budget;  // bytes of L2 the group pipeline may fill
   long long resident_limit;  // largest replica (bytes) whose sweeps run resident in shared memory; 0 = never
+  void* pipe_counters;       // device memory of the group pipeline's ticket and completion counters
+  size_t pipe_bytes;
+  int pipe_device;           // the device that holds them
 };
 
 namespace sck {
@@ -144,5 +147,8 @@ int find_spec(const sck_plan* plan);
 size_t resident_bytes(const sck_plan* plan);
 int launch_resident(const sck_plan* plan, const Common& c, int n_sweeps, cudaStream_t s);
 int launch_spec_class(const sck_plan* plan, const Common& c, int colour, int alpha, cudaStream_t s);
-int launch_spec_pipeline(const sck_plan* plan, const Common& c, int n_sweeps, int group, cudaStream_t s);
+int launch_spec_pipeline(const sck_plan* plan, const Common& c, int n_sweeps, int group, void* counters,
+                         cudaStream_t s);
+size_t stream_counter_bytes(const sck_plan* plan, int group);
+int stream_wait_timeouts(unsigned long long* count);   // group pipeline waits that gave up
 }  // namespace sck

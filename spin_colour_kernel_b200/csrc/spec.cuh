@@ -25,6 +25,21 @@ struct SpecParams {
   Task tasks[kMaxTasks];
 };
 
+// The streamed group pipeline (fast_sweep.cu:stream_kernel).
+struct StreamParams {
+  Common c;
+  float J[SCK_MAX_BASIS][SCK_MAX_GROUPS];
+  int C;                  // classes per sweep, in sweep order
+  int cls[8][2];          // (colour, alpha) of each class
+  int group, ngroups;     // replicas per group, groups
+  int units;              // sweeps of this launch x groups
+  int sweep_base;         // sweeps run by earlier launches of the same call
+  int chunks;             // tickets per slot (replica or replica pair) and class
+  int T;                  // tickets per class task: slots per group x chunks
+  unsigned* ticket;       // next ticket
+  unsigned* done;         // finished tickets per (group, class), summed over the launch's sweeps
+};
+
 __device__ __forceinline__ uint32_t counter_of(int rep, int nsite, int own) {
   return (uint32_t)((unsigned long long)rep * (unsigned long long)nsite + (unsigned long long)own);
 }

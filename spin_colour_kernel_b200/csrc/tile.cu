@@ -280,10 +280,11 @@ extern "C" int sck_wait_timeouts(int64_t* count) {
     sck::set_error("null output");
     return SCK_ERR_INVALID;
   }
-  unsigned long long v = 0, w = 0;
+  unsigned long long v = 0, w = 0, x = 0;
   int rc = sck::cuda_status(cudaMemcpyFromSymbol(&v, sck::g_wait_timeouts, sizeof(v)), "wait timeouts");
   if (rc == SCK_OK) rc = sck::made_wait_timeouts(&w);
+  if (rc == SCK_OK) rc = sck::stream_wait_timeouts(&x);
   if (rc != SCK_OK) return rc;
-  *count = (int64_t)(v + w);
+  *count = (int64_t)(v + w + x);
   return SCK_OK;
 }

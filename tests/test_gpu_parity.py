@@ -185,6 +185,36 @@ def test_l2_group_pipeline_equals_class_by_class(build):
     assert int(A.state[1]) == int(R.state[1]) == 3
 
 
+@pytest.mark.parametrize("B,groups", [(64, 32), (23, 6), (40, 5)])
+def test_streamed_pipeline_many_groups(B, groups):
+    """The streamed group pipeline with many groups in flight (one launch per call, blocks ordered by tickets and
+    by completion counters per group and class), odd replica counts and a short last group: five sweeps
+    bit-identical to class-by-class launches, and no bounded wait gave up."""
+    from spin_colour_kernel_b200.sampler import Sampler
+    s = C.heisenberg_bcc_j1j2(sy, cr, 16)
+    A, R = Sampler(s, B, device="cuda", seed=21, packed=False), Sampler(s, B, device="cuda", seed=21, packed=False)
+    per_rep = s.nsite * s.n * 4
+    group = -(-B // groups)
+    group += group % 2
+    pa = A.tune(True, len(A.classes) * per_rep * group, 0)
+    assert pa["group"] == group and pa["specialised"] // 100 == 1, pa
+    pr = R.tune(True, 0, 0)                   # class-by-class lattice launches (not the resident kernel)
+    assert pr["group"] == 0 and not pr["resident"] and pr["specialised"] // 100 == 1, pr
+    for X in (A, R):
+        X.set_temperature(torch.linspace(0.3, 3.0, B))
+    S1 = A.init_spins(seed=6)
+    S2 = S1.clone()
+    before = ctypes.c_int64()
+    L.check(L.lib().sck_wait_timeouts(ctypes.byref(before)))
+    A.sweep(S1, 5)
+    R.sweep(S2, 5)
+    assert torch.equal(S1, S2)
+    after = ctypes.c_int64()
+    L.check(L.lib().sck_wait_timeouts(ctypes.byref(after)))
+    assert after.value == before.value
+    assert int(A.state[1]) == 5
+
+
 @pytest.mark.parametrize("name", ["heis_bcc2", "w3_heis_bcc4_j1j2", "xy_square4", "ising_sc5_odd", "w5_ising_sc8",
                                   "ising_triangular6_packed", "heis_fcc2", "w4_xy_square16"])
 def test_specialised_and_generic_kernels_agree(name):
