@@ -138,7 +138,10 @@ int sck_plan_shape(const sck_plan* plan, int32_t* computed_replicas, int32_t* ro
  *                         periodic box, classes alternating along x);
  *                         1: compile-time lattice kernels only (default); 0: generic kernels;
  *   l2_budget_bytes       L2 bytes the group pipeline may fill; 0 disables it (the default: the class kernels
- *                         are issue-bound, and smaller launches lose more than the saved HBM traffic);
+ *                         are issue-bound, and the pipeline's ordering costs more than the saved HBM traffic).
+ *                         Enabling it allocates the pipeline's completion counters (4 bytes per replica group
+ *                         and class) on the current device, which then runs this plan's sweeps; freed by
+ *                         sck_plan_destroy. Call it outside stream capture;
  *   resident_limit_bytes  replicas up to this size (int8 / float32 storage) run all sweeps of a call in shared
  *                         memory, one block per replica; 0 disables it (default 200 KiB, at most 220 KiB).
  * sck_plan_path reports the chosen path: specialised = 100 * kernel kind (1 lattice, 2 segment, 3 tile) + table
