@@ -195,9 +195,10 @@ int sck_observables_noalloc(const sck_plan* plan, const sck_buffers* buf, const 
                             int32_t batch, double* E, double* M, void* stream);
 
 /* Bounded device-side waits that gave up since the library was loaded (0 in normal operation). The tile
- * kernels wait on the shared-memory fill of a brick, and the learned proposal's tcgen05 GEMMs on their tensor-core
- * products, with an iteration limit; a brick whose fill timed out leaves its sites unchanged, a GEMM tile whose
- * products timed out leaves its output unwritten, and each adds one here. Reads the count from the current
+ * kernels wait on the shared-memory fill of a brick, the group pipeline's blocks on the completion of the class
+ * task they follow, and the learned proposal's tcgen05 GEMMs on their tensor-core products, with an iteration
+ * limit; a brick whose fill timed out and a pipeline block whose wait timed out leave their sites unchanged, a
+ * GEMM tile whose products timed out leaves its output unwritten, and each adds one here. Reads the count from the current
  * device (synchronising it). No counterpart in the reference. */
 int sck_wait_timeouts(int64_t* count);
 
