@@ -282,33 +282,54 @@ __global__ void __launch_bounds__(256) observables_tile_kernel(const __grid_cons
   constexpr int RS = RW::RS, R2 = RW::R2;
   constexpr int COMP = R2 * RS;                    // doubles of one component of one sublattice
   constexpr int SLOT = Lat::b * N * COMP;
+  constexpr int Q = L1T / 4;                       // float4 loads per row
+  constexpr int ITEMS = Lat::b * N * R2 * Q;       // float4 loads per plane
+  constexpr int LOADS = (ITEMS + 255) / 256;       // per thread
   const Geometry& g = p.g;
   const int rep = blockIdx.y, y0 = blockIdx.x * OBS_TY;
   const float* src = (const float*)p.spins + (size_t)rep * N * g.nsite;
-  constexpr int Q = L1T / 4;
-  constexpr int ROWS = Lat::b * N * R2;
-  auto load_plane = [&](int zu) {   // unwrapped plane index -1 .. L3
+  // The next plane's loads are issued into registers before the current plane is computed and written to
+  // shared memory (as FP64) after it, so HBM latency overlaps the FP64 work.
+  float4 pf[LOADS];
+  auto fetch = [&](int zu) {   // unwrapped plane index -1 .. L3
     const int zz = zu < 0 ? zu + g.L3 : (zu >= g.L3 ? zu - g.L3 : zu);
-    double* dst = ring + ((zu + 3) % 3) * SLOT;
-    for (int i = threadIdx.x; i < ROWS * Q; i += blockDim.x) {
-      const int row = i / Q, q = i % Q;
-      const int r = row % R2, ak = row / R2, k = ak % N, a = ak / N;
-      int y = y0 - 1 + r;
-      y = y < 0 ? y + g.L2 : (y >= g.L2 ? y - g.L2 : y);
-      const float4 v = *(const float4*)(src + (size_t)k * g.nsite + (size_t)a * g.plane +
-                                        ((size_t)zz * g.L2 + y) * L1T + 4 * q);
-      double* d = dst + row * RS + OBS_PAD + 4 * q;
-      d[0] = v.x;
-      d[1] = v.y;
-      d[2] = v.z;
-      d[3] = v.w;
-      if (q == 0) d[L1T] = v.x;            // x = L1 is x = 0
-      if (q == Q - 1) d[-L1T + 3] = v.w;   // x = -1 is x = L1 - 1
+#pragma unroll
+    for (int j = 0; j < LOADS; ++j) {
+      const int i = threadIdx.x + 256 * j;
+      if (ITEMS % 256 == 0 || i < ITEMS) {
+        const int row = i / Q, q = i % Q;
+        const int r = row % R2, ak = row / R2, k = ak % N, a = ak / N;
+        int y = y0 - 1 + r;
+        y = y < 0 ? y + g.L2 : (y >= g.L2 ? y - g.L2 : y);
+        pf[j] = *(const float4*)(src + (size_t)k * g.nsite + (size_t)a * g.plane +
+                                 ((size_t)zz * g.L2 + y) * L1T + 4 * q);
+      }
     }
   };
-  load_plane(-1);
-  load_plane(0);
-  load_plane(1);
+  auto deposit = [&](int zu) {
+    double* dst = ring + ((zu + 3) % 3) * SLOT;
+#pragma unroll
+    for (int j = 0; j < LOADS; ++j) {
+      const int i = threadIdx.x + 256 * j;
+      if (ITEMS % 256 == 0 || i < ITEMS) {
+        const int row = i / Q, q = i % Q;
+        double* d = dst + row * RS + OBS_PAD + 4 * q;
+        const float4 v = pf[j];
+        d[0] = v.x;
+        d[1] = v.y;
+        d[2] = v.z;
+        d[3] = v.w;
+        if (q == 0) d[L1T] = v.x;            // x = L1 is x = 0
+        if (q == Q - 1) d[-L1T + 3] = v.w;   // x = -1 is x = L1 - 1
+      }
+    }
+  };
+  fetch(-1);
+  deposit(-1);
+  fetch(0);
+  deposit(0);
+  fetch(1);
+  deposit(1);
   __syncthreads();
   constexpr int NV = 1 + SCK_MAX_BASIS * N;
   double acc[NV];
@@ -317,63 +338,61 @@ __global__ void __launch_bounds__(256) observables_tile_kernel(const __grid_cons
   const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(ring);
   constexpr uint32_t SLOT_BYTES = 8u * SLOT;
   uint32_t pl[3] = {sbase + 2 * SLOT_BYTES, sbase, sbase + SLOT_BYTES};   // planes zu - 1, zu, zu + 1 at zu = 0
-  constexpr int SITES = Lat::b * OBS_TY * L1T;
+  constexpr int XY = OBS_TY * L1T;                 // (x, row) positions of a band; each covers every sublattice
+  const bool masked = p.mask != nullptr;
   for (int zu = 0; zu < g.L3; ++zu) {
-#pragma unroll 2
-    for (int i = threadIdx.x; i < SITES; i += blockDim.x) {
-      const int x = i % L1T, ty = (i / L1T) % OBS_TY, alpha = i / (L1T * OBS_TY);
-      const int site = alpha * g.plane + (zu * g.L2 + y0 + ty) * L1T + x;
-      if (p.mask != nullptr && p.mask[site] == 0) continue;
+    const bool more = zu + 1 < g.L3;
+    if (more) fetch(zu + 2);
+    for (int i = threadIdx.x; i < XY; i += 256) {
+      const int x = i % L1T, ty = i / L1T;
+      const int rsite = (zu * g.L2 + y0 + ty) * L1T + x;
       const uint32_t so = 8u * (uint32_t)((ty + 1) * RS + OBS_PAD + x);
-      double s[N];
-      double e = 0.0;
       static_for<0, Lat::b>([&](auto ac) {
         constexpr int a = decltype(ac)::value;
-        if (a != alpha) return;
+        const int site = a * g.plane + rsite;
+        if (masked && p.mask[site] == 0) return;
+        double s[N];
         static_for<0, N>([&](auto kc) {
           constexpr int k = decltype(kc)::value;
           s[k] = ldsd<8 * (a * N + k) * COMP>(pl[1] + so);
         });
         const SubObs& ob = p.obs[a];
+        double e = 0.0;
         static_for<0, Lat::n_bonds(a)>([&](auto ic) {
           constexpr int bi = decltype(ic)::value;
           if constexpr (forward_bond<Lat, a>(bi)) {
             constexpr BondC bd = Lat::bond(a, bi);
             constexpr int off = 8 * (bd.a2 * N * COMP + bd.dy * RS + bd.dx);
             const uint32_t q = pl[bd.dz + 1] + so;
-            double dot = 0.0;
-            static_for<0, N>([&](auto kc) {
+            double dot = s[0] * ldsd<off>(q);
+            static_for<1, N>([&](auto kc) {
               constexpr int k = decltype(kc)::value;
-              dot += s[k] * ldsd<off + 8 * k * COMP>(q);
+              dot = fma(s[k], ldsd<off + 8 * k * COMP>(q), dot);
             });
-            e -= ob.J[bi] * dot;
+            e = fma(-ob.J[bi], dot, e);
           }
         });
+#pragma unroll
+        for (int k = 0; k < N; ++k) e = fma(-p.h64[k], s[k], e);
+        if constexpr (N == 3) {
+          if (g.has_cubic) {
+            const double k1 = (double)p.k1[site];
+            const double xy = s[0] * s[1], xz = s[0] * s[2], yz = s[1] * s[2], xyz = xy * s[2];
+            e += k1 * (xy * xy + xz * xz + yz * yz) + p.k2 * xyz * xyz;
+          }
+        }
+        acc[0] += e;
+#pragma unroll
+        for (int k = 0; k < N; ++k) acc[1 + a * N + k] += s[k];
       });
-#pragma unroll
-      for (int k = 0; k < N; ++k) e -= p.h64[k] * s[k];
-      if constexpr (N == 3) {
-        if (g.has_cubic) {
-          const double k1 = (double)p.k1[site];
-          const double xy = s[0] * s[1], xz = s[0] * s[2], yz = s[1] * s[2], xyz = s[0] * s[1] * s[2];
-          e += k1 * (xy * xy + xz * xz + yz * yz) + p.k2 * xyz * xyz;
-        }
-      }
-      acc[0] += e;
-#pragma unroll
-      for (int a = 0; a < SCK_MAX_BASIS; ++a)
-        if (a == alpha) {
-#pragma unroll
-          for (int k = 0; k < N; ++k) acc[1 + a * N + k] += s[k];
-        }
     }
     __syncthreads();                              // every thread is done with plane zu - 1
     const uint32_t rot = pl[0];                   // the ring turns
     pl[0] = pl[1];
     pl[1] = pl[2];
     pl[2] = rot;
-    if (zu + 1 < g.L3) {
-      load_plane(zu + 2);                         // into plane zu - 1's slot
+    if (more) {
+      deposit(zu + 2);                            // into plane zu - 1's slot
       __syncthreads();
     }
   }
