@@ -181,6 +181,18 @@ int sck_observables_workspace_size(const sck_plan* plan, int32_t batch, int64_t*
 int sck_observables(const sck_plan* plan, const sck_buffers* buf, const void* spins, int32_t storage,
                     int32_t batch, double* E, double* M, void* workspace, void* stream);
 
+/* One observation of a measure step folded into FP64 accumulators: the reference's ladder runner
+ * (simulate_state, simulate.py:338-353) observes every `every` sweeps and accumulates, per replica r,
+ *   acc[0*batch + r] += E - E_ref[r],  acc[1*batch + r] += (E - E_ref[r])^2,
+ *   acc[2*batch + r] += |m|,           acc[3*batch + r] += |m|^2,            accv[r*n + k] += m_k,
+ * with E the total FP64 energy and m = (sum over sublattices of M) / n_active the mean magnetization vector.
+ * This entry point runs the sck_observables pass (E [batch], M [batch][b][n] receive the observation) and folds
+ * it in on the device, each quantity rounded in the reference's operation order; no host work, so a measure
+ * step of sweeps and this call can be captured in one CUDA graph. `workspace` as for sck_observables. */
+int sck_observables_accumulate(const sck_plan* plan, const sck_buffers* buf, const void* spins, int32_t storage,
+                               int32_t batch, double n_active, const double* E_ref, double* E, double* M,
+                               double* acc, double* accv, void* workspace, void* stream);
+
 /* sck_observables without a caller workspace — no counterpart in the reference (added for callers that cannot
  * allocate device memory: a host whose device memory all belongs to its own pool or caching allocator, a loop
  * that cannot afford the synchronisation an allocation may bring, an FFI binding that cannot own a device

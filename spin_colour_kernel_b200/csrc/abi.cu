@@ -541,6 +541,17 @@ int sck_observables(const sck_plan* plan, const sck_buffers* buf, const void* sp
   return launch_observables(plan, spins, storage, batch, buf->mask, buf->k1, E, M, workspace, (cudaStream_t)stream);
 }
 
+int sck_observables_accumulate(const sck_plan* plan, const sck_buffers* buf, const void* spins, int32_t storage,
+                               int32_t batch, double n_active, const double* E_ref, double* E, double* M,
+                               double* acc, double* accv, void* workspace, void* stream) {
+  if (E == nullptr || M == nullptr || E_ref == nullptr || acc == nullptr || accv == nullptr)
+    return fail(SCK_ERR_INVALID, "null observation or accumulator buffer");
+  if (!(n_active >= 1.0)) return fail(SCK_ERR_INVALID, "n_active must be at least 1");
+  int rc = sck_observables(plan, buf, spins, storage, batch, E, M, workspace, stream);
+  if (rc != SCK_OK) return rc;
+  return launch_observables_fold(plan, batch, E, M, n_active, E_ref, acc, accv, (cudaStream_t)stream);
+}
+
 int sck_pack(const sck_plan* plan, const int8_t* spins, int32_t* words, void* stream) {
   if (plan == nullptr || spins == nullptr || words == nullptr) return fail(SCK_ERR_INVALID, "null argument");
   if (plan->geom.n != 1) return fail(SCK_ERR_UNSUPPORTED, "packing is for Ising (n = 1) only");

@@ -140,6 +140,8 @@ int obs_blocks_per_rep(const sck_plan* plan, int batch);
 int made_wait_timeouts(unsigned long long* count);   // bounded waits of the learned proposal's kernels that gave up
 int launch_observables(const sck_plan* plan, const void* spins, int storage, int batch, const int8_t* mask,
                        const float* k1, double* E, double* M, void* workspace, cudaStream_t s);
+int launch_observables_fold(const sck_plan* plan, int batch, const double* E, const double* M, double n_active,
+                            const double* E_ref, double* acc, double* accv, cudaStream_t s);
 int launch_pack(const sck_plan* plan, const int8_t* spins, int32_t* words, cudaStream_t s);
 int launch_unpack(const sck_plan* plan, const int32_t* words, const int8_t* mask, int8_t* spins, cudaStream_t s);
 int launch_advance(int64_t* state, int n, cudaStream_t s);

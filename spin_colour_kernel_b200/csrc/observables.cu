@@ -243,6 +243,7 @@ static void launch_obs_spec(const ObsParams& p, dim3 grid, cudaStream_t s) {
 // left: the conversions and the index arithmetic, not the FP64 arithmetic or the HBM reads, bound the per-site
 // kernel above. Same bond-once energy and the same fixed-order partial sums.
 constexpr int OBS_TY = 4;                     // rows per band
+constexpr int OBS_THREADS = 256;              // threads per block
 constexpr int OBS_PAD = 2;                    // doubles before x = 0 in a shared row: x = -1 sits at OBS_PAD - 1
 constexpr size_t OBS_TILE_SMEM_MAX = 110 * 1024;
 
@@ -276,7 +277,7 @@ __device__ __forceinline__ double ldsd(uint32_t addr) {
 }
 
 template <class Lat, int N, int L1T>
-__global__ void __launch_bounds__(256) observables_tile_kernel(const __grid_constant__ ObsParams p) {
+__global__ void __launch_bounds__(OBS_THREADS) observables_tile_kernel(const __grid_constant__ ObsParams p) {
   extern __shared__ __align__(16) double ring[];   // [3 planes][b][N][R2 rows][RS]
   using RW = ObsRow<L1T>;
   constexpr int RS = RW::RS, R2 = RW::R2;
@@ -284,41 +285,45 @@ __global__ void __launch_bounds__(256) observables_tile_kernel(const __grid_cons
   constexpr int SLOT = Lat::b * N * COMP;
   constexpr int Q = L1T / 4;                       // float4 loads per row
   constexpr int ITEMS = Lat::b * N * R2 * Q;       // float4 loads per plane
-  constexpr int LOADS = (ITEMS + 255) / 256;       // per thread
+  constexpr int LOADS = (ITEMS + OBS_THREADS - 1) / OBS_THREADS;       // per thread
   const Geometry& g = p.g;
   const int rep = blockIdx.y, y0 = blockIdx.x * OBS_TY;
   const float* src = (const float*)p.spins + (size_t)rep * N * g.nsite;
   // The next plane's loads are issued into registers before the current plane is computed and written to
   // shared memory (as FP64) after it, so HBM latency overlaps the FP64 work.
+  // Each thread's loads keep the same rows and columns from plane to plane: their offsets within a plane (floats)
+  // and their shared-memory destinations (doubles) are formed once.
   float4 pf[LOADS];
+  uint32_t gofs[LOADS];
+  int sdst[LOADS];
+#pragma unroll
+  for (int j = 0; j < LOADS; ++j) {
+    const int i = threadIdx.x + OBS_THREADS * j;
+    const int row = i / Q, q = i % Q;
+    const int r = row % R2, ak = row / R2, k = ak % N, a = ak / N;
+    int y = y0 - 1 + r;
+    y = y < 0 ? y + g.L2 : (y >= g.L2 ? y - g.L2 : y);
+    gofs[j] = (uint32_t)k * (uint32_t)g.nsite + (uint32_t)a * (uint32_t)g.plane + (uint32_t)y * L1T + 4u * q;
+    sdst[j] = row * RS + OBS_PAD + 4 * q;
+  }
+  const uint32_t zstride = (uint32_t)g.L2 * L1T;
   auto fetch = [&](int zu) {   // unwrapped plane index -1 .. L3
     const int zz = zu < 0 ? zu + g.L3 : (zu >= g.L3 ? zu - g.L3 : zu);
+    const float* sp = src + (uint32_t)zz * zstride;
 #pragma unroll
-    for (int j = 0; j < LOADS; ++j) {
-      const int i = threadIdx.x + 256 * j;
-      if (ITEMS % 256 == 0 || i < ITEMS) {
-        const int row = i / Q, q = i % Q;
-        const int r = row % R2, ak = row / R2, k = ak % N, a = ak / N;
-        int y = y0 - 1 + r;
-        y = y < 0 ? y + g.L2 : (y >= g.L2 ? y - g.L2 : y);
-        pf[j] = *(const float4*)(src + (size_t)k * g.nsite + (size_t)a * g.plane +
-                                 ((size_t)zz * g.L2 + y) * L1T + 4 * q);
-      }
-    }
+    for (int j = 0; j < LOADS; ++j)
+      if (ITEMS % OBS_THREADS == 0 || threadIdx.x + OBS_THREADS * j < ITEMS) pf[j] = *(const float4*)(sp + gofs[j]);
   };
   auto deposit = [&](int zu) {
     double* dst = ring + ((zu + 3) % 3) * SLOT;
 #pragma unroll
     for (int j = 0; j < LOADS; ++j) {
-      const int i = threadIdx.x + 256 * j;
-      if (ITEMS % 256 == 0 || i < ITEMS) {
-        const int row = i / Q, q = i % Q;
-        double* d = dst + row * RS + OBS_PAD + 4 * q;
+      if (ITEMS % OBS_THREADS == 0 || threadIdx.x + OBS_THREADS * j < ITEMS) {
+        double* d = dst + sdst[j];
         const float4 v = pf[j];
-        d[0] = v.x;
-        d[1] = v.y;
-        d[2] = v.z;
-        d[3] = v.w;
+        *(double2*)d = make_double2(v.x, v.y);          // 16-byte aligned: RS and OBS_PAD are even
+        *(double2*)(d + 2) = make_double2(v.z, v.w);
+        const int q = (threadIdx.x + OBS_THREADS * j) % Q;
         if (q == 0) d[L1T] = v.x;            // x = L1 is x = 0
         if (q == Q - 1) d[-L1T + 3] = v.w;   // x = -1 is x = L1 - 1
       }
@@ -343,7 +348,7 @@ __global__ void __launch_bounds__(256) observables_tile_kernel(const __grid_cons
   for (int zu = 0; zu < g.L3; ++zu) {
     const bool more = zu + 1 < g.L3;
     if (more) fetch(zu + 2);
-    for (int i = threadIdx.x; i < XY; i += 256) {
+    for (int i = threadIdx.x; i < XY; i += OBS_THREADS) {
       const int x = i % L1T, ty = i / L1T;
       const int rsite = (zu * g.L2 + y0 + ty) * L1T + x;
       const uint32_t so = 8u * (uint32_t)((ty + 1) * RS + OBS_PAD + x);
@@ -396,7 +401,7 @@ __global__ void __launch_bounds__(256) observables_tile_kernel(const __grid_cons
       __syncthreads();
     }
   }
-  __shared__ double red[NV][8];
+  __shared__ double red[NV][OBS_THREADS / 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int i = 0; i < NV; ++i) {
@@ -420,7 +425,7 @@ static int launch_obs_tile_t(const sck_plan* plan, const ObsParams& p, cudaStrea
   const int rc = cuda_status(cudaFuncSetAttribute(observables_tile_kernel<Lat, N, L1T>,
                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                              "obs tile");
-  if (rc == SCK_OK) observables_tile_kernel<Lat, N, L1T><<<grid, 256, smem, s>>>(p);
+  if (rc == SCK_OK) observables_tile_kernel<Lat, N, L1T><<<grid, OBS_THREADS, smem, s>>>(p);
   return rc;
 }
 
@@ -471,6 +476,39 @@ int obs_blocks_per_rep(const sck_plan* plan, int batch) {
   const int gen = obs_blocks_generic(plan, batch);
   const int tile = obs_tile_geometry(plan) ? plan->geom.L2 / OBS_TY : 0;
   return gen > tile ? gen : tile;
+}
+
+// One observation of a measure step folded into FP64 accumulators, per replica r (one thread each): with
+// d = E - E_ref and m = (sum over sublattices of M) / n_active,
+//   acc[0][r] += d, acc[1][r] += d^2, acc[2][r] += |m|, acc[3][r] += |m|^2, accv[r][k] += m_k,
+// the quantities the reference's ladder runner accumulates per observation (simulate.py:338-353), rounded
+// operation by operation in the same order (no contraction into fused multiply-adds).
+__global__ void observables_fold(const double* __restrict__ E, const double* __restrict__ M, int B, int b, int n,
+                                 double n_active, const double* __restrict__ E_ref, double* __restrict__ acc,
+                                 double* __restrict__ accv) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= B) return;
+  const double d = __dsub_rn(E[r], E_ref[r]);
+  double sq = 0.0;
+  for (int k = 0; k < n; ++k) {
+    double m = 0.0;
+    for (int a = 0; a < b; ++a) m = __dadd_rn(m, M[((size_t)r * b + a) * n + k]);
+    m = __ddiv_rn(m, n_active);
+    sq = __dadd_rn(sq, __dmul_rn(m, m));
+    accv[(size_t)r * n + k] = __dadd_rn(accv[(size_t)r * n + k], m);
+  }
+  const double am = __dsqrt_rn(sq);
+  acc[r] = __dadd_rn(acc[r], d);
+  acc[B + r] = __dadd_rn(acc[B + r], __dmul_rn(d, d));
+  acc[2 * B + r] = __dadd_rn(acc[2 * B + r], am);
+  acc[3 * B + r] = __dadd_rn(acc[3 * B + r], __dmul_rn(am, am));
+}
+
+int launch_observables_fold(const sck_plan* plan, int batch, const double* E, const double* M, double n_active,
+                            const double* E_ref, double* acc, double* accv, cudaStream_t s) {
+  observables_fold<<<(batch + 127) / 128, 128, 0, s>>>(E, M, batch, plan->geom.b, plan->geom.n, n_active, E_ref,
+                                                       acc, accv);
+  return cuda_status(cudaGetLastError(), "observables fold");
 }
 
 int launch_observables(const sck_plan* plan, const void* spins, int storage, int batch, const int8_t* mask,

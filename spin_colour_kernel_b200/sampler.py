@@ -395,6 +395,32 @@ class Sampler:
                                             _ptr(self._workspace(batch)), self._stream()))
         return E, M
 
+    def observe(self, S: torch.Tensor, E_ref: torch.Tensor, acc: torch.Tensor, accv: torch.Tensor,
+                E: torch.Tensor, M: torch.Tensor):
+        """One observation folded into FP64 accumulators on the device (the measure step of the ladder runner,
+        simulate.py:338-353): with d = E - E_ref and m the mean magnetization vector, acc[0] += d,
+        acc[1] += d^2, acc[2] += |m|, acc[3] += |m|^2 and accv += m, per replica. acc is (4, B), accv (B, n),
+        E (B,) and M (B, b, n) receive the observation; all float64 on this device. Graph-safe."""
+        s = self.sys
+        B = self.B
+        for t, shape in ((E_ref, (B,)), (E, (B,)), (M, (B, s.b, s.n)), (acc, (4, B)), (accv, (B, s.n))):
+            if t.dtype != torch.float64 or tuple(t.shape) != shape or t.device != self.device or not t.is_contiguous():
+                raise ValueError(f"observe wants contiguous float64 {shape} tensors on {self.device}")
+        if S.dtype == torch.int32 and self.packed:
+            self._check(S)
+            storage = L.MODE_PACKED
+        else:
+            storage = L.MODE_INT8 if (S.dtype == torch.int8 and s.n == 1) else L.MODE_F32
+            if storage == L.MODE_F32 and S.dtype != torch.float32:
+                raise ValueError("observe reads this sampler's storage: int8, float32 or packed words")
+            if tuple(S.shape) != (B, s.n) + s.shape or S.device != self.device or not S.is_contiguous():
+                raise ValueError(f"spins must have shape ({B}, {s.n}) + {s.shape} on {self.device}")
+        buf = self._buffers(S)
+        with torch.cuda.device(self.device):
+            L.check(L.lib().sck_observables_accumulate(
+                self._plan, ctypes.byref(buf), _ptr(S), storage, B, float(s.n_active), _ptr(E_ref), _ptr(E),
+                _ptr(M), _ptr(acc), _ptr(accv), _ptr(self._workspace(B)), self._stream()))
+
     def energy(self, S: torch.Tensor) -> torch.Tensor:
         """Total energy per replica, float64."""
         return self.observables(S)[0]

@@ -40,7 +40,7 @@ def main(argv=None):
 
     import cases as C
 
-    names = a.cases or list(C.CASES) + ["philox", "quickstart", "tables"]
+    names = a.cases or list(C.CASES) + ["philox", "quickstart", "tables", "simulate"]
     for name in names:
         t0 = time.time()
         if name == "philox":
@@ -49,6 +49,8 @@ def main(argv=None):
             _quickstart(torch, sy, Sampler)
         elif name == "tables":
             _tables(np, bw, sy, cr)
+        elif name == "simulate":
+            _simulate(np, a.ref)
         else:
             case = C.CASES[name]
             s = case["build"](sy, cr)
@@ -153,6 +155,24 @@ def _tables(np, bw, sy, cr):
     out["masked_h_metropolis_P"] = bw.p_fixed(m, betas)
     out["betas"] = betas
     np.savez_compressed(HERE / "tables.npz", **out)
+
+
+def _simulate(np, ref):
+    """The reference's one-state ladder runner (simulate.py:322-402) on its CPU path: Ising chains (bit-exact on
+    every backend), so the accumulated FP64 observables are a fixture for the same runner on the GPU."""
+    from Spin_Colour_Kernel import simulate as SIM
+    out = {}
+    runs = {
+        "square": (SIM.build_system("ising", "square", (8, 8), (True, True), {"J": {1: 1.0}, "H": 0.1}),
+                   dict(replicas=4, temps=[3.0, 2.5, 2.0], n_therm=4, n_meas=6, every=2, config_every=2, seed=1)),
+        "sc_word": (SIM.build_system("ising", "sc", (4, 4, 4), (True, True, True), {"J": {1: 1.0}}),
+                    dict(replicas=32, temps=[5.0, 4.0], n_therm=3, n_meas=4, every=1, config_every=1, seed=2)),
+    }
+    for key, (s, kw) in runs.items():
+        r = SIM.simulate_state(s, device="cpu", kB=1.0, log=lambda m: None, **kw)
+        for f in ("M", "E", "E2", "Mabs", "M2", "configs", "config_temperatures"):
+            out[f"{key}_{f}"] = np.asarray(r[f])
+    np.savez_compressed(HERE / "simulate.npz", **out)
 
 
 if __name__ == "__main__":

@@ -206,3 +206,19 @@ def test_seam_condition_rejects_odd_box():
     assert not co.seam_ok(col, (4, 4), (True, True))
     with pytest.raises(ValueError):
         sy.System("bad", 1, c, (4, 4), (True, True), {1: 1.0}, colouring=col)
+
+
+def test_temperature_ladder_and_runner_fixture():
+    """The ladder of the one-state runner, and the recorded outputs of the reference's runner it is tested on."""
+    from spin_colour_kernel_b200.simulate import temperature_ladder
+    assert list(temperature_ladder(2.0, 1.0, 0.5)) == [2.0, 1.5, 1.0]
+    assert list(temperature_ladder(3.0, 2.0, 0.3)) == [3.0, 2.7, 2.4, 2.1]
+    for bad in ((1.0, 2.0, 0.5), (2.0, 0.0, 0.5), (2.0, 1.0, 0.0)):
+        with pytest.raises(ValueError):
+            temperature_ladder(*bad)
+    g = np.load(GOLD / "simulate.npz")
+    for key, B, nT, sites in (("square", 4, 3, 64), ("sc_word", 32, 2, 64)):
+        assert g[f"{key}_E"].shape == (B, nT) and g[f"{key}_M"].shape == (B, nT, 3)
+        assert np.all(g[f"{key}_E2"] >= g[f"{key}_E"] ** 2 - 1e-9)        # a variance is not negative
+        assert np.all(np.isin(g[f"{key}_configs"][..., 0], (-1.0, 1.0)))
+        assert g[f"{key}_configs"].shape[2] == sites
