@@ -72,13 +72,14 @@ struct SegRows {
 
 __device__ __forceinline__ int wrap1(int v, int L) { return v < 0 ? v + L : (v >= L ? v - L : v); }
 
-// the two class sites x0 + D and x0 + D + 2 of row (y, z), sublattice A, replica rep
-template <class Lat, int A, int N, int D>
+// the two class sites x0 + D and x0 + D + 2 of row (y, z), sublattice A, replica rep; NSL > 0: the replica has
+// 2^NSL sites and the component planes sit at compile-time offsets from one address
+template <class Lat, int A, int N, int D, int NSL>
 __device__ __forceinline__ void seg_sites(const Common& c, const float (&J)[SCK_MAX_GROUPS], int rep, int y, int z,
                                           int x0, int32_t key) {
   using R = SegRows<Lat, A>;
   const Geometry& g = c.g;
-  const size_t NS = (size_t)g.nsite;
+  const size_t NS = NSL ? ((size_t)1 << NSL) : (size_t)g.nsite;
   const float* base = (const float*)c.src + (size_t)rep * N * NS;
   float* obase = (float*)c.dst + (size_t)rep * N * NS;
   const float* bk[N];   // component planes of the replica: each load is one 32-bit index off these
@@ -148,7 +149,7 @@ __device__ __forceinline__ void seg_sites(const Common& c, const float (&J)[SCK_
 }
 
 // Grid (ceil(rows * L1 / 4 / 256), n_tasks * units_per_task); block y-slot -> (task, replica).
-template <class Lat, int N>
+template <class Lat, int N, int NSL>
 __global__ void __launch_bounds__(256, 4) seg_kernel(const __grid_constant__ SpecParams p) {
   const Common& c = p.c;
   const Geometry& g = c.g;
@@ -174,9 +175,9 @@ __global__ void __launch_bounds__(256, 4) seg_kernel(const __grid_constant__ Spe
     constexpr int a = decltype(ac)::value;
     if (a != alpha) return;
     if (d == 0)
-      seg_sites<Lat, a, N, 0>(c, p.J[a], rep, y, z, x0, key);
+      seg_sites<Lat, a, N, 0, NSL>(c, p.J[a], rep, y, z, x0, key);
     else
-      seg_sites<Lat, a, N, 1>(c, p.J[a], rep, y, z, x0, key);
+      seg_sites<Lat, a, N, 1, NSL>(c, p.J[a], rep, y, z, x0, key);
   });
 }
 
@@ -205,12 +206,24 @@ bool seg_kernel_ok(const sck_plan* plan) {
   }
 }
 
+template <class Lat, int N>
+static void launch_seg_n(const sck_plan* plan, const SpecParams& p, dim3 grid, cudaStream_t s) {
+  // replicas of 2^16 .. 2^19 sites: component offsets up to 4 MB fit a load's immediate offset
+  switch (plan->geom.nsite) {
+    case 1 << 16: seg_kernel<Lat, N, 16><<<grid, 256, 0, s>>>(p); break;
+    case 1 << 17: seg_kernel<Lat, N, 17><<<grid, 256, 0, s>>>(p); break;
+    case 1 << 18: seg_kernel<Lat, N, 18><<<grid, 256, 0, s>>>(p); break;
+    case 1 << 19: seg_kernel<Lat, N, 19><<<grid, 256, 0, s>>>(p); break;
+    default: seg_kernel<Lat, N, 0><<<grid, 256, 0, s>>>(p); break;
+  }
+}
+
 template <class Lat>
 static void launch_seg_lat(const sck_plan* plan, const SpecParams& p, dim3 grid, cudaStream_t s) {
   if (plan->geom.n == 2)
-    seg_kernel<Lat, 2><<<grid, 256, 0, s>>>(p);
+    launch_seg_n<Lat, 2>(plan, p, grid, s);
   else
-    seg_kernel<Lat, 3><<<grid, 256, 0, s>>>(p);
+    launch_seg_n<Lat, 3>(plan, p, grid, s);
 }
 
 int launch_seg_tasks(const sck_plan* plan, SpecParams& p, int ys, cudaStream_t s) {

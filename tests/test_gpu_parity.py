@@ -258,6 +258,12 @@ SEG_SYSTEMS = {
     "xy_square_128x10": lambda: sy.System("XY square", 2, cr.make("square"), (128, 10), (True, True), {1: 1.0},
                                           h=(0.05, 0.0)),
     "xy_square_24x7": lambda: sy.System("XY square", 2, cr.make("square"), (24, 7), (True, True), {1: 1.0}),
+    # 2^16 sites: compile-time component offsets
+    "heis_bcc_j1j2_32x16x64": lambda: sy.System("Heisenberg bcc J1-J2", 3, cr.make("bcc", (1, 2)), (32, 16, 64),
+                                                (True,) * 3, {1: 1.0, 2: 0.3}, h=(0.0, 0.0, 0.1),
+                                                cubic_k1=np.full((2, 64, 16, 32), 0.05, np.float32)),
+    "xy_square_256x256": lambda: sy.System("XY square", 2, cr.make("square"), (256, 256), (True, True), {1: 1.0},
+                                           h=(0.05, 0.0)),
 }
 
 
