@@ -291,39 +291,35 @@ __global__ void __launch_bounds__(OBS_THREADS) observables_tile_kernel(const __g
   const float* src = (const float*)p.spins + (size_t)rep * N * g.nsite;
   // The next plane's loads are issued into registers before the current plane is computed and written to
   // shared memory (as FP64) after it, so HBM latency overlaps the FP64 work.
-  // Each thread's loads keep the same rows and columns from plane to plane: their offsets within a plane (floats)
-  // and their shared-memory destinations (doubles) are formed once.
   float4 pf[LOADS];
-  uint32_t gofs[LOADS];
-  int sdst[LOADS];
-#pragma unroll
-  for (int j = 0; j < LOADS; ++j) {
-    const int i = threadIdx.x + OBS_THREADS * j;
-    const int row = i / Q, q = i % Q;
-    const int r = row % R2, ak = row / R2, k = ak % N, a = ak / N;
-    int y = y0 - 1 + r;
-    y = y < 0 ? y + g.L2 : (y >= g.L2 ? y - g.L2 : y);
-    gofs[j] = (uint32_t)k * (uint32_t)g.nsite + (uint32_t)a * (uint32_t)g.plane + (uint32_t)y * L1T + 4u * q;
-    sdst[j] = row * RS + OBS_PAD + 4 * q;
-  }
-  const uint32_t zstride = (uint32_t)g.L2 * L1T;
   auto fetch = [&](int zu) {   // unwrapped plane index -1 .. L3
     const int zz = zu < 0 ? zu + g.L3 : (zu >= g.L3 ? zu - g.L3 : zu);
-    const float* sp = src + (uint32_t)zz * zstride;
 #pragma unroll
-    for (int j = 0; j < LOADS; ++j)
-      if (ITEMS % OBS_THREADS == 0 || threadIdx.x + OBS_THREADS * j < ITEMS) pf[j] = *(const float4*)(sp + gofs[j]);
+    for (int j = 0; j < LOADS; ++j) {
+      const int i = threadIdx.x + OBS_THREADS * j;
+      if (ITEMS % OBS_THREADS == 0 || i < ITEMS) {
+        const int row = i / Q, q = i % Q;
+        const int r = row % R2, ak = row / R2, k = ak % N, a = ak / N;
+        int y = y0 - 1 + r;
+        y = y < 0 ? y + g.L2 : (y >= g.L2 ? y - g.L2 : y);
+        pf[j] = *(const float4*)(src + (size_t)k * g.nsite + (size_t)a * g.plane +
+                                 ((size_t)zz * g.L2 + y) * L1T + 4 * q);
+      }
+    }
   };
   auto deposit = [&](int zu) {
     double* dst = ring + ((zu + 3) % 3) * SLOT;
 #pragma unroll
     for (int j = 0; j < LOADS; ++j) {
-      if (ITEMS % OBS_THREADS == 0 || threadIdx.x + OBS_THREADS * j < ITEMS) {
-        double* d = dst + sdst[j];
+      const int i = threadIdx.x + OBS_THREADS * j;
+      if (ITEMS % OBS_THREADS == 0 || i < ITEMS) {
+        const int row = i / Q, q = i % Q;
+        double* d = dst + row * RS + OBS_PAD + 4 * q;
         const float4 v = pf[j];
-        *(double2*)d = make_double2(v.x, v.y);          // 16-byte aligned: RS and OBS_PAD are even
-        *(double2*)(d + 2) = make_double2(v.z, v.w);
-        const int q = (threadIdx.x + OBS_THREADS * j) % Q;
+        d[0] = v.x;
+        d[1] = v.y;
+        d[2] = v.z;
+        d[3] = v.w;
         if (q == 0) d[L1T] = v.x;            // x = L1 is x = 0
         if (q == Q - 1) d[-L1T + 3] = v.w;   // x = -1 is x = L1 - 1
       }
