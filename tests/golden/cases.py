@@ -155,3 +155,21 @@ def temperatures(spec, B):
 
 def sampler_kwargs(case: dict) -> dict:
     return {k: case[k] for k in ("packed", "bitwise", "independent", "compact", "max_block") if k in case}
+
+
+# run-driver cases (tests/test_runs.py; fixtures from make_golden.py runs)
+SHAPES = [("sc", (9, 9, 9), "spherical", "r <= 3"), ("sc", (11, 11, 6), "cylindrical", "(rho <= 4) & (abs(z) <= 1.5)"),
+          ("bcc", (6, 6, 6), "cartesian", "~((abs(x) < 1) | (abs(y) < 1)) ^ (z > 0)"),
+          ("triangular", (12, 10), "cylindrical", "(rho <= 4) & (rho >= 1.5)"),
+          ("fcc", (4, 4, 4), "spherical", "(cos(theta) > 0) & (r ** 2 <= 2 * pi)"), ("kagome", (6, 6), "", "")]
+THETAS = [("heisenberg", "sc", (7, 7, 3), (False, False, False), "cylindrical", "rho <= 3",
+           {"J": {1: 1.0}, "D": 0.88, "K1": 0.177, "Ks": 0.139, "K2": 0.034, "H": 0.483, "H_theta": 30.0,
+            "H_phi": 45.0}),
+          ("heisenberg", "bcc", (4, 4, 4), (True, True, True), "", "", {"J": {1: 1.0, 2: 0.3}, "K1": 0.05, "H": 0.1}),
+          ("xy", "triangular", (6, 6), (True, True), "", "", {"J": {1: 1.0, 2: -0.3}, "H": 0.1, "H_phi": 60.0}),
+          ("ising", "square", (37, 5), (True, True), "", "", {"J": {1: 1.0}, "H": 0.2}),
+          ("heisenberg", "honeycomb", (6, 6), (True, True), "", "", {"J": {"1": 1.0}, "D": 0.3})]
+RUN_CFG = dict(model="ising", crystal="square", box=[6, 6], periodic=[True, True], coords="cylindrical",
+               shape="rho <= 2.6", states=[{"name": "a", "J": {"1": 1.0}}, {"name": "b", "J": {"1": 1.0}, "H": 0.2}],
+               replicas=5, T_max=3.0, T_min=2.0, T_step=0.5, thermalization=3, measurement=3, measure_every=1,
+               units="reduced", seed=1)

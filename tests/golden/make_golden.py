@@ -40,7 +40,7 @@ def main(argv=None):
 
     import cases as C
 
-    names = a.cases or list(C.CASES) + ["philox", "quickstart", "tables", "simulate"]
+    names = a.cases or list(C.CASES) + ["philox", "quickstart", "tables", "simulate", "runs"]
     for name in names:
         t0 = time.time()
         if name == "philox":
@@ -51,6 +51,8 @@ def main(argv=None):
             _tables(np, bw, sy, cr)
         elif name == "simulate":
             _simulate(np, a.ref)
+        elif name == "runs":
+            _runs(np, sy)
         else:
             case = C.CASES[name]
             s = case["build"](sy, cr)
@@ -173,6 +175,40 @@ def _simulate(np, ref):
         for f in ("M", "E", "E2", "Mabs", "M2", "configs", "config_temperatures"):
             out[f"{key}_{f}"] = np.asarray(r[f])
     np.savez_compressed(HERE / "simulate.npz", **out)
+
+
+def _runs(np, sy):
+    """The reference's run driver (simulate.py): geometry, Hamiltonians, prepared files, collect, and a small
+    Ising run in two replica blocks on its CPU path."""
+    import tempfile
+    from Spin_Colour_Kernel import simulate as SIM
+    out = {}
+    import cases as C
+    for i, (cry, box, coords, shape) in enumerate(C.SHAPES):
+        pos, mask = SIM.active_sites(cry, box, coords, shape)
+        out[f"shape{i}_pos"], out[f"shape{i}_mask"] = pos, mask
+    for i, (model, cry, box, per, coords, shape, theta) in enumerate(C.THETAS):
+        _, mask = SIM.active_sites(cry, box, coords, shape)
+        s = SIM.build_system(model, cry, box, per, theta, mask=mask if shape else None, log=lambda m: None)
+        out[f"theta{i}_bonds"] = np.stack([s.bond_matrix(k) for k in range(len(s.crystal.bonds))])
+        out[f"theta{i}_k1"] = np.zeros(0) if s.cubic_k1 is None else s.cubic_k1
+        out[f"theta{i}_h"] = np.zeros(0) if s.h is None else np.asarray(s.h)
+        out[f"theta{i}_periodic"] = np.asarray(s.periodic)
+        out[f"theta{i}_k2"] = np.float64(s.cubic_k2)
+    with tempfile.TemporaryDirectory() as d:
+        run = SIM.prepare(dict(C.RUN_CFG), d, log=lambda m: None)
+        out["run_json"] = np.array((Path(d) / "run.json").read_text())
+        out["run_sites"] = np.load(Path(d) / "sites.npy")
+        out["run_mask"] = np.load(Path(d) / "mask.npy")
+        for part, rng in enumerate(SIM.replica_blocks(run["replicas"], 2)):
+            SIM.run(run, [0, 1], d, device="cpu", log=lambda m: None, replicas=rng, part=part)
+        res = SIM.collect(d)
+        for k, v in res.items():
+            out[f"run_res_{k}"] = v
+        out["run_configs"] = np.load(Path(d) / "configurations.npy")
+        z = np.load(Path(d) / "state_001_p01.npz")
+        out["run_state_keys"] = np.array(sorted(z.files))
+    np.savez_compressed(HERE / "runs.npz", **out)
 
 
 if __name__ == "__main__":
