@@ -193,6 +193,13 @@ int sck_observables_accumulate(const sck_plan* plan, const sck_buffers* buf, con
                                int32_t batch, double n_active, const double* E_ref, double* E, double* M,
                                double* acc, double* accv, void* workspace, void* stream);
 
+/* Berg-Luscher topological charge per replica of z-layer `layer` of sublattice 0 (the nanodisk anneal's middle
+ * layer, anneal.py:69-80 and Observer.__call__ :125-146): over every plaquette of the layer whose four corners
+ * are active, the solid angles of its two spherical triangles, Q = sum / 4 pi, in FP64. Float32 Heisenberg
+ * storage; Q holds `batch` doubles. No workspace; one block per replica. */
+int sck_topological_charge(const sck_plan* plan, const sck_buffers* buf, const float* spins, int32_t batch,
+                           int32_t layer, double* Q, void* stream);
+
 /* sck_observables without a caller workspace — no counterpart in the reference (added for callers that cannot
  * allocate device memory: a host whose device memory all belongs to its own pool or caching allocator, a loop
  * that cannot afford the synchronisation an allocation may bring, an FFI binding that cannot own a device

@@ -56,3 +56,17 @@ def energy(sys_, S: np.ndarray) -> np.ndarray:
 def magnetization(S: np.ndarray) -> np.ndarray:
     """(B, b, n) float64."""
     return np.asarray(S, np.float64).sum(axis=(3, 4, 5)).transpose(0, 2, 1)
+
+
+def berg_luscher_q(layer: np.ndarray, valid: np.ndarray) -> np.ndarray:
+    """Topological charge per replica of one layer (B, 3, Ny, Nx), FP64: every valid plaquette (Ny-1, Nx-1) cut
+    into the spherical triangles (s00, s10, s11), (s00, s11, s01) of solid angle
+    2 atan2(a . (b x c), 1 + a . b + b . c + c . a), summed and divided by 4 pi (anneal.py:69-80)."""
+    s = np.moveaxis(np.asarray(layer, np.float64), 1, -1)
+    s00, s10, s01, s11 = s[:, :-1, :-1], s[:, :-1, 1:], s[:, 1:, :-1], s[:, 1:, 1:]
+
+    def omega(a, b, c):
+        num = (a * np.cross(b, c)).sum(-1)
+        den = 1.0 + (a * b).sum(-1) + (b * c).sum(-1) + (c * a).sum(-1)
+        return 2.0 * np.arctan2(num, den)
+    return ((omega(s00, s10, s11) + omega(s00, s11, s01)) * valid).sum(axis=(1, 2)) / (4.0 * np.pi)

@@ -60,6 +60,7 @@ _SIGNATURES = {
     "sck_reference_sweep": ([_vp, ctypes.POINTER(Buffers), _i32, _vp], _i32),
     "sck_observables_workspace_size": ([_vp, _i32, ctypes.POINTER(_i64)], _i32),
     "sck_observables": ([_vp, ctypes.POINTER(Buffers), _vp, _i32, _i32, _vp, _vp, _vp, _vp], _i32),
+    "sck_topological_charge": ([_vp, ctypes.POINTER(Buffers), _vp, _i32, _i32, _vp, _vp], _i32),
     "sck_observables_accumulate": ([_vp, ctypes.POINTER(Buffers), _vp, _i32, _i32, ctypes.c_double, _vp, _vp, _vp,
                                     _vp, _vp, _vp, _vp], _i32),
     "sck_observables_noalloc": ([_vp, ctypes.POINTER(Buffers), _vp, _i32, _i32, _vp, _vp, _vp], _i32),

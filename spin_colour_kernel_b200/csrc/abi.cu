@@ -552,6 +552,20 @@ int sck_observables_accumulate(const sck_plan* plan, const sck_buffers* buf, con
   return launch_observables_fold(plan, batch, E, M, n_active, E_ref, acc, accv, (cudaStream_t)stream);
 }
 
+int sck_topological_charge(const sck_plan* plan, const sck_buffers* buf, const float* spins, int32_t batch,
+                           int32_t layer, double* Q, void* stream) {
+  if (plan == nullptr || buf == nullptr || spins == nullptr || Q == nullptr)
+    return fail(SCK_ERR_INVALID, "null plan, buffers, spins or output");
+  const Geometry& g = plan->geom;
+  if (g.n != 3 || plan->mode != SCK_MODE_F32) return fail(SCK_ERR_INVALID, "the charge needs float32 Heisenberg spins");
+  if (g.dim != 3 && layer != 0) return fail(SCK_ERR_INVALID, "a 2D system has one layer: 0");
+  if (layer < 0 || layer >= g.L3) return fail(SCK_ERR_INVALID, "layer outside 0..L3-1");
+  if (batch < 1 || batch > plan->batch) return fail(SCK_ERR_INVALID, "batch outside 1..the plan's batch");
+  if (g.L1 < 2 || g.L2 < 2) return fail(SCK_ERR_INVALID, "a layer needs at least 2 x 2 sites");
+  if (g.has_mask && buf->mask == nullptr) return fail(SCK_ERR_INVALID, "the system has a mask: pass it");
+  return launch_topological_charge(plan, spins, buf->mask, batch, layer, Q, (cudaStream_t)stream);
+}
+
 int sck_pack(const sck_plan* plan, const int8_t* spins, int32_t* words, void* stream) {
   if (plan == nullptr || spins == nullptr || words == nullptr) return fail(SCK_ERR_INVALID, "null argument");
   if (plan->geom.n != 1) return fail(SCK_ERR_UNSUPPORTED, "packing is for Ising (n = 1) only");

@@ -142,6 +142,8 @@ int launch_observables(const sck_plan* plan, const void* spins, int storage, int
                        const float* k1, double* E, double* M, void* workspace, cudaStream_t s);
 int launch_observables_fold(const sck_plan* plan, int batch, const double* E, const double* M, double n_active,
                             const double* E_ref, double* acc, double* accv, cudaStream_t s);
+int launch_topological_charge(const sck_plan* plan, const float* spins, const int8_t* mask, int batch, int z,
+                              double* Q, cudaStream_t s);
 int launch_pack(const sck_plan* plan, const int8_t* spins, int32_t* words, cudaStream_t s);
 int launch_unpack(const sck_plan* plan, const int32_t* words, const int8_t* mask, int8_t* spins, cudaStream_t s);
 int launch_advance(int64_t* state, int n, cudaStream_t s);

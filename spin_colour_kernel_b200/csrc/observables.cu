@@ -507,6 +507,61 @@ int launch_observables_fold(const sck_plan* plan, int batch, const double* E, co
   return cuda_status(cudaGetLastError(), "observables fold");
 }
 
+// Berg-Luscher topological charge of one z-layer of sublattice 0 (the nanodisk's middle layer,
+// anneal.py:69-80): every plaquette (y, x)-(y+1, x+1) whose four corners are active is cut into the spherical
+// triangles (s00, s10, s11) and (s00, s11, s01), each of solid angle
+//   Omega(a, b, c) = 2 atan2(a . (b x c), 1 + a . b + b . c + c . a),
+// and Q = sum Omega / 4 pi, in FP64 from the float32 spins. One block per replica, partial sums in a fixed order.
+__device__ __forceinline__ double solid_angle(const double (&a)[3], const double (&b)[3], const double (&c)[3]) {
+  const double x0 = __dsub_rn(__dmul_rn(b[1], c[2]), __dmul_rn(b[2], c[1]));
+  const double x1 = __dsub_rn(__dmul_rn(b[2], c[0]), __dmul_rn(b[0], c[2]));
+  const double x2 = __dsub_rn(__dmul_rn(b[0], c[1]), __dmul_rn(b[1], c[0]));
+  const double num = __dadd_rn(__dadd_rn(__dmul_rn(a[0], x0), __dmul_rn(a[1], x1)), __dmul_rn(a[2], x2));
+  auto dot = [](const double (&u)[3], const double (&v)[3]) {
+    return __dadd_rn(__dadd_rn(__dmul_rn(u[0], v[0]), __dmul_rn(u[1], v[1])), __dmul_rn(u[2], v[2]));
+  };
+  const double den = __dadd_rn(__dadd_rn(__dadd_rn(1.0, dot(a, b)), dot(b, c)), dot(c, a));
+  return 2.0 * atan2(num, den);
+}
+
+__global__ void __launch_bounds__(256) topological_charge_kernel(const float* __restrict__ spins,
+                                                                 const int8_t* __restrict__ mask, Geometry g, int z,
+                                                                 double* __restrict__ Q) {
+  const int rep = blockIdx.x;
+  const int nx = g.L1 - 1, ny = g.L2 - 1;
+  const float* base = spins + (size_t)rep * 3 * g.nsite + (size_t)z * g.L2 * g.L1;   // sublattice 0, layer z
+  const int8_t* mz = mask != nullptr ? mask + (size_t)z * g.L2 * g.L1 : nullptr;
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < nx * ny; i += blockDim.x) {
+    const int y = i / nx, x = i - y * nx;
+    const int o00 = y * g.L1 + x, o10 = o00 + 1, o01 = o00 + g.L1, o11 = o01 + 1;
+    if (mz != nullptr && !(mz[o00] && mz[o10] && mz[o01] && mz[o11])) continue;
+    double s00[3], s10[3], s01[3], s11[3];
+    for (int k = 0; k < 3; ++k) {
+      const float* c = base + (size_t)k * g.nsite;
+      s00[k] = c[o00];
+      s10[k] = c[o10];
+      s01[k] = c[o01];
+      s11[k] = c[o11];
+    }
+    acc += solid_angle(s00, s10, s11) + solid_angle(s00, s11, s01);
+  }
+  __shared__ double part[256];
+  part[threadIdx.x] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double sum = 0.0;
+    for (int i = 0; i < (int)blockDim.x; ++i) sum += part[i];
+    Q[rep] = sum / (4.0 * 3.14159265358979323846);
+  }
+}
+
+int launch_topological_charge(const sck_plan* plan, const float* spins, const int8_t* mask, int batch, int z,
+                              double* Q, cudaStream_t s) {
+  topological_charge_kernel<<<batch, 256, 0, s>>>(spins, plan->geom.has_mask ? mask : nullptr, plan->geom, z, Q);
+  return cuda_status(cudaGetLastError(), "topological charge");
+}
+
 int launch_observables(const sck_plan* plan, const void* spins, int storage, int batch, const int8_t* mask,
                        const float* k1, double* E, double* M, void* workspace, cudaStream_t s) {
   ObsParams p;

@@ -421,6 +421,20 @@ class Sampler:
                 self._plan, ctypes.byref(buf), _ptr(S), storage, B, float(s.n_active), _ptr(E_ref), _ptr(E),
                 _ptr(M), _ptr(acc), _ptr(accv), _ptr(self._workspace(B)), self._stream()))
 
+    def topological_charge(self, S: torch.Tensor, layer: int, Q: torch.Tensor | None = None) -> torch.Tensor:
+        """Berg-Luscher charge (B,) float64 of z-layer `layer` of sublattice 0 (anneal.py:69-80). Graph-safe
+        with a preallocated Q."""
+        s = self.sys
+        if S.dtype != torch.float32 or tuple(S.shape) != (self.B, s.n) + s.shape or not S.is_contiguous():
+            raise ValueError(f"spins must be contiguous float32 ({self.B}, {s.n}) + {s.shape}")
+        if Q is None:
+            Q = torch.empty(self.B, dtype=torch.float64, device=self.device)
+        buf = self._buffers(S)
+        with torch.cuda.device(self.device):
+            L.check(L.lib().sck_topological_charge(self._plan, ctypes.byref(buf), _ptr(S), self.B, int(layer),
+                                                   _ptr(Q), self._stream()))
+        return Q
+
     def energy(self, S: torch.Tensor) -> torch.Tensor:
         """Total energy per replica, float64."""
         return self.observables(S)[0]

@@ -40,7 +40,7 @@ def main(argv=None):
 
     import cases as C
 
-    names = a.cases or list(C.CASES) + ["philox", "quickstart", "tables", "simulate", "runs"]
+    names = a.cases or list(C.CASES) + ["philox", "quickstart", "tables", "simulate", "runs", "anneal"]
     for name in names:
         t0 = time.time()
         if name == "philox":
@@ -53,6 +53,8 @@ def main(argv=None):
             _simulate(np, a.ref)
         elif name == "runs":
             _runs(np, sy)
+        elif name == "anneal":
+            _anneal(np, torch, sy, Sampler)
         else:
             case = C.CASES[name]
             s = case["build"](sy, cr)
@@ -209,6 +211,36 @@ def _runs(np, sy):
         z = np.load(Path(d) / "state_001_p01.npz")
         out["run_state_keys"] = np.array(sorted(z.files))
     np.savez_compressed(HERE / "runs.npz", **out)
+
+
+def _anneal(np, torch, sy, Sampler):
+    """The reference's nanodisk observer (E, mean magnetization vector, middle-layer charge; anneal.py:83-146)
+    on states after a few low-temperature sweeps, its reducer on a fixed accumulator array, and its helpers."""
+    from Spin_Colour_Kernel import anneal as AN
+    out = {}
+    for i, (params, Rd, L, angle, shells) in enumerate(
+            [((0.0, 0.0, 0.0, 0.177, 0.139, 0.483, 0.88), 3.3, 3, 90.0, (1,)),
+             ((0.2, 0.0, 0.0, 0.1, 0.2, 0.3, 1.2), 4.2, 3, 30.0, (1, 2))]):
+        s = AN.build_state(params, Rd, L, angle, shells)
+        A = Sampler(s, 3, "cpu", 7)
+        A.set_temperature(0.05)
+        S = A.init_spins(seed=5)
+        A.sweep(S, 6)
+        E, Mv, Q = AN.Observer(A)(S)
+        out[f"state{i}_S"] = S.numpy().copy()
+        out[f"state{i}_E"], out[f"state{i}_Mv"], out[f"state{i}_Q"] = E.numpy(), Mv.numpy(), Q.numpy()
+        out[f"state{i}_k1"] = s.cubic_k1
+        out[f"state{i}_bonds"] = np.stack([s.bond_matrix(k) for k in range(len(s.crystal.bonds))])
+    rng = np.random.default_rng(3)
+    obs = rng.normal(size=(4, 8, 5))
+    obs[:, 1] = obs[:, 0] ** 2 + rng.random((4, 5))
+    obs[:, 3] = obs[:, 2] ** 2 + rng.random((4, 5))
+    temps = np.array([40.0, 30.0, 20.0, 10.0])
+    out["reduce_obs"], out["reduce_T"] = obs, temps
+    for k, v in AN.reduce_obs(obs, temps, 221).items():
+        out[f"reduce_{k}_out"] = v
+    out["shells"] = np.asarray(AN.active_shells([[0.0, 0.1, 0.0, 1, 1, 1, 1], [0.0, 0.0, 0.2, 1, 1, 1, 1]]))
+    np.savez_compressed(HERE / "anneal.npz", **out)
 
 
 if __name__ == "__main__":
