@@ -40,7 +40,7 @@ def main(argv=None):
 
     import cases as C
 
-    names = a.cases or list(C.CASES) + ["philox", "quickstart", "tables", "simulate", "runs", "anneal"]
+    names = a.cases or list(C.CASES) + ["philox", "quickstart", "tables", "simulate", "runs", "anneal", "critical"]
     for name in names:
         t0 = time.time()
         if name == "philox":
@@ -55,6 +55,8 @@ def main(argv=None):
             _runs(np, sy)
         elif name == "anneal":
             _anneal(np, torch, sy, Sampler)
+        elif name == "critical":
+            _critical(np, sy)
         else:
             case = C.CASES[name]
             s = case["build"](sy, cr)
@@ -241,6 +243,34 @@ def _anneal(np, torch, sy, Sampler):
         out[f"reduce_{k}_out"] = v
     out["shells"] = np.asarray(AN.active_shells([[0.0, 0.1, 0.0, 1, 1, 1, 1], [0.0, 0.0, 0.2, 1, 1, 1, 1]]))
     np.savez_compressed(HERE / "anneal.npz", **out)
+
+
+def _critical(np, sy):
+    """The reference's E4 numerics (exp_perf.py:728-822): the series of plain chains on its CPU path (an Ising
+    size, bit-exact everywhere), multi-histogram reweighting, Binder curves and their crossing."""
+    from Spin_Colour_Kernel import exp_perf as EP
+    out = {}
+    s = sy.ising("square", 8)
+    temps = np.array([2.1, 2.269, 2.45])
+    E, m2, m4 = EP._series(s, 8, temps, 3, 20, 12, 2, "cpu")
+    out["series_E"], out["series_m2"], out["series_m4"] = E, m2, m4
+    rng = np.random.default_rng(11)
+    T = np.array([1.9, 2.0, 2.1, 2.2, 2.3])
+    Es = np.stack([rng.normal(-200 + 40 * t, 8.0, 400) for t in T])          # overlapping energy histograms
+    o1 = np.tanh(-Es / 100.0) ** 2
+    o2 = o1 ** 2
+    grid = np.linspace(1.95, 2.25, 7)
+    (a1, a2), lnZ = EP.multi_histogram(Es, [o1, o2], T, grid, return_lnZ=True)
+    wts = rng.integers(0, 3, size=Es.shape).astype(np.float64)
+    (b1,) = EP.multi_histogram(Es, [o1], T, grid, weights=wts)
+    U, lnZb = EP._binder_curve(Es, o1, o2, T, grid)
+    out.update(mh_E=Es, mh_o1=o1, mh_o2=o2, mh_T=T, mh_grid=grid, mh_a1=a1, mh_a2=a2, mh_lnZ=lnZ, mh_w=wts,
+               mh_b1=b1, binder_U=U, binder_lnZ=lnZb)
+    x = np.linspace(0.0, 1.0, 9)
+    out["cross"] = np.array([EP._crossing(x, np.sin(3 * x), np.cos(3 * x) * 0.5), EP._crossing(x, x, x + 1.0)])
+    out["temps_e4"] = EP.e4_temperatures(4.5115, 30.0, 9, 0.05)
+    out["temps_e4_cap"] = EP.e4_temperatures(4.5115, 300.0, 9, 0.01)
+    np.savez_compressed(HERE / "critical.npz", **out)
 
 
 if __name__ == "__main__":
