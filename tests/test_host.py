@@ -222,3 +222,34 @@ def test_temperature_ladder_and_runner_fixture():
         assert np.all(g[f"{key}_E2"] >= g[f"{key}_E"] ** 2 - 1e-9)        # a variance is not negative
         assert np.all(np.isin(g[f"{key}_configs"][..., 0], (-1.0, 1.0)))
         assert g[f"{key}_configs"].shape[2] == sites
+
+
+def test_measure_step_and_charge_entry_points_refuse_bad_arguments_before_any_launch():
+    """sck_observables_accumulate and sck_topological_charge check their arguments on the host: no device is
+    touched for these refusals."""
+    lib = L.lib()
+
+    def plan_of(s, B):
+        h = ctypes.c_void_p()
+        L.check(lib.sck_plan_create(ctypes.byref(P.describe(s)), B, L.MODE_F32, ctypes.byref(h)))
+        return h
+
+    heis, xy = plan_of(sy.heisenberg("sc", 4), 3), plan_of(sy.xy("square", 8), 3)
+    try:
+        buf = L.Buffers(1, 0, 0, 1, 0, 1)
+        Q = ctypes.c_void_p(1)
+        assert lib.sck_topological_charge(xy, ctypes.byref(buf), Q, 3, 0, Q, None) == L.ERR_INVALID
+        assert "Heisenberg" in lib.sck_last_error().decode()
+        assert lib.sck_topological_charge(heis, ctypes.byref(buf), Q, 3, 4, Q, None) == L.ERR_INVALID
+        assert "layer" in lib.sck_last_error().decode()
+        assert lib.sck_topological_charge(heis, ctypes.byref(buf), Q, 4, 0, Q, None) == L.ERR_INVALID
+        assert lib.sck_topological_charge(heis, ctypes.byref(buf), None, 3, 0, Q, None) == L.ERR_INVALID
+        p = ctypes.c_void_p(1)
+        assert lib.sck_observables_accumulate(heis, ctypes.byref(buf), p, L.MODE_F32, 3, 64.0, None, p, p, p, p, p,
+                                              None) == L.ERR_INVALID
+        assert lib.sck_observables_accumulate(heis, ctypes.byref(buf), p, L.MODE_F32, 3, 0.0, p, p, p, p, p, p,
+                                              None) == L.ERR_INVALID
+        assert "n_active" in lib.sck_last_error().decode()
+    finally:
+        lib.sck_plan_destroy(heis)
+        lib.sck_plan_destroy(xy)
