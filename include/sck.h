@@ -12,7 +12,9 @@
  *   - Device buffers are caller-owned and updated in place. `state` = {base_seed, sweep} (int64) lives on the
  *     device; a sweep advances state[1] on the device, so a captured CUDA graph keeps the random stream.
  *   - Every call is asynchronous on the given stream (a cudaStream_t passed as void*, NULL = default stream),
- *     allocates nothing, synchronises nothing, and may be captured into a CUDA graph.
+ *     allocates nothing, synchronises nothing, and may be captured into a CUDA graph (the set-up calls excepted:
+ *     sck_plan_tune allocates the group pipeline's counters when it enables the pipeline; the counter queries
+ *     such as sck_wait_timeouts synchronise).
  *   - Every function returns 0 (SCK_OK) or a negative SCK_ERR_* code; sck_last_error() explains the last
  *     failure of the calling thread. Kernels never trap.
  *   - Layout: S[B, n, b, L3, L2, L1] (x fastest; L3 = 1 in 2D) in the plan's storage type; packed and bitwise
