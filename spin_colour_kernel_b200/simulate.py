@@ -180,8 +180,7 @@ def _validate_shape(shape: str, coords: tuple) -> None:
         if not isinstance(node, _ALLOWED):
             raise ValueError(f"the shape {shape!r} may hold only numbers, coordinates, operators and {funcs}; "
                              f"found {type(node).__name__}")
-        if isinstance(node, ast.Constant) and (isinstance(node.value, bool) or
-                                               not isinstance(node.value, (int, float))):
+        if isinstance(node, ast.Constant) and not isinstance(node.value, (int, float)):
             raise ValueError(f"the shape {shape!r} may hold only numbers as constants")
         if isinstance(node, ast.Call):
             if not (isinstance(node.func, ast.Name) and node.func.id in _FUNCS) or node.keywords:

@@ -94,10 +94,15 @@ def test_replica_blocks_sizes_and_estimate():
 
 @pytest.mark.parametrize("shape", ["().__class__.__bases__[0].__subclasses__()", "__import__('os').system('true')",
                                    "(lambda: 1)()", "x.real <= 2", "'a' < 'b'", "open('f')", "abs(x, key=1) < 2",
-                                   "(x < 1) and (y < 1)", "True", "q < 1"])
+                                   "(x < 1) and (y < 1)", "q < 1"])
 def test_a_shape_that_is_not_a_condition_on_the_coordinates_is_refused(shape):
     with pytest.raises(ValueError):
         SIM.active_sites("sc", [4, 4, 4], "cartesian", shape)
+
+
+def test_a_constant_shape_keeps_every_site_as_the_reference_does():
+    _, mask = SIM.active_sites("sc", [4, 4, 4], "cartesian", "True")
+    assert mask.all()
 
 
 def test_shape_refusals_name_what_to_use():
