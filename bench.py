@@ -54,20 +54,23 @@ def heisenberg_bcc(L=64):
                      cubic_k1=np.full((2, L, L, L), 0.05, np.float32))
 
 
-def make_workload(name, rank, device, L=64, replicas=1536):
+def make_workload(name, rank, device, L=64, replicas=1536, layout="quad"):
     from spin_colour_kernel_b200 import system as sy
     from spin_colour_kernel_b200.sampler import Sampler
     g = torch.Generator(device=device).manual_seed(2 + rank)
     if name == "heisenberg-bcc":
         s = heisenberg_bcc(L)
         B = replicas
-        A = Sampler(s, B, device=device, seed=1234 + 100000 * rank)
+        A = Sampler(s, B, device=device, seed=1234 + 100000 * rank, layout=layout)
         T = torch.linspace(0.5, 2.5, 24).repeat_interleave(-(-B // 24))[:B]
         S = torch.randn((B, 3) + s.shape, device=device, generator=g)
         S = (S / S.norm(dim=1, keepdim=True)).contiguous()
+        if A.quad:
+            S = A.pack(S)
         gb = B * 3 * s.nsite * 4 / 1e9
         cfg = {"workload": f"heisenberg-bcc-{L}^3x2-J1J2-K1-hz", "replicas": B, "sites": s.nsite,
                "temperatures": f"24 linear in [0.5, 2.5], {-(-B // 24)} replicas each", "spin_dtype": "float32",
+               "layout": layout,
                "l2": f"no flush: {gb:.2f} GB state > 126 MB L2"}
     elif name == "ising-sc-bitwise":
         s = sy.ising("sc", 128)
@@ -186,23 +189,20 @@ def cpu_baseline(name, budget_s=15.0):
 
 
 def reference_arm(args, rank, world):
+    """The reference's CPU arithmetic for this path on the host cores: the oracle's C port (the reference itself is
+    Python generating Triton kernels and cannot travel to the GPU box), W untimed and K timed repetitions of
+    one sweep of one replica per host thread over the full lattice; the same steady-state rate as the
+    `cpu_baseline` leg of the default arm."""
     if rank != 0:
         return
-    name = args.workload
     s = heisenberg_bcc(64)
     T = torch.linspace(0.5, 2.5, 24).repeat_interleave(64).numpy()
     from oracle import native
-    rates = []
     if native.available():
-        for k in range(args.warmup + args.steps):
-            r = native.time_heisenberg(s, T, budget_s=0.0, sweeps=1, replicas=native.threads())
-            if k >= args.warmup:
-                rates.append(r["value"])
-        base = r
+        base = native.time_heisenberg(s, T, warmup=max(1, args.warmup), reps=max(1, args.steps))
     else:
-        base = cpu_baseline(name)
-        rates = [base["value"]]
-    v = float(np.median(rates))
+        base = cpu_baseline(args.workload)
+    v = base["value"]
     cfg = {"workload": "heisenberg-bcc-64^3x2-J1J2-K1-hz", "replicas": 1536, "sites": s.nsite}
     line = {"impl": "reference", "metric": "spin-update attempts/ns", "value": v, "unit": "attempts/ns",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
@@ -381,6 +381,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--L", type=int, default=64, help="heisenberg-bcc cells per axis (profiling runs use less)")
     ap.add_argument("--replicas", type=int, default=1536, help="heisenberg-bcc replicas")
+    ap.add_argument("--layout", default="quad", choices=["quad", "reference"],
+                    help="heisenberg-bcc resident storage: interleaved quads (default) or the reference layout")
     ap.add_argument("--path", default="auto",
                     choices=["auto", "autotune", "tile", "segment", "row", "lattice", "generic"],
                     help="sweep path: plan default, autotuned, tile kernels, segment kernels ('row' is an alias), "
@@ -417,9 +419,11 @@ def main():
             tdist.barrier()
             tdist.destroy_process_group()
         return
-    s, A, S, T, cfg = make_workload(args.workload, rank, device, args.L, args.replicas)
+    s, A, S, T, cfg = make_workload(args.workload, rank, device, args.L, args.replicas, args.layout)
     budget = int((args.l2_mb or 0) * (1 << 20))
-    if args.path in ("tile", "segment", "row", "lattice", "generic"):
+    if A.quad:
+        pass                               # one kernel family: the interleaved class kernels
+    elif args.path in ("tile", "segment", "row", "lattice", "generic"):
         A.tune({"tile": 3, "segment": 2, "row": 2, "lattice": 1, "generic": 0}[args.path], budget, RESIDENT_LIMIT)
     elif args.path == "autotune":
         from spin_colour_kernel_b200.autotune import autotune
@@ -501,7 +505,7 @@ def main():
     mean_launch_ms = ms / launches
     achieved = bytes_per_launch / (mean_launch_ms * 1e-3) / 1e9
     peak, peak_kind = hbm_peak()
-    traffic = traffic_per_launch(f"{args.workload}")
+    traffic = traffic_per_launch(f"{args.workload}" + ("-quad" if A.quad else ""))
     line = {
         "metric": "spin-update attempts/ns", "value": value, "unit": "attempts/ns", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -510,7 +514,7 @@ def main():
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "note": f"algorithmic {bpa} B/attempt; peak {peak_kind}; kernel = "
-                             f"{['generic', 'lattice', 'segment', 'tile'][path['specialised'] // 100]} class update, "
+                             f"{['generic', 'lattice', 'segment', 'tile', 'interleaved'][path['specialised'] // 100]} class update, "
                              f"{launches_per_sweep} launches per sweep (L2 group {path['group']}), "
                              f"step times from CUDA events"},
         "e2e": {"value": e2e, "unit": "attempts/ns", "h2d_bytes_per_step": int(beta_h.numel() * 4),

@@ -19,6 +19,12 @@
  *     failure of the calling thread. Kernels never trap.
  *   - Layout: S[B, n, b, L3, L2, L1] (x fastest; L3 = 1 in 2D) in the plan's storage type; packed and bitwise
  *     storage hold W = ceil(B / 32) int32 words per site, bit j of word w = replica 32 w + j (1 = spin +1).
+ *   - Interleaved storage (SCK_MODE_QUAD, vector models) holds Q = ceil(B / 4) quads of n * sites float4
+ *     elements; lane j of an element is replica 4 q + j (lanes past B are padding: swept, never observed). Within
+ *     a quad, element (((alpha L3 + z) L2 + y) n + k) L1 + (x mod P) (L1 / P) + x / P holds component k of site
+ *     (alpha, z, y, x), P being the colouring's x-period (1 or 2): the rows of one class are contiguous. It is
+ *     the sampler's resident state, converted from and to S by sck_quad_pack / sck_quad_unpack, as the
+ *     reference converts its packed Ising words (Sampler.pack / unpack). Spins and beta must be 16-byte aligned.
  */
 #ifndef SCK_H
 #define SCK_H
@@ -45,6 +51,7 @@ extern "C" {
 #define SCK_MODE_PACKED 2         /* Ising, 32 replicas per int32 word, per-replica Philox == SCK_MODE_INT8 */
 #define SCK_MODE_BITWISE 3        /* Ising multi-spin coding, one uniform per (word, site, sweep) */
 #define SCK_MODE_BITWISE_INDEP 4  /* Ising multi-spin coding, one 32-bit draw per (replica, site, sweep) */
+#define SCK_MODE_QUAD 5           /* XY / Heisenberg, float32 components of four replicas interleaved (below) */
 
 #define SCK_METROPOLIS 0
 #define SCK_BARKER 1
@@ -173,8 +180,9 @@ int sck_sync_sweep(const sck_plan* plan, const sck_buffers* buf, void* scratch, 
  * systems and checks only. */
 int sck_reference_sweep(const sck_plan* plan, const sck_buffers* buf, int32_t n_sweeps, void* stream);
 
-/* FP64 observables (Sampler.energy / magnetization, sampler.py:296-345) of `batch` replicas stored as
- * `storage` (SCK_MODE_INT8: int8 spins, SCK_MODE_F32: float32 components, SCK_MODE_PACKED: int32 words):
+/* FP64 observables (Sampler.energy / magnetization, sampler.py:296-345) of the first `batch` replicas (1 .. the
+ * plan's batch) stored as `storage` (SCK_MODE_INT8: int8 spins, SCK_MODE_F32: float32 components,
+ * SCK_MODE_PACKED: int32 words, SCK_MODE_QUAD: interleaved quads of a SCK_MODE_QUAD plan):
  *   E[r]            = -1/2 sum_i s_i . v_i - sum_i h . s_i + sum_i a(s_i)   (r < batch)
  *   M[r][alpha][k]  = sum over sublattice alpha of s_k                       (batch x b x n doubles)
  * `workspace` holds per-block partial sums; its size in bytes comes from sck_observables_workspace_size.
@@ -207,8 +215,9 @@ int sck_topological_charge(const sck_plan* plan, const sck_buffers* buf, const f
  * that cannot afford the synchronisation an allocation may bring, an FFI binding that cannot own a device
  * buffer). The partial sums go to a fixed 2 MiB array compiled into the library, which every GPU that loads the
  * library keeps until the process exits; a request needing more (batch x blocks per replica x 16 doubles) fails
- * with SCK_ERR_INVALID — use sck_observables then. The entry point allocates nothing. Its first call on a device
- * looks up the array's device address (make that first call before any stream capture). Every call shares the
+ * with SCK_ERR_INVALID — use sck_observables then. The entry point allocates nothing. Every call looks up the
+ * array's device address in the current context; the first call on a device may load the library's kernels into
+ * that context, so make that first call before any stream capture. Every call shares the
  * one array and leaves its partial sums there; no part needs clearing, since each slot the final sum reads is
  * written earlier in the same call, but calls that overlap on the GPU (other streams, other threads) race on it:
  * keep them ordered. */
@@ -222,6 +231,17 @@ int sck_observables_noalloc(const sck_plan* plan, const sck_buffers* buf, const 
  * GEMM tile whose products timed out leaves its output unwritten, and each adds one here. Reads the count from the current
  * device (synchronising it). No counterpart in the reference. */
 int sck_wait_timeouts(int64_t* count);
+
+/* Interleaved storage (SCK_MODE_QUAD plans): pack float32 S[B, n, b, L3, L2, L1] into quads (padding lanes 0),
+ * unpack quads into S (padding lanes dropped). No counterpart in the reference, whose vector models keep S; the
+ * analogue of its packed-word conversion (Sampler.pack / unpack, sampler.py:169-188). The plan accepts a
+ * vector-model system with a compile-time lattice table (square, triangular, sc, bcc, bcc J1-J2, fcc; no extra
+ * bond matrices), every axis periodic, no mask and a colouring of x-period 1 or 2 dividing L1; otherwise
+ * sck_plan_create returns SCK_ERR_UNSUPPORTED. sck_sweep, sck_class_update (src = spins), sck_observables*
+ * (storage SCK_MODE_QUAD) read the quads directly; the synchronous control, the sequential reference and the
+ * topological charge take S (unpack first). */
+int sck_quad_pack(const sck_plan* plan, const float* spins, void* quads, void* stream);
+int sck_quad_unpack(const sck_plan* plan, const void* quads, float* spins, void* stream);
 
 /* Storage conversion (Sampler.pack / unpack, sampler.py:169-188). pack: int8 spins [B, 1, b, L3, L2, L1]
  * (+-1, 0 masked) -> int32 words [W, 1, b, L3, L2, L1] (padding replicas 0). unpack: words -> int8 spins,

@@ -4,10 +4,14 @@
  *
  * Same arithmetic as the reference's generated class kernel (Spin_Colour_Kernel/generator.py:150-319) in
  * float32 with no FMA contraction (built with -ffp-contract=off): local field by coupling groups, extra
- * matrices and field; Philox4x32-10 proposals keyed per sweep; cubic anisotropy; Metropolis or Barker. cos,
- * sin, exp and sqrt come from the C library, so vector-model trajectories agree with the NumPy oracle within
- * float32 rounding, not bit for bit. Replicas run in parallel over OpenMP threads; each replica's sites are
- * visited class by class, which equals the parallel class update because no bond joins two sites of a class.
+ * matrices and field; Philox4x32-10 proposals keyed per sweep; cubic anisotropy; Metropolis or Barker. The
+ * reference's CPU path evaluates exp with NumPy's float32 exp, which differs from the C library's expf in the
+ * last bits for a large share of arguments; Ising energy changes form a finite set, so for Ising the caller
+ * passes, per replica, the sorted arguments the chain can reach with NumPy's exp of each, and the port looks
+ * the exact argument up (bit-exact Ising chains). Vector models take cos, sin, exp and sqrt from the C library
+ * and agree with the NumPy oracle within float32 rounding, not bit for bit. Replicas run in parallel over
+ * OpenMP threads; each replica's sites are visited class by class, which equals the parallel class update
+ * because no bond joins two sites of a class.
  */
 #include <math.h>
 #include <omp.h>
@@ -76,8 +80,29 @@ static inline int axis(int x, int dx, int L, int per) {
   return (q >= 0 && q < L) ? q : -1;
 }
 
+/* exp of an Ising argument from the caller's table: xs[0..n) sorted ascending, es the matching values; sets *miss
+ * when the argument is absent (the caller's enumeration did not cover it). */
+typedef struct {
+  const float* xs;
+  const float* es;
+  int64_t n;
+} or_exp_table;
+
+static float table_exp(const or_exp_table* t, float x, int* miss) {
+  int64_t lo = 0, hi = t->n - 1;
+  while (lo <= hi) {
+    const int64_t mid = (lo + hi) / 2;
+    const float v = t->xs[mid];
+    if (v == x) return t->es[mid];
+    if (v < x) lo = mid + 1; else hi = mid - 1;
+  }
+  *miss = 1;
+  return expf(x);
+}
+
 static void site_update(const or_desc* d, float* S, const float* k1, const int8_t* mask, int64_t rep, float beta,
-                        int alpha, int x, int y, int z, uint32_t k0, uint32_t k1w) {
+                        int alpha, int x, int y, int z, uint32_t k0, uint32_t k1w, const or_exp_table* et,
+                        int* miss) {
   const int n = d->n, L1 = d->L[0], L2 = d->L[1], L3 = d->L[2];
   const int plane = L1 * L2 * L3, nsite = d->b * plane;
   const int own = alpha * plane + (z * L2 + y) * L1 + x;
@@ -149,23 +174,37 @@ static void site_update(const or_desc* d, float* S, const float* k1, const int8_
     dE = dE + (at - as);
   }
   int acc;
-  if (d->acceptance == 1)
-    acc = u0 * (1.0f + expf(beta * dE)) < 1.0f;
-  else
-    acc = u0 < expf(-beta * dE);
+  if (d->acceptance == 1) {
+    const float xa = beta * dE;
+    acc = u0 * (1.0f + (et ? table_exp(et, xa, miss) : expf(xa))) < 1.0f;
+  } else {
+    const float xa = -beta * dE;
+    acc = u0 < (et ? table_exp(et, xa, miss) : expf(xa));
+  }
   if (acc)
     for (int k = 0; k < n; ++k) R[(size_t)k * nsite + own] = t[k];
 }
 
-/* n_sweeps sweeps of B replicas, S = [B][n][b][L3][L2][L1] float32; reps[i] = global replica index of row i. */
+/* n_sweeps sweeps of B replicas, S = [B][n][b][L3][L2][L1] float32; reps[i] = global replica index of row i.
+ * Ising exp tables (may be NULL): replica row i's arguments are exp_x[exp_off[i] .. exp_off[i + 1]), sorted, with
+ * NumPy's exp of each in exp_e. Returns 0, or 1 when an argument was missing from a table. */
 int oracle_sweep(const or_desc* d, float* S, const float* beta, const float* k1, const int8_t* mask, int B,
-                 const int64_t* reps, int64_t base_seed, int64_t sweep0, int n_sweeps, int threads) {
+                 const int64_t* reps, int64_t base_seed, int64_t sweep0, int n_sweeps, int threads,
+                 const float* exp_x, const float* exp_e, const int64_t* exp_off) {
   const int L1 = d->L[0], L2 = d->L[1], L3 = d->L[2];
   const size_t nsite = (size_t)d->b * L1 * L2 * L3;
+  int missed = 0;
   if (threads > 0) omp_set_num_threads(threads);
-#pragma omp parallel for schedule(dynamic, 1)
+#pragma omp parallel for schedule(dynamic, 1) reduction(| : missed)
   for (int i = 0; i < B; ++i) {
     float* R = S + (size_t)i * d->n * nsite;
+    or_exp_table et = {0, 0, 0};
+    if (exp_x) {
+      et.xs = exp_x + exp_off[i];
+      et.es = exp_e + exp_off[i];
+      et.n = exp_off[i + 1] - exp_off[i];
+    }
+    int miss = 0;
     for (int sw = 0; sw < n_sweeps; ++sw) {
       uint64_t v = (uint64_t)base_seed * 1000003ull + (uint64_t)(sweep0 + sw) * 7919ull + 12345ull;
       int32_t key = (int32_t)((int64_t)v % 2147483629ll);
@@ -176,11 +215,105 @@ int oracle_sweep(const or_desc* d, float* S, const float* beta, const float* k1,
           for (int y = 0; y < L2; ++y)
             for (int x = 0; x < L1; ++x)
               if (colour_of(d, alpha, x, y, z) == colour)
-                site_update(d, R, k1, mask, reps ? reps[i] : i, beta[i], alpha, x, y, z, k0, k1w);
+                site_update(d, R, k1, mask, reps ? reps[i] : i, beta[i], alpha, x, y, z, k0, k1w,
+                            exp_x ? &et : 0, &miss);
+      }
+    }
+    missed |= miss;
+  }
+  return missed;
+}
+
+int oracle_max_threads(void) { return omp_get_max_threads(); }
+
+/* ------------------------------------------------------------------------------------------- bitwise Ising
+ * The reference's multi-spin-coded chain (Spin_Colour_Kernel/bitwise.py:59-246, restated in oracle/bitwise.py)
+ * on unpacked int8 spins S[B][b][L3][L2][L1] (+-1, 0 on masked sites): word w holds replicas 32 w .. 32 w + 31;
+ * for a class site with z_eff present neighbours (inside the box and the mask, bonds of applied couplings) and
+ * k anti-aligned ones, replica r flips when its draw is below table[w][s][z_eff][k] (s = 1 for spin +1 when the
+ * system has a field, else 0).
+ *   shared:      one float32 uniform per (word, site, sweep): output w % 4 of Philox(int32((w / 4) nsite + site));
+ *   independent: one 32-bit integer U per (replica, site, sweep), bit 31 - l of replica 32 w + j's U = bit j of
+ *                R_l, R_{4g+q} = output q of Philox(int32(w nsite + site)) under key_g =
+ *                (key + (g + 1) 104729) mod 2147483629 (floored); flip iff U < P (int64 table).
+ * words[lw] = global word index of local word lw (its counters); table rows follow local words. Sites of one
+ * class run in parallel over OpenMP threads (no bond joins two sites of a class). */
+static int32_t sweep_key_of(int64_t base_seed, int64_t sweep) {
+  uint64_t v = (uint64_t)base_seed * 1000003ull + (uint64_t)sweep * 7919ull + 12345ull;
+  return (int32_t)((int64_t)v % 2147483629ll);
+}
+
+int oracle_bitwise_sweep(const or_desc* d, int8_t* S, const int8_t* mask, int B, const int64_t* words,
+                         const void* table, int Z1, int has_field, int independent, int64_t base_seed,
+                         int64_t sweep0, int n_sweeps, int threads) {
+  const int L1 = d->L[0], L2 = d->L[1], L3 = d->L[2];
+  const int plane = L1 * L2 * L3, nsite = d->b * plane;
+  const int W = (B + 31) / 32;
+  if (threads > 0) omp_set_num_threads(threads);
+  for (int sw = 0; sw < n_sweeps; ++sw) {
+    const int32_t key = sweep_key_of(base_seed, sweep0 + sw);
+    const uint32_t k0 = (uint32_t)key, k1 = key < 0 ? 0xFFFFFFFFu : 0u;
+    uint32_t kg[8];
+    for (int g = 0; g < 8; ++g) {
+      int64_t r = ((int64_t)key + (int64_t)(g + 1) * 104729) % 2147483629ll;
+      kg[g] = (uint32_t)(r < 0 ? r + 2147483629ll : r);
+    }
+    for (int ci = 0; ci < d->n_classes; ++ci) {
+      const int colour = d->classes[ci][0], a = d->classes[ci][1];
+#pragma omp parallel for schedule(static)
+      for (int rem = 0; rem < plane; ++rem) {
+        const int x = rem % L1, y = (rem / L1) % L2, z = rem / (L1 * L2);
+        const int site = a * plane + rem;
+        if (colour_of(d, a, x, y, z) != colour || (mask && !mask[site])) continue;
+        int q[OR_MAX_BONDS], nq = 0;
+        int bi = 0;
+        for (int g = 0; g < d->n_groups[a]; ++g) {
+          for (; bi < d->group_end[a][g]; ++bi) {
+            if (!d->apply[a][g]) continue;
+            const or_bond* bd = &d->bonds[a][bi];
+            const int qx = axis(x, bd->dx, L1, d->periodic[0]), qy = axis(y, bd->dy, L2, d->periodic[1]);
+            const int qz = axis(z, bd->dz, L3, d->periodic[2]);
+            if (qx < 0 || qy < 0 || qz < 0) continue;
+            const int qs = bd->a2 * plane + (qz * L2 + qy) * L1 + qx;
+            if (mask && !mask[qs]) continue;
+            q[nq++] = qs;
+          }
+        }
+        for (int lw = 0; lw < W; ++lw) {
+          const int64_t gw = words ? words[lw] : lw;
+          float u = 0.0f;
+          uint32_t R[32];
+          if (!independent) {
+            uint32_t out[4];
+            philox((uint32_t)((uint64_t)(gw / 4) * (uint64_t)nsite + (uint64_t)site), k0, k1, out);
+            u = uniform(out[gw % 4]);
+          } else {
+            for (int g = 0; g < 8; ++g)
+              philox((uint32_t)((uint64_t)gw * (uint64_t)nsite + (uint64_t)site), kg[g], 0u, &R[4 * g]);
+          }
+          for (int j = 0; j < 32; ++j) {
+            const int r = 32 * lw + j;
+            if (r >= B) break;
+            int8_t* Rr = S + (size_t)r * nsite;
+            const int s = Rr[site];
+            int tot = 0;
+            for (int i = 0; i < nq; ++i) tot += Rr[q[i]];
+            const int kk = (nq - s * tot) / 2;
+            const int sidx = has_field ? (s > 0) : 0;
+            const size_t ti = (((size_t)lw * 2 + sidx) * Z1 + nq) * Z1 + kk;
+            int flip;
+            if (!independent) {
+              flip = u < ((const float*)table)[ti];
+            } else {
+              uint64_t U = 0;
+              for (int l = 0; l < 32; ++l) U |= (uint64_t)((R[l] >> j) & 1u) << (31 - l);
+              flip = (int64_t)U < ((const int64_t*)table)[ti];
+            }
+            if (flip) Rr[site] = (int8_t)(-s);
+          }
+        }
       }
     }
   }
   return 0;
 }
-
-int oracle_max_threads(void) { return omp_get_max_threads(); }

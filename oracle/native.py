@@ -63,8 +63,13 @@ def _load():
             raise OSError("oracle C port not built")
         L = ctypes.CDLL(str(LIB))
         L.oracle_sweep.argtypes = [ctypes.POINTER(_Desc), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
-                                   ctypes.c_void_p, _i32, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, _i32, _i32]
+                                   ctypes.c_void_p, _i32, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, _i32, _i32,
+                                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.oracle_sweep.restype = _i32
+        L.oracle_bitwise_sweep.argtypes = [ctypes.POINTER(_Desc), ctypes.c_void_p, ctypes.c_void_p, _i32,
+                                           ctypes.c_void_p, ctypes.c_void_p, _i32, _i32, _i32, ctypes.c_int64,
+                                           ctypes.c_int64, _i32, _i32]
+        L.oracle_bitwise_sweep.restype = _i32
         L.oracle_max_threads.restype = _i32
         L.oracle_desc_size.restype = _i32
         if L.oracle_desc_size() != ctypes.sizeof(_Desc):
@@ -130,8 +135,55 @@ def describe(sys_) -> _Desc:
     return d
 
 
+def ising_exp_table(sys_, beta: np.ndarray):
+    """Every argument of exp an Ising chain of this system can reach, per replica, sorted, with NumPy's float32
+    exp of each: (xs, es, offsets). The local field is enumerated with the port's float32 operation order
+    (applied coupling groups, then extra bonds, then the field) over every neighbour sum a group can take
+    (masks and open boundaries included) and every value an extra bond's neighbour can take; the argument is
+    -beta dE (Metropolis) or beta dE (Barker) with dE = -((-s) - s) v."""
+    f32 = np.float32
+    vals = []
+    for a in range(sys_.b):
+        groups, extras = field_groups(sys_, a)
+        axes = []
+        coef = []
+        for J, members in groups.items():
+            if J == 0.0:
+                continue
+            z = len(members)
+            axes.append(np.arange(-z, z + 1, dtype=np.float32))
+            coef.append(("J", f32(J)))
+        for i in extras:
+            c = f32(np.asarray(sys_.extra[i], np.float64)[0, 0])
+            if c != 0.0:
+                axes.append(np.array([-1.0, 0.0, 1.0], np.float32))
+                coef.append(("E", c))
+        grids = np.meshgrid(*axes, indexing="ij") if axes else []
+        v = np.zeros(grids[0].shape if grids else (1,), np.float32)
+        for (kind, c), G in zip(coef, grids):
+            v = (v + (c * G).astype(np.float32)).astype(np.float32)
+        if sys_.h is not None and f32(sys_.h[0]) != 0.0:
+            v = (v + f32(sys_.h[0])).astype(np.float32)
+        vals.append(v.reshape(-1))
+    v = np.unique(np.concatenate(vals))
+    dEs = []
+    for s in (f32(-1.0), f32(1.0)):
+        acc_sum = ((-s - s) * v).astype(np.float32)
+        dEs.append((-acc_sum).astype(np.float32))
+    dE = np.unique(np.concatenate(dEs))
+    xs, es, off = [], [], [0]
+    barker = sys_.acceptance == "barker"
+    for b in np.asarray(beta, np.float32):
+        x = np.unique(((b if barker else -b) * dE).astype(np.float32))
+        xs.append(x)
+        es.append(np.exp(x).astype(np.float32))
+        off.append(off[-1] + x.size)
+    return np.concatenate(xs), np.concatenate(es), np.asarray(off, np.int64)
+
+
 def sweep(sys_, S: np.ndarray, beta: np.ndarray, state: list[int], n: int = 1, reps=None, nthreads: int = 0):
-    """n sweeps in place on float32 spins S (B, n, b, L3, L2, L1); state advances by n."""
+    """n sweeps in place on float32 spins S (B, n, b, L3, L2, L1); state advances by n. Ising chains read exp from
+    ising_exp_table (NumPy's values, as the reference's CPU path) and are bit-exact."""
     L = _load()
     S = np.ascontiguousarray(S, dtype=np.float32)
     B = S.shape[0]
@@ -140,35 +192,68 @@ def sweep(sys_, S: np.ndarray, beta: np.ndarray, state: list[int], n: int = 1, r
     mask = None if sys_.mask is None else np.ascontiguousarray(sys_.site_mask(), dtype=np.int8)
     r = None if reps is None else np.ascontiguousarray(reps, dtype=np.int64)
     d = describe(sys_)
-    L.oracle_sweep(ctypes.byref(d), S.ctypes.data, beta.ctypes.data, None if k1 is None else k1.ctypes.data,
-                   None if mask is None else mask.ctypes.data, B, None if r is None else r.ctypes.data,
-                   int(state[0]), int(state[1]), int(n), int(nthreads))
+    tab = ising_exp_table(sys_, beta) if sys_.n == 1 else None
+    rc = L.oracle_sweep(ctypes.byref(d), S.ctypes.data, beta.ctypes.data, None if k1 is None else k1.ctypes.data,
+                        None if mask is None else mask.ctypes.data, B, None if r is None else r.ctypes.data,
+                        int(state[0]), int(state[1]), int(n), int(nthreads),
+                        *((None, None, None) if tab is None else (t.ctypes.data for t in tab)))
+    if rc != 0:
+        raise RuntimeError("an Ising exp argument fell outside the enumerated table")
     state[1] += n
     return S
 
 
-def time_heisenberg(sys_, T: np.ndarray, budget_s: float = 15.0, sweeps: int = 1, replicas: int | None = None):
-    """Attempts/ns of the C port on all host threads: `replicas` replicas (default one per thread) of the full
-    lattice, `sweeps` sweeps, repeated until `budget_s` seconds have passed (at least once)."""
+def bitwise_sweep(sys_, spins: np.ndarray, table: np.ndarray, base_seed: int, sweep0: int, n: int = 1,
+                  independent: bool = False, words=None, nthreads: int = 0) -> np.ndarray:
+    """n sweeps of the bitwise chain on unpacked spins (B, b, L3, L2, L1) of +-1 (0 masked); `words` gives the
+    global word index of each block of 32 rows (default 0, 1, ...), `table` is indexed by local word: float32
+    p_table (shared) or int64 p_fixed (independent). Returns the new spins (int8)."""
+    from .bitwise import check
+    L = _load()
+    _, h, Z = check(sys_)
+    S = np.ascontiguousarray(spins, dtype=np.int8).copy()
+    B = S.shape[0]
+    tab = np.ascontiguousarray(table, dtype=np.int64 if independent else np.float32)
+    if tab.shape[-1] != Z + 1:
+        raise ValueError("table does not match the system's coordination")
+    mask = None if sys_.mask is None else np.ascontiguousarray(sys_.site_mask(), dtype=np.int8)
+    w = None if words is None else np.ascontiguousarray(words, dtype=np.int64)
+    d = describe(sys_)
+    L.oracle_bitwise_sweep(ctypes.byref(d), S.ctypes.data, None if mask is None else mask.ctypes.data, B,
+                           None if w is None else w.ctypes.data, tab.ctypes.data, Z + 1, int(h != 0.0),
+                           int(independent), int(base_seed), int(sweep0), int(n), int(nthreads))
+    return S
+
+
+def time_heisenberg(sys_, T: np.ndarray, budget_s: float = 15.0, sweeps: int = 1, replicas: int | None = None,
+                    warmup: int = 1, reps: int | None = None):
+    """Attempts/ns of the C port on all host threads, in steady state: `replicas` replicas (default one per
+    thread) of the full lattice, `sweeps` sweeps per repetition; `warmup` untimed repetitions (thread start-up,
+    first touch of the spins), then `reps` timed repetitions, or as many as fit `budget_s` seconds (at least one).
+    The CPU baseline and the reference arm of bench.py both report this rate."""
     nth = threads()
     R = replicas or nth
     g = np.random.default_rng(2)
     S = g.standard_normal((R, sys_.n) + sys_.shape).astype(np.float32)
     S /= np.linalg.norm(S, axis=1, keepdims=True)
-    reps = np.arange(R, dtype=np.int64) * (len(T) // R if len(T) >= R else 1)
-    beta = (np.float32(1.0) / np.asarray(T, np.float32)[reps % len(T)]).astype(np.float32)
+    rows = np.arange(R, dtype=np.int64) * (len(T) // R if len(T) >= R else 1)
+    beta = (np.float32(1.0) / np.asarray(T, np.float32)[rows % len(T)]).astype(np.float32)
     state = [1234, 0]
+    for _ in range(warmup):
+        sweep(sys_, S, beta, state, sweeps, reps=rows, nthreads=nth)
     t0 = time.perf_counter()
-    done = 0
+    done = n_rep = 0
     while True:
-        sweep(sys_, S, beta, state, sweeps, reps=reps, nthreads=nth)
+        sweep(sys_, S, beta, state, sweeps, reps=rows, nthreads=nth)
         done += R * sys_.n_active * sweeps
+        n_rep += 1
         el = time.perf_counter() - t0
-        if el >= budget_s:
+        if (reps is not None and n_rep >= reps) or (reps is None and el >= budget_s):
             break
     return {"value": done / (el * 1e9), "unit": "attempts/ns", "cores": nth, "kind": "port",
-            "sample": f"C port (oracle/cpu_sweep.c, OpenMP): {R} replicas x {sweeps} sweep(s) of the full "
-                      f"{sys_.nsite}-site lattice per repetition, {el:.1f} s"}
+            "sample": f"C port (oracle/cpu_sweep.c, OpenMP, {nth} threads): {R} replicas x {sweeps} sweep(s) of the "
+                      f"full {sys_.nsite}-site lattice per repetition, {warmup} untimed + {n_rep} timed "
+                      f"repetitions ({el:.1f} s)"}
 
 
 if __name__ == "__main__":

@@ -13,7 +13,7 @@ LIB_PATH = Path(__file__).resolve().parent / "libsckb200.so"
 
 ABI_VERSION = 1
 OK, ERR_INVALID, ERR_COUNTER, ERR_UNSUPPORTED, ERR_CUDA, ERR_TIMEOUT = 0, -1, -2, -3, -4, -5
-MODE_INT8, MODE_F32, MODE_PACKED, MODE_BITWISE, MODE_BITWISE_INDEP = 0, 1, 2, 3, 4
+MODE_INT8, MODE_F32, MODE_PACKED, MODE_BITWISE, MODE_BITWISE_INDEP, MODE_QUAD = 0, 1, 2, 3, 4, 5
 METROPOLIS, BARKER = 0, 1
 MAX_BASIS, MAX_BONDS, MAX_GROUPS, MAX_EXTRA, MAX_FACTORS, MAX_CLASSES = 4, 64, 8, 8, 4, 128
 
@@ -66,6 +66,8 @@ _SIGNATURES = {
     "sck_observables_noalloc": ([_vp, ctypes.POINTER(Buffers), _vp, _i32, _i32, _vp, _vp, _vp], _i32),
     "sck_wait_timeouts": ([ctypes.POINTER(_i64)], _i32),
     "sck_pack": ([_vp, _vp, _vp, _vp], _i32),
+    "sck_quad_pack": ([_vp, _vp, _vp, _vp], _i32),
+    "sck_quad_unpack": ([_vp, _vp, _vp, _vp], _i32),
     "sck_unpack": ([_vp, _vp, _vp, _vp, _vp], _i32),
     "sck_advance": ([_vp, _i32, _vp], _i32),
     "sck_batch_create": ([ctypes.POINTER(_vp), _i32, _i64, ctypes.POINTER(_vp)], _i32),

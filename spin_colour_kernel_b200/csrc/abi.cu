@@ -73,6 +73,8 @@ Common make_common_public(const sck_plan* plan, const sck_buffers* buf) { return
 
 static bool is_bitwise(int mode) { return mode == SCK_MODE_BITWISE || mode == SCK_MODE_BITWISE_INDEP; }
 
+static bool is_aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
 constexpr long long kResidentDefault = 200ll << 10;
 constexpr long long kResidentMax = 220ll << 10;
 
@@ -85,7 +87,7 @@ static bool use_resident(const sck_plan* p) {
 // Replicas per group of the L2 pipeline, or 0 when the sweep runs class by class over all replicas: the
 // specialised kernels only, a state larger than the budget, at least as many groups as classes.
 static int pipeline_group(const sck_plan* p) {
-  if (!p->spec || p->l2_budget <= 0) return 0;
+  if (!p->spec || p->l2_budget <= 0 || p->mode == SCK_MODE_QUAD) return 0;
   const int C = p->desc.n_classes;
   if (C < 2 || C > 8) return 0;
   const long long per_rep = (long long)p->geom.nsite * p->geom.n * (p->mode == SCK_MODE_INT8 ? 1 : 4);
@@ -107,6 +109,8 @@ static int check_buffers(const sck_plan* plan, const sck_buffers* buf, bool need
     return fail(SCK_ERR_INVALID, "this mode needs its acceptance table");
   if (!plan->ising_lut && !is_bitwise(plan->mode) && buf->beta == nullptr)
     return fail(SCK_ERR_INVALID, "null beta");
+  if (plan->mode == SCK_MODE_QUAD && !(is_aligned16(buf->spins) && is_aligned16(buf->beta)))
+    return fail(SCK_ERR_INVALID, "interleaved storage needs 16-byte aligned spins and beta");
   return SCK_OK;
 }
 
@@ -146,9 +150,11 @@ int sck_plan_create(const sck_system_desc* d, int32_t batch, int32_t mode, sck_p
   for (int r = 0; r < d->n_factors; ++r)
     if (d->m[r] < 1) return fail(SCK_ERR_INVALID, "colouring group orders must be positive");
   if (d->n_classes < 1 || d->n_classes > 128) return fail(SCK_ERR_INVALID, "class list out of range");
-  if (mode < SCK_MODE_INT8 || mode > SCK_MODE_BITWISE_INDEP) return fail(SCK_ERR_INVALID, "unknown mode");
-  if (mode != SCK_MODE_F32 && d->n != 1)
+  if (mode < SCK_MODE_INT8 || mode > SCK_MODE_QUAD) return fail(SCK_ERR_INVALID, "unknown mode");
+  if (mode != SCK_MODE_F32 && mode != SCK_MODE_QUAD && d->n != 1)
     return fail(SCK_ERR_UNSUPPORTED, "int8, packed and bitwise storage are for Ising (n = 1) only");
+  if (mode == SCK_MODE_QUAD && d->n == 1)
+    return fail(SCK_ERR_UNSUPPORTED, "interleaved storage is for vector models (n = 2 or 3)");
 
   sck_plan* p = new sck_plan();
   memset(p, 0, sizeof(*p));
@@ -192,8 +198,8 @@ int sck_plan_create(const sck_system_desc* d, int32_t batch, int32_t mode, sck_p
   }
   const bool packed = mode == SCK_MODE_PACKED || is_bitwise(mode);
   p->W = (batch + 31) / 32;
-  p->Bp = packed ? p->W * 32 : batch;
-  p->rows_storage = packed ? p->W : batch;
+  p->Bp = packed ? p->W * 32 : (mode == SCK_MODE_QUAD ? 4 * ((batch + 3) / 4) : batch);
+  p->rows_storage = packed ? p->W : (mode == SCK_MODE_QUAD ? p->Bp / 4 : batch);
   if ((long long)p->Bp * (long long)g.nsite >= 2147483647LL) {
     delete p;
     return fail(SCK_ERR_COUNTER, "replica batch too large for the int32 Philox counter");
@@ -340,6 +346,13 @@ int sck_plan_create(const sck_system_desc* d, int32_t batch, int32_t mode, sck_p
   p->NP = np < 1 ? 1 : np;
   p->field = (d->n == 1 && d->h64[0] != 0.0) ? 1 : 0;
   p->spec = find_spec(p);
+  if (mode == SCK_MODE_QUAD) {
+    std::string why;
+    if (!quad_ok(p, &why)) {
+      delete p;
+      return fail(SCK_ERR_UNSUPPORTED, why);
+    }
+  }
   p->kernel_kind = 1;
   p->l2_budget = 0;
   p->resident_limit = kResidentDefault;
@@ -351,7 +364,7 @@ int sck_plan_tune(sck_plan* plan, int32_t specialised, int64_t l2_budget_bytes, 
   if (plan == nullptr || l2_budget_bytes < 0 || resident_limit_bytes < 0)
     return fail(SCK_ERR_INVALID, "null plan or negative budget");
   if (resident_limit_bytes > kResidentMax) return fail(SCK_ERR_INVALID, "resident limit above 220 KiB of shared memory");
-  plan->spec = specialised ? find_spec(plan) : 0;
+  plan->spec = (specialised || plan->mode == SCK_MODE_QUAD) ? find_spec(plan) : 0;   // interleaved: always
   plan->kernel_kind = specialised >= 3 ? 3 : (specialised >= 2 ? 2 : 1);
   plan->l2_budget = l2_budget_bytes;
   plan->resident_limit = resident_limit_bytes;
@@ -382,7 +395,8 @@ int sck_plan_path(const sck_plan* plan, int32_t* specialised, int64_t* l2_budget
                   int32_t* resident) {
   if (plan == nullptr) return fail(SCK_ERR_INVALID, "null plan");
   if (specialised) {
-    const int kind = pipeline_group(plan) > 0 ? 1 : (tile_kernel_ok(plan) ? 3 : (seg_kernel_ok(plan) ? 2 : 1));
+    int kind = pipeline_group(plan) > 0 ? 1 : (tile_kernel_ok(plan) ? 3 : (seg_kernel_ok(plan) ? 2 : 1));
+    if (plan->mode == SCK_MODE_QUAD) kind = 4;
     *specialised = plan->spec ? kind * 100 + plan->spec : 0;
   }
   if (l2_budget_bytes) *l2_budget_bytes = plan->l2_budget;
@@ -424,6 +438,11 @@ int sck_plan_shape(const sck_plan* p, int32_t* computed, int32_t* rows) {
 
 static int class_launch(const sck_plan* plan, const sck_buffers* buf, const void* src, int colour, int alpha,
                         cudaStream_t s) {
+  if (plan->mode == SCK_MODE_QUAD) {
+    if (src != buf->spins || colour < 0)
+      return fail(SCK_ERR_UNSUPPORTED, "interleaved storage updates in place (src = spins, no synchronous control)");
+    return launch_quad_class(plan, buf, colour, alpha, s);
+  }
   Common c = make_common(plan, buf, src);
   if (is_bitwise(plan->mode)) return launch_bitwise_class(plan, c, colour, alpha, s);
   return launch_class(plan, c, colour, alpha, s);
@@ -444,6 +463,17 @@ int sck_sweep(const sck_plan* plan, const sck_buffers* buf, int32_t n_sweeps, vo
   if (n_sweeps < 0) return fail(SCK_ERR_INVALID, "negative sweep count");
   cudaStream_t s = (cudaStream_t)stream;
   if (n_sweeps == 0) return SCK_OK;
+  if (plan->mode == SCK_MODE_QUAD) {
+    for (int k = 0; k < n_sweeps; ++k) {
+      for (int i = 0; i < plan->desc.n_classes; ++i) {
+        rc = launch_quad_class(plan, buf, plan->desc.classes[i][0], plan->desc.classes[i][1], s);
+        if (rc != SCK_OK) return rc;
+      }
+      rc = launch_advance(buf->state, 1, s);
+      if (rc != SCK_OK) return rc;
+    }
+    return SCK_OK;
+  }
   if (use_resident(plan)) {
     const Common c = make_common(plan, buf, buf->spins);
     rc = launch_resident(plan, c, n_sweeps, s);
@@ -488,6 +518,8 @@ int sck_sync_sweep(const sck_plan* plan, const sck_buffers* buf, void* scratch, 
   int rc = check_buffers(plan, buf, true);
   if (rc != SCK_OK) return rc;
   if (scratch == nullptr) return fail(SCK_ERR_INVALID, "the synchronous control needs a scratch copy of the spins");
+  if (plan->mode == SCK_MODE_QUAD)
+    return fail(SCK_ERR_UNSUPPORTED, "the synchronous control reads S: unpack interleaved storage first");
   cudaStream_t s = (cudaStream_t)stream;
   size_t elem = plan->mode == SCK_MODE_INT8 ? 1 : 4;
   size_t bytes = (size_t)plan->rows_storage * (plan->mode == SCK_MODE_F32 ? plan->geom.n : 1) * plan->geom.nsite * elem;
@@ -511,6 +543,8 @@ int sck_sync_sweep(const sck_plan* plan, const sck_buffers* buf, void* scratch, 
 int sck_reference_sweep(const sck_plan* plan, const sck_buffers* buf, int32_t n_sweeps, void* stream) {
   int rc = check_buffers(plan, buf, true);
   if (rc != SCK_OK) return rc;
+  if (plan->mode == SCK_MODE_QUAD)
+    return fail(SCK_ERR_UNSUPPORTED, "the sequential reference reads S: unpack interleaved storage first");
   cudaStream_t s = (cudaStream_t)stream;
   for (int k = 0; k < n_sweeps; ++k) {
     Common c = make_common(plan, buf, buf->spins);
@@ -528,14 +562,37 @@ int sck_observables_workspace_size(const sck_plan* plan, int32_t batch, int64_t*
   return SCK_OK;
 }
 
+}  // extern "C"
+
+namespace sck {
+// The checks every observables entry point shares: a storage the plan can hold, and a batch within the plan's
+// (the spins buffer behind a plan holds at most that many replicas, so larger requests would read past it).
+int check_observables_request(const sck_plan* plan, int storage, int batch) {
+  if (batch < 1 || batch > plan->batch)
+    return fail(SCK_ERR_INVALID, "batch must be within 1 .. the plan's batch (" + std::to_string(plan->batch) + ")");
+  if (batch > 65535) return fail(SCK_ERR_INVALID, "observables: batch above 65535");
+  if (storage != SCK_MODE_INT8 && storage != SCK_MODE_F32 && storage != SCK_MODE_PACKED && storage != SCK_MODE_QUAD)
+    return fail(SCK_ERR_INVALID, "observables read int8, float32, packed or interleaved storage");
+  if (storage == SCK_MODE_QUAD && plan->mode != SCK_MODE_QUAD)
+    return fail(SCK_ERR_INVALID, "interleaved storage needs a plan of SCK_MODE_QUAD");
+  if (storage != SCK_MODE_F32 && storage != SCK_MODE_QUAD && plan->geom.n != 1)
+    return fail(SCK_ERR_INVALID, "vector models use float32 or interleaved storage");
+  if (storage == SCK_MODE_PACKED && plan->mode != SCK_MODE_PACKED && !is_bitwise(plan->mode))
+    return fail(SCK_ERR_INVALID, "packed storage needs a packed or bitwise plan");
+  return SCK_OK;
+}
+}  // namespace sck
+
+extern "C" {
+
 int sck_observables(const sck_plan* plan, const sck_buffers* buf, const void* spins, int32_t storage,
                     int32_t batch, double* E, double* M, void* workspace, void* stream) {
   if (plan == nullptr || buf == nullptr || spins == nullptr) return fail(SCK_ERR_INVALID, "null plan, buffers or spins");
   if (workspace == nullptr) return fail(SCK_ERR_INVALID, "null workspace (see sck_observables_workspace_size)");
-  if (batch < 1) return fail(SCK_ERR_INVALID, "batch must be positive");
-  if (storage != SCK_MODE_INT8 && storage != SCK_MODE_F32 && storage != SCK_MODE_PACKED)
-    return fail(SCK_ERR_INVALID, "observables read int8, float32 or packed storage");
-  if (storage != SCK_MODE_F32 && plan->geom.n != 1) return fail(SCK_ERR_INVALID, "vector models use float32 storage");
+  int rc = check_observables_request(plan, storage, batch);
+  if (rc != SCK_OK) return rc;
+  if (storage == SCK_MODE_QUAD && !is_aligned16(spins))
+    return fail(SCK_ERR_INVALID, "interleaved storage needs 16-byte aligned spins");
   if (plan->geom.has_mask && buf->mask == nullptr) return fail(SCK_ERR_INVALID, "the system has a mask: pass it");
   if (plan->geom.has_cubic && buf->k1 == nullptr) return fail(SCK_ERR_INVALID, "the system has cubic anisotropy: pass k1");
   return launch_observables(plan, spins, storage, batch, buf->mask, buf->k1, E, M, workspace, (cudaStream_t)stream);
@@ -564,6 +621,20 @@ int sck_topological_charge(const sck_plan* plan, const sck_buffers* buf, const f
   if (g.L1 < 2 || g.L2 < 2) return fail(SCK_ERR_INVALID, "a layer needs at least 2 x 2 sites");
   if (g.has_mask && buf->mask == nullptr) return fail(SCK_ERR_INVALID, "the system has a mask: pass it");
   return launch_topological_charge(plan, spins, buf->mask, batch, layer, Q, (cudaStream_t)stream);
+}
+
+int sck_quad_pack(const sck_plan* plan, const float* spins, void* quads, void* stream) {
+  if (plan == nullptr || spins == nullptr || quads == nullptr) return fail(SCK_ERR_INVALID, "null argument");
+  if (plan->mode != SCK_MODE_QUAD) return fail(SCK_ERR_UNSUPPORTED, "interleaved storage needs a plan of SCK_MODE_QUAD");
+  if (!is_aligned16(quads)) return fail(SCK_ERR_INVALID, "interleaved storage needs 16-byte alignment");
+  return launch_quad_convert(plan, (float*)spins, (float4*)quads, 0, (cudaStream_t)stream);
+}
+
+int sck_quad_unpack(const sck_plan* plan, const void* quads, float* spins, void* stream) {
+  if (plan == nullptr || spins == nullptr || quads == nullptr) return fail(SCK_ERR_INVALID, "null argument");
+  if (plan->mode != SCK_MODE_QUAD) return fail(SCK_ERR_UNSUPPORTED, "interleaved storage needs a plan of SCK_MODE_QUAD");
+  if (!is_aligned16(quads)) return fail(SCK_ERR_INVALID, "interleaved storage needs 16-byte alignment");
+  return launch_quad_convert(plan, spins, (float4*)quads, 1, (cudaStream_t)stream);
 }
 
 int sck_pack(const sck_plan* plan, const int8_t* spins, int32_t* words, void* stream) {

@@ -318,7 +318,7 @@ static bool matches(const sck_plan* p) {
 }
 
 int find_spec(const sck_plan* p) {
-  if (p->mode != SCK_MODE_INT8 && p->mode != SCK_MODE_F32) return 0;
+  if (p->mode != SCK_MODE_INT8 && p->mode != SCK_MODE_F32 && p->mode != SCK_MODE_QUAD) return 0;
   if (matches<Lat_square_1>(p)) return Lat_square_1::id;
   if (matches<Lat_triangular_1>(p)) return Lat_triangular_1::id;
   if (matches<Lat_sc_1>(p)) return Lat_sc_1::id;

@@ -137,9 +137,13 @@ int launch_sequential(const sck_plan* plan, const Common& c, cudaStream_t s);
 int launch_bitwise_class(const sck_plan* plan, const Common& c, int colour, int alpha, cudaStream_t s);
 int launch_bitwise_sequential(const sck_plan* plan, const Common& c, cudaStream_t s);
 int obs_blocks_per_rep(const sck_plan* plan, int batch);
+int obs_launch_blocks(const sck_plan* plan, int storage, int batch);
+int check_observables_request(const sck_plan* plan, int storage, int batch);
 int made_wait_timeouts(unsigned long long* count);   // bounded waits of the learned proposal's kernels that gave up
 int launch_observables(const sck_plan* plan, const void* spins, int storage, int batch, const int8_t* mask,
                        const float* k1, double* E, double* M, void* workspace, cudaStream_t s);
+int launch_observables_finish(const double* partial, int B, int blocks_per_rep, int b, int n, double* E, double* M,
+                              cudaStream_t s);
 int launch_observables_fold(const sck_plan* plan, int batch, const double* E, const double* M, double n_active,
                             const double* E_ref, double* acc, double* accv, cudaStream_t s);
 int launch_topological_charge(const sck_plan* plan, const float* spins, const int8_t* mask, int batch, int z,
@@ -155,4 +159,11 @@ int launch_spec_pipeline(const sck_plan* plan, const Common& c, int n_sweeps, in
                          cudaStream_t s);
 size_t stream_counter_bytes(const sck_plan* plan, int group);
 int stream_wait_timeouts(unsigned long long* count);   // group pipeline waits that gave up
+// interleaved storage of vector models (quad.cu)
+bool quad_ok(const sck_plan* plan, std::string* why);
+int launch_quad_class(const sck_plan* plan, const sck_buffers* buf, int colour, int alpha, cudaStream_t s);
+int launch_quad_convert(const sck_plan* plan, float* flat, float4* quads, int to_flat, cudaStream_t s);
+int quad_obs_blocks(const sck_plan* plan);
+int launch_quad_observables(const sck_plan* plan, const void* spins, int batch, const float* k1, double* E, double* M,
+                            void* workspace, cudaStream_t s);
 }  // namespace sck

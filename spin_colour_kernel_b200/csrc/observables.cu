@@ -6,7 +6,6 @@
 // + k2 (sx sy sz)^2 and its contribution to M[alpha][k]. Warp shuffles, then shared memory, reduce a block to one
 // partial per value; a second kernel sums the partials of a replica in block order, so results do not depend
 // on scheduling.
-#include <mutex>
 #include <string>
 
 #include "internal.h"
@@ -108,35 +107,6 @@ __global__ void __launch_bounds__(256) observables_kernel(const __grid_constant_
 // positive offset in z, then y, then x); its reverse sits in the partner's table with the same coupling, so
 // E = -sum_bonds J s_i . s_j - h . sum s + anisotropy equals -1/2 sum_i s_i . v_i of the generic kernel up to
 // FP64 rounding, at half the neighbour reads. Still FP64 throughout.
-template <class Lat, int A>
-__host__ __device__ constexpr bool forward_bond(int i) {
-  const BondC b = Lat::bond(A, i);
-  if (b.a2 != A) return b.a2 > A;
-  if (b.dz != 0) return b.dz > 0;
-  if (b.dy != 0) return b.dy > 0;
-  return b.dx > 0;
-}
-
-template <class Lat>
-__host__ __device__ constexpr bool bonds_paired() {
-  for (int a = 0; a < Lat::b; ++a)
-    for (int i = 0; i < Lat::n_bonds(a); ++i) {
-      const BondC b = Lat::bond(a, i);
-      bool found = false;
-      for (int j = 0; j < Lat::n_bonds(b.a2); ++j) {
-        const BondC r = Lat::bond(b.a2, j);
-        if (r.a2 == a && r.dx == -b.dx && r.dy == -b.dy && r.dz == -b.dz) {
-          int gi = 0, gj = 0;
-          while (Lat::group_end(a, gi) <= i) ++gi;
-          while (Lat::group_end(b.a2, gj) <= j) ++gj;
-          found = found || gi == gj;
-        }
-      }
-      if (!found) return false;
-    }
-  return true;
-}
-
 __device__ __forceinline__ bool step_axis(int& v, int d, int L, int per) {
   v += d;
   if (v < 0) {
@@ -466,12 +436,27 @@ static int obs_blocks_generic(const sck_plan* plan, int batch) {
   return want < per_rep ? (want < 1 ? 1 : want) : per_rep;
 }
 
-// Partial sums per replica the workspace must hold: the larger of the two paths' counts, so that a workspace
-// stays valid whatever the plan's tuning selects later.
+// Whether an observables call of this storage takes the tiled path (its lattice table on, float32 storage, a
+// geometry the tiled kernel serves).
+static bool obs_tiled(const sck_plan* plan, int storage) {
+  return plan->spec != 0 && storage == SCK_MODE_F32 && obs_tile_geometry(plan);
+}
+
+// Blocks per replica, hence partial-sum slots per replica, of one observables call: the one count that both the
+// launch and the size checks of its callers use, so the slots written and the slots summed always agree.
+int obs_launch_blocks(const sck_plan* plan, int storage, int batch) {
+  if (storage == SCK_MODE_QUAD) return quad_obs_blocks(plan);
+  return obs_tiled(plan, storage) ? plan->geom.L2 / OBS_TY : obs_blocks_generic(plan, batch);
+}
+
+// Partial sums per replica a caller's workspace must hold: the largest count any storage and tuning of this plan
+// can launch, so that a workspace stays valid whatever the plan's tuning selects later.
 int obs_blocks_per_rep(const sck_plan* plan, int batch) {
-  const int gen = obs_blocks_generic(plan, batch);
+  int most = obs_blocks_generic(plan, batch);
   const int tile = obs_tile_geometry(plan) ? plan->geom.L2 / OBS_TY : 0;
-  return gen > tile ? gen : tile;
+  if (tile > most) most = tile;
+  if (plan->mode == SCK_MODE_QUAD && quad_obs_blocks(plan) > most) most = quad_obs_blocks(plan);
+  return most;
 }
 
 // One observation of a measure step folded into FP64 accumulators, per replica r (one thread each): with
@@ -564,6 +549,7 @@ int launch_topological_charge(const sck_plan* plan, const float* spins, const in
 
 int launch_observables(const sck_plan* plan, const void* spins, int storage, int batch, const int8_t* mask,
                        const float* k1, double* E, double* M, void* workspace, cudaStream_t s) {
+  if (storage == SCK_MODE_QUAD) return launch_quad_observables(plan, spins, batch, k1, E, M, workspace, s);
   ObsParams p;
   p.g = plan->geom;
   p.B = batch;
@@ -575,8 +561,8 @@ int launch_observables(const sck_plan* plan, const void* spins, int storage, int
   for (int k = 0; k < 3; ++k) p.h64[k] = plan->desc.h64[k];
   p.k2 = plan->desc.k2_64;
   // float32 storage of a tiled-geometry system with its lattice table on: bands of OBS_TY rows
-  const bool tile = plan->spec != 0 && storage == SCK_MODE_F32 && obs_tile_geometry(plan);
-  p.blocks_per_rep = tile ? plan->geom.L2 / OBS_TY : obs_blocks_generic(plan, batch);
+  const bool tile = obs_tiled(plan, storage);
+  p.blocks_per_rep = obs_launch_blocks(plan, storage, batch);
   p.fd_plane = make_fastdiv((uint32_t)plan->geom.plane);
   p.fd_L1 = make_fastdiv((uint32_t)plan->geom.L1);
   p.fd_L2 = make_fastdiv((uint32_t)plan->geom.L2);
@@ -616,8 +602,13 @@ int launch_observables(const sck_plan* plan, const void* spins, int storage, int
   else observables_kernel<3, 1><<<grid, 256, 0, s>>>(p);
   int rc = cuda_status(cudaGetLastError(), "observables");
   if (rc != SCK_OK) return rc;
+  return launch_observables_finish(p.partial, p.B, p.blocks_per_rep, plan->geom.b, n, E, M, s);
+}
+
+int launch_observables_finish(const double* partial, int B, int blocks_per_rep, int b, int n, double* E, double* M,
+                              cudaStream_t s) {
   dim3 fb(OBS_VALUES, 8);
-  observables_finish<<<(p.B + 7) / 8, fb, 0, s>>>(p.partial, p.B, p.blocks_per_rep, plan->geom.b, n, E, M);
+  observables_finish<<<(B + 7) / 8, fb, 0, s>>>(partial, B, blocks_per_rep, b, n, E, M);
   return cuda_status(cudaGetLastError(), "observables finish");
 }
 
@@ -634,25 +625,16 @@ namespace sck {
 constexpr size_t kScratchDoubles = (size_t)1 << 18;   // 2 MiB of FP64 partial sums
 static __device__ __align__(256) double g_observables_scratch[kScratchDoubles];
 
-constexpr int kScratchDevices = 256;
-static std::mutex g_scratch_lock;
-static double* g_scratch_addr[kScratchDevices] = {};
 
-// Device address of the scratch array on the current device, looked up once per device. In host code the
-// array's name is only a host-side handle, so the address must come from the runtime.
+// Device address of the scratch array in the current context. In host code the array's name is only a host-side
+// handle, so the address must come from the runtime; it is looked up on every call (cheap, allocates nothing),
+// so a context that was reset or replaced never receives a stale address. The first lookup on a device may load
+// the library's module into the context, which is why the first call on a device belongs before any capture.
 static int scratch_address(double** out) {
-  int dev = 0;
-  int rc = cuda_status(cudaGetDevice(&dev), "no-alloc observables: current device");
+  void* p = nullptr;
+  const int rc = cuda_status(cudaGetSymbolAddress(&p, g_observables_scratch), "no-alloc observables: scratch address");
   if (rc != SCK_OK) return rc;
-  if (dev < 0 || dev >= kScratchDevices) return cuda_status(cudaErrorInvalidDevice, "no-alloc observables: device");
-  std::lock_guard<std::mutex> guard(g_scratch_lock);
-  if (g_scratch_addr[dev] == nullptr) {
-    void* p = nullptr;
-    rc = cuda_status(cudaGetSymbolAddress(&p, g_observables_scratch), "no-alloc observables: scratch address");
-    if (rc != SCK_OK) return rc;
-    g_scratch_addr[dev] = (double*)p;
-  }
-  *out = g_scratch_addr[dev];
+  *out = (double*)p;
   return SCK_OK;
 }
 
@@ -665,23 +647,13 @@ extern "C" int sck_observables_noalloc(const sck_plan* plan, const sck_buffers* 
     set_error("null plan, buffers or spins");
     return SCK_ERR_INVALID;
   }
-  if (batch < 1 || batch > 65535) {
-    set_error("batch must be within 1 .. 65535");
-    return SCK_ERR_INVALID;
-  }
-  if (storage != SCK_MODE_INT8 && storage != SCK_MODE_F32 && storage != SCK_MODE_PACKED) {
-    set_error("observables read int8, float32 or packed storage");
-    return SCK_ERR_INVALID;
-  }
-  if (storage != SCK_MODE_F32 && plan->geom.n != 1) {
-    set_error("vector models use float32 storage");
-    return SCK_ERR_INVALID;
-  }
+  const int rc0 = check_observables_request(plan, storage, batch);
+  if (rc0 != SCK_OK) return rc0;
   if ((plan->geom.has_mask && buf->mask == nullptr) || (plan->geom.has_cubic && buf->k1 == nullptr)) {
     set_error("the system needs its mask / k1 buffers");
     return SCK_ERR_INVALID;
   }
-  const size_t need = (size_t)batch * obs_blocks_per_rep(plan, batch) * OBS_VALUES;
+  const size_t need = (size_t)batch * obs_launch_blocks(plan, storage, batch) * OBS_VALUES;
   if (need > kScratchDoubles) {
     set_error("no-alloc observables: " + std::to_string(need * sizeof(double)) + " bytes of partial sums exceed the " +
               std::to_string(kScratchDoubles * sizeof(double)) + "-byte scratch; use sck_observables with a workspace");

@@ -62,6 +62,37 @@ struct GroupRange {
   static constexpr int end = Lat::group_end(A, G);
 };
 
+// A bond of a compile-time table points "forward" when it goes to a higher sublattice, or within a sublattice
+// to a positive offset in z, then y, then x; summing forward bonds only visits every bond of the lattice once.
+template <class Lat, int A>
+__host__ __device__ constexpr bool forward_bond(int i) {
+  const BondC b = Lat::bond(A, i);
+  if (b.a2 != A) return b.a2 > A;
+  if (b.dz != 0) return b.dz > 0;
+  if (b.dy != 0) return b.dy > 0;
+  return b.dx > 0;
+}
+
+template <class Lat>
+__host__ __device__ constexpr bool bonds_paired() {
+  for (int a = 0; a < Lat::b; ++a)
+    for (int i = 0; i < Lat::n_bonds(a); ++i) {
+      const BondC b = Lat::bond(a, i);
+      bool found = false;
+      for (int j = 0; j < Lat::n_bonds(b.a2); ++j) {
+        const BondC r = Lat::bond(b.a2, j);
+        if (r.a2 == a && r.dx == -b.dx && r.dy == -b.dy && r.dz == -b.dz) {
+          int gi = 0, gj = 0;
+          while (Lat::group_end(a, gi) <= i) ++gi;
+          while (Lat::group_end(b.a2, gj) <= j) ++gj;
+          found = found || gi == gj;
+        }
+      }
+      if (!found) return false;
+    }
+  return true;
+}
+
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 
 // sin and cos of phi in [0, 2 pi] through the SFU on the reduced range [-pi, pi].
@@ -72,15 +103,16 @@ __device__ __forceinline__ void sincos_2pi(float phi, float& sn, float& cs) {
 }
 
 // Proposal, energy change with cubic anisotropy, and Metropolis / Barker decision of two attempts (lane .x, lane
-// .y) with Philox counters cnt0 / cnt1, anisotropy sites k1_0 / k1_1 and inverse temperatures beta, given their
-// spins s and local fields v (field included). Returns the proposals in t and the decisions in acc0 / acc1. Same
-// operation order as the reference's kernel (generator.py:275-305); packed float32x2 operations round each lane
-// to nearest. With two == false lane .y repeats lane .x's draws and its result is ignored.
+// .y) with Philox counters cnt0 / cnt1, anisotropy coefficients k1 (used only when `cubic`) and inverse
+// temperatures beta, given their spins s and local fields v (field included). Returns the proposals in t and the
+// decisions in acc0 / acc1. Same operation order as the reference's kernel (generator.py:275-305); packed
+// float32x2 operations round each lane to nearest. With two == false lane .y repeats lane .x's draws and its
+// result is ignored. The lattice kernels (finish_core below) and the interleaved kernels (quad.cu) both call it,
+// so the two storage layouts compute identical numbers.
 template <int N>
-__device__ __forceinline__ void finish_core(const Common& c, uint32_t cnt0, uint32_t cnt1, bool two, int k1_0,
-                                            int k1_1, float2 beta, int32_t key, const float2 (&s)[N],
-                                            const float2 (&v)[N], float2 (&t)[N], bool& acc0, bool& acc1) {
-  const Geometry& g = c.g;
+__device__ __forceinline__ void finish_values(int acceptance, bool cubic, float2 k1, float k2c, uint32_t cnt0,
+                                              uint32_t cnt1, bool two, float2 beta, int32_t key, const float2 (&s)[N],
+                                              const float2 (&v)[N], float2 (&t)[N], bool& acc0, bool& acc1) {
   const Philox4 ra = philox4x32_10(cnt0, 0u, key_lo(key), key_hi(key));
   const Philox4 rb = two ? philox4x32_10(cnt1, 0u, key_lo(key), key_hi(key)) : ra;
   const float2 u0 = make_float2(to_uniform(ra.x0), to_uniform(rb.x0));
@@ -111,9 +143,8 @@ __device__ __forceinline__ void finish_core(const Common& c, uint32_t cnt0, uint
   for (int k = 1; k < N; ++k) d = __fadd2_rn(d, __fmul2_rn(__fadd2_rn(t[k], neg(s[k])), v[k]));
   float2 dE = neg(d);
   if constexpr (N == 3) {
-    if (g.has_cubic) {
-      const float2 k1 = make_float2(c.k1[k1_0], c.k1[k1_1]);
-      const float2 k2 = f2(c.k2);
+    if (cubic) {
+      const float2 k2 = f2(k2c);
       auto aniso = [&](const float2* p) {
         const float2 q01 = __fmul2_rn(p[0], p[1]), q02 = __fmul2_rn(p[0], p[2]), q12 = __fmul2_rn(p[1], p[2]);
         const float2 tri = __fmul2_rn(q01, p[2]);
@@ -123,7 +154,7 @@ __device__ __forceinline__ void finish_core(const Common& c, uint32_t cnt0, uint
       dE = __fadd2_rn(dE, __fadd2_rn(aniso(t), neg(aniso(s))));
     }
   }
-  if (g.acceptance == SCK_BARKER) {
+  if (acceptance == SCK_BARKER) {
     const float2 xb = __fmul2_rn(beta, dE);
     acc0 = __fmul_rn(u0.x, __fadd_rn(1.0f, __expf(xb.x))) < 1.0f;
     acc1 = __fmul_rn(u0.y, __fadd_rn(1.0f, __expf(xb.y))) < 1.0f;
@@ -132,6 +163,15 @@ __device__ __forceinline__ void finish_core(const Common& c, uint32_t cnt0, uint
     acc0 = u0.x < __expf(xm.x);
     acc1 = u0.y < __expf(xm.y);
   }
+}
+
+template <int N>
+__device__ __forceinline__ void finish_core(const Common& c, uint32_t cnt0, uint32_t cnt1, bool two, int k1_0,
+                                            int k1_1, float2 beta, int32_t key, const float2 (&s)[N],
+                                            const float2 (&v)[N], float2 (&t)[N], bool& acc0, bool& acc1) {
+  const bool cubic = N == 3 && c.g.has_cubic;
+  const float2 k1 = cubic ? make_float2(c.k1[k1_0], c.k1[k1_1]) : f2(0.0f);
+  finish_values<N>(c.g.acceptance, cubic, k1, c.k2, cnt0, cnt1, two, beta, key, s, v, t, acc0, acc1);
 }
 
 // Two replicas rep0 / rep1 of site `own`.

@@ -7,6 +7,9 @@ Spin_Colour_Kernel/sampler.py:39-345, so code written against the reference runs
   .set_temperature(T)  .set_seed(seed, sweep)  .init_spins(kind, seed)  .pack(x)  .unpack(S)
   .sweep(S, n)  .graph(S, k)  .sync_sweep(S, n)  .reference_sweep(S, n)
   .local_field(S)  .energy(S)  .magnetization(S)
+plus one keyword of its own, `layout`: "reference" (default) keeps S[B, n, b, L3, L2, L1]; "quad" keeps vector-model
+spins interleaved four replicas per float4 with rows split by colour residue (include/sck.h, SCK_MODE_QUAD) —
+the sampler's resident state, converted by pack / unpack as the reference converts its packed Ising words.
 `state` (int64 {seed, sweep}), `beta` and the acceptance tables are device tensors updated in place, so a
 captured CUDA graph keeps reading them by address. Every update runs in the CUDA kernels behind the C ABI of
 include/sck.h; there is no CPU path, and a CPU device is refused.
@@ -56,8 +59,14 @@ class Sampler:
     def __init__(self, system: System, batch: int, device="cuda", seed: int = 0, compact: bool = True,
                  spin_dtype: torch.dtype | None = None, packed: bool | None = None, bitwise: bool = False,
                  words_per_program: int | None = None, independent: bool = False, bitwise_tile: int | None = None,
-                 bitwise_warps: int | None = None, max_block: int = MAX_BLOCK):
+                 bitwise_warps: int | None = None, max_block: int = MAX_BLOCK, layout: str = "reference"):
         self.sys = system
+        if layout not in ("reference", "quad"):
+            raise ValueError("layout must be 'reference' or 'quad'")
+        self.layout = layout
+        self.quad = layout == "quad"
+        if self.quad and (system.n == 1 or bitwise or packed):
+            raise ValueError("the interleaved 'quad' layout is for vector models (n = 2 or 3) in float32")
         self.bitwise = bool(bitwise)
         self.independent = bool(independent)
         if self.independent and not self.bitwise:
@@ -78,7 +87,8 @@ class Sampler:
         self.B = int(batch)
         n, b, L3, L2, L1 = system.n, system.b, system.L3, system.L2, system.L1
         self.W = -(-self.B // WORD) if self.packed else self.B
-        self.Bp = self.W * WORD if self.packed else self.B
+        self.Bp = self.W * WORD if self.packed else (4 * -(-self.B // 4) if self.quad else self.B)
+        self.Q = self.Bp // 4 if self.quad else 0
         if self.Bp * b * L3 * L2 * L1 >= 2 ** 31 - 1:
             raise ValueError("replica batch too large for the int32 Philox counter")
         gmax = words_per_program or BWG
@@ -94,6 +104,10 @@ class Sampler:
             self.mode = L.MODE_BITWISE_INDEP if self.independent else L.MODE_BITWISE
         elif self.packed:
             self.mode = L.MODE_PACKED
+        elif self.quad:
+            if self.spin_dtype != torch.float32:
+                raise ValueError("the interleaved 'quad' layout stores float32 components")
+            self.mode = L.MODE_QUAD
         elif self.spin_dtype == torch.int8:
             self.mode = L.MODE_INT8
         else:
@@ -131,6 +145,7 @@ class Sampler:
         self.classes = P.sweep_classes(system)
         self._mask_f = torch.as_tensor(m, device=dev).to(torch.float32)
         self._obs_ws = {}
+        self._flat_sampler = None
         self._workspace(self.B)
 
     def tune(self, specialised=True, l2_budget: int = 0, resident_limit: int = 200 << 10):
@@ -228,12 +243,29 @@ class Sampler:
             x = torch.randn(shape, generator=g)
             x = x / x.norm(dim=1, keepdim=True)
         x = x.to(self.device) * self._mask_f
-        if self.packed:
+        if self.packed or self.quad:
             return self.pack(x)
         return x.to(self.spin_dtype).contiguous()
 
+    def quad_shape(self) -> tuple:
+        """Shape of interleaved storage: (quads, b, L3, L2, n, L1, 4) float32."""
+        s = self.sys
+        return (self.Q, s.b, s.L3, s.L2, s.n, s.L1, 4)
+
+    def _is_quad(self, S: torch.Tensor) -> bool:
+        return self.quad and S.dim() == 7 and tuple(S.shape) == self.quad_shape()
+
     def pack(self, x: torch.Tensor) -> torch.Tensor:
-        """(B, 1, b, L3, L2, L1) spins of +-1 (0 on masked sites) -> (W, 1, b, L3, L2, L1) int32 words."""
+        """(B, 1, b, L3, L2, L1) spins of +-1 (0 on masked sites) -> (W, 1, b, L3, L2, L1) int32 words; with the
+        'quad' layout, (B, n, b, L3, L2, L1) float32 components -> interleaved quads (padding lanes 0)."""
+        if self.quad:
+            x = x.to(device=self.device, dtype=torch.float32).contiguous()
+            if tuple(x.shape) != (self.B, self.sys.n) + self.sys.shape:
+                raise ValueError(f"pack expects float32 spins of shape {(self.B, self.sys.n) + self.sys.shape}")
+            out = torch.empty(self.quad_shape(), dtype=torch.float32, device=self.device)
+            with torch.cuda.device(self.device):
+                L.check(L.lib().sck_quad_pack(self._plan, _ptr(x), _ptr(out), self._stream()))
+            return out
         sgn = (x > 0).to(torch.int8).to(self.device).contiguous()
         if sgn.shape[0] != self.B:
             raise ValueError("pack expects one row per replica")
@@ -242,7 +274,14 @@ class Sampler:
         return out
 
     def unpack(self, S: torch.Tensor) -> torch.Tensor:
-        """Packed words -> (B, 1, b, L3, L2, L1) int8 spins of +-1, 0 on masked sites; identity when unpacked."""
+        """Packed words -> (B, 1, b, L3, L2, L1) int8 spins of +-1, 0 on masked sites; interleaved quads ->
+        (B, n, b, L3, L2, L1) float32; identity for the reference layout."""
+        if self._is_quad(S):
+            self._check(S)
+            out = torch.empty((self.B, self.sys.n) + self.sys.shape, dtype=torch.float32, device=self.device)
+            with torch.cuda.device(self.device):
+                L.check(L.lib().sck_quad_unpack(self._plan, _ptr(S), _ptr(out), self._stream()))
+            return out
         if not self.packed or S.dtype != torch.int32:
             return S
         self._check(S)
@@ -257,6 +296,8 @@ class Sampler:
     def _check(self, S: torch.Tensor):
         want_dtype = torch.int32 if self.packed else self.spin_dtype
         want_shape = ((self.W, 1) if self.packed else (self.B, self.sys.n)) + self.sys.shape
+        if self.quad:
+            want_shape = self.quad_shape()
         if S.device != self.device or S.dtype != want_dtype or tuple(S.shape) != want_shape or not S.is_contiguous():
             raise ValueError(f"spins must be a contiguous {want_dtype} tensor of shape {want_shape} on {self.device}")
 
@@ -310,8 +351,26 @@ class Sampler:
         replay.keep = (self, S, g)
         return replay
 
+    def _flat(self):
+        """A reference-layout sampler over the same system, sharing this sampler's state and beta buffers (the
+        checks that read S: synchronous control, sequential reference)."""
+        if self._flat_sampler is None:
+            f = Sampler(self.sys, self.B, device=self.device, seed=0)
+            f.state = self.state
+            f.beta = self.beta
+            self._flat_sampler = f
+        return self._flat_sampler
+
+    def _via_flat(self, S, fn, n):
+        X = self.unpack(S)
+        getattr(self._flat(), fn)(X, n)
+        S.copy_(self.pack(X))
+        return S
+
     def sync_sweep(self, S: torch.Tensor, n: int = 1) -> torch.Tensor:
         """The negative control: every site updated in the same step from the old state."""
+        if self.quad:
+            return self._via_flat(S, "sync_sweep", n)
         self._check(S)
         scratch = torch.empty_like(S)
         buf = self._buffers(S)
@@ -321,6 +380,8 @@ class Sampler:
 
     def reference_sweep(self, S: torch.Tensor, n: int = 1) -> torch.Tensor:
         """Sequential reference chain on the GPU: classes in order, sites one at a time in raster order."""
+        if self.quad:
+            return self._via_flat(S, "reference_sweep", n)
         self._check(S)
         buf = self._buffers(S)
         with torch.cuda.device(self.device):
@@ -374,6 +435,9 @@ class Sampler:
         if S.dtype == torch.int32 and self.packed:
             self._check(S)
             storage, batch = L.MODE_PACKED, self.B
+        elif self._is_quad(S):
+            self._check(S)
+            storage, batch = L.MODE_QUAD, self.B
         else:
             if S.dtype == torch.int8 and s.n == 1:
                 storage = L.MODE_INT8
@@ -409,6 +473,9 @@ class Sampler:
         if S.dtype == torch.int32 and self.packed:
             self._check(S)
             storage = L.MODE_PACKED
+        elif self._is_quad(S):
+            self._check(S)
+            storage = L.MODE_QUAD
         else:
             storage = L.MODE_INT8 if (S.dtype == torch.int8 and s.n == 1) else L.MODE_F32
             if storage == L.MODE_F32 and S.dtype != torch.float32:
@@ -425,6 +492,8 @@ class Sampler:
         """Berg-Luscher charge (B,) float64 of z-layer `layer` of sublattice 0 (anneal.py:69-80). Graph-safe
         with a preallocated Q."""
         s = self.sys
+        if self._is_quad(S):
+            return self._flat().topological_charge(self.unpack(S), layer, Q)
         if S.dtype != torch.float32 or tuple(S.shape) != (self.B, s.n) + s.shape or not S.is_contiguous():
             raise ValueError(f"spins must be contiguous float32 ({self.B}, {s.n}) + {s.shape}")
         if Q is None:

@@ -78,17 +78,26 @@ def test_cuda_chain_matches_reference_fixture(name):
     S = A.init_spins(seed=case["init"])
     assert np.array_equal(_spins(A, S), g["S0"].astype(_spins(A, S).dtype)), "initial spins differ"
     snaps = {int(k): i for i, k in enumerate(g["snap_ids"])}
+    assert g["E"].shape[0] == case["sweeps"], "the fixtures record E and M after every sweep"
     fracs = []
     for k in range(1, case["sweeps"] + 1):
         A.sweep(S)
+        exact_here = s.n == 1
         if k in snaps:
             _compare(name, s, _spins(A, S), g["snaps"][snaps[k]], fracs)
-            E = A.energy(S).cpu().numpy()
-            if s.n == 1:
-                np.testing.assert_allclose(E, g["E"][k - 1], rtol=1e-12, atol=1e-9)
-                np.testing.assert_allclose(A.magnetization(S).cpu().numpy(), g["M"][k - 1], rtol=1e-12, atol=1e-9)
-    if s.n == 1:
-        assert int(A.state[1]) == case["sweeps"]
+            exact_here = exact_here or fracs[-1] == 0.0
+        # E and M after every sweep (all 200 of the 2D Ising workload): Ising to FP64 rounding; vector models,
+        # where no decision flipped, to the float32 differences of their spins
+        E, M = (t.cpu().numpy() for t in A.observables(S))
+        if s.n == 1:
+            np.testing.assert_allclose(E, g["E"][k - 1], rtol=1e-12, atol=1e-9, err_msg=f"E after sweep {k}")
+            np.testing.assert_allclose(M, g["M"][k - 1], rtol=1e-12, atol=1e-9, err_msg=f"M after sweep {k}")
+        elif exact_here:
+            np.testing.assert_allclose(E, g["E"][k - 1], rtol=1e-5, atol=1e-4 * s.n_active,
+                                       err_msg=f"E after sweep {k}")
+            np.testing.assert_allclose(M, g["M"][k - 1], rtol=1e-5, atol=1e-4 * s.n_active,
+                                       err_msg=f"M after sweep {k}")
+    assert int(A.state[1]) == case["sweeps"]
     print(f"{name}: fraction of spins beyond tolerance per recorded sweep: {fracs}")
 
 
@@ -564,12 +573,15 @@ def test_workload3_full_size_replicas_match_oracle():
 @pytest.mark.parametrize("independent", [False, True])
 def test_workload2_full_size_words_match_oracle(independent):
     """3D Ising sc L=128, bitwise, as two counter-legal instances of 512 replicas (base seeds 1 and 2; the
-    reference refuses 1024 x 128^3 >= 2^31 - 1 counters). One sweep of each instance on the GPU; words 0 and 15
-    of each instance (64 replicas) are recomputed by the oracle on their own."""
+    reference refuses 1024 x 128^3 >= 2^31 - 1 counters). The GPU sweeps each whole instance; words 0 and 15 of
+    each (64 replicas) are recomputed on their own by the oracle's C port (their counters depend only on their
+    own word index), spin for spin: 50 sweeps of the first instance, 2 of the second."""
+    from oracle import native
     from spin_colour_kernel_b200.sampler import Sampler
+    native.build()
     s = sy.ising("sc", 128)
     T16 = torch.linspace(4.0, 5.0, 16)
-    for inst, seed in enumerate((1, 2)):
+    for inst, (seed, sweeps) in enumerate(((1, 50), (2, 2))):
         A = Sampler(s, 512, device="cuda", seed=seed, bitwise=True, independent=independent)
         T = T16[8 * inst: 8 * inst + 8].repeat_interleave(64)
         A.set_temperature(T)
@@ -577,10 +589,10 @@ def test_workload2_full_size_words_match_oracle(independent):
         S = A.pack(torch.randint(0, 2, (512, 1) + s.shape, device="cuda", generator=g, dtype=torch.int8) * 2 - 1)
         words = [0, 15]
         x = A.unpack(S).cpu().numpy()
-        ref = np.concatenate([x[32 * w: 32 * w + 32, 0] for w in words]).astype(np.int64)
+        ref = np.concatenate([x[32 * w: 32 * w + 32, 0] for w in words])
         table = A.ptab.cpu().numpy()[words]
-        A.sweep(S)
+        A.sweep(S, sweeps)
         got = A.unpack(S).cpu().numpy()
         got = np.concatenate([got[32 * w: 32 * w + 32, 0] for w in words])
-        ref = obw.sweep(s, ref, table, seed, 0, independent=independent, words=words)
-        assert np.array_equal(got, ref)
+        ref = native.bitwise_sweep(s, ref, table, seed, 0, sweeps, independent=independent, words=words)
+        assert np.array_equal(got, ref), f"instance {inst}: {int((got != ref).sum())} spins differ"

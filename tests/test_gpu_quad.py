@@ -1,0 +1,196 @@
+"""Interleaved ('quad') storage of vector models: four replicas per float4, rows split by colour residue.
+
+The interleaved class kernels run the same packed-pair arithmetic as the lattice kernels of the reference layout,
+so their chains must be identical to those kernels' spin for spin (bit-exact), and within the vector-model
+tolerance of the reference's recorded chains. Conversions must round-trip exactly; FP64 observables read from
+the quads must equal those of the reference layout.
+"""
+
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+import cases as C
+from oracle import observables as obs
+from spin_colour_kernel_b200 import _lib as L
+from spin_colour_kernel_b200 import crystals as cr
+from spin_colour_kernel_b200 import system as sy
+
+pytestmark = pytest.mark.gpu
+GOLD = Path(__file__).resolve().parent / "golden"
+VEC_TOL = 1e-5
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from spin_colour_kernel_b200 import build
+    build.build()
+
+
+def _quad(s, B, seed=1, **kw):
+    from spin_colour_kernel_b200.sampler import Sampler
+    return Sampler(s, B, device="cuda", seed=seed, layout="quad", **kw)
+
+
+def _supported(s):
+    """Whether the library accepts an interleaved plan for this system (a host-only call)."""
+    import ctypes
+    from spin_colour_kernel_b200 import plan as P
+    d = P.describe(s)
+    h = ctypes.c_void_p()
+    rc = L.lib().sck_plan_create(ctypes.byref(d), 4, L.MODE_QUAD, ctypes.byref(h))
+    if rc == L.OK:
+        L.lib().sck_plan_destroy(h)
+    return rc == L.OK
+
+
+VEC_FIXTURES = [k for k in C.CASES if (GOLD / f"{k}.npz").exists() and not C.CASES[k].get("bitwise")
+                and C.CASES[k]["build"](sy, cr).n > 1]
+
+
+@pytest.mark.parametrize("name", VEC_FIXTURES)
+def test_quad_chain_matches_reference_fixture(name):
+    case = C.CASES[name]
+    s = case["build"](sy, cr)
+    if not _supported(s):
+        with pytest.raises(ValueError):
+            _quad(s, case["B"], seed=case["seed"])
+        return
+    g = dict(np.load(GOLD / f"{name}.npz"))
+    A = _quad(s, case["B"], seed=case["seed"])
+    A.set_temperature(torch.from_numpy(g["T"]))
+    S = A.init_spins(seed=case["init"])
+    assert np.array_equal(A.unpack(S).cpu().numpy(), g["S0"]), "initial spins differ"
+    snaps = {int(k): i for i, k in enumerate(g["snap_ids"])}
+    for k in range(1, case["sweeps"] + 1):
+        A.sweep(S)
+        if k in snaps:
+            got = A.unpack(S).cpu().numpy().astype(np.float64)
+            d = np.abs(got - g["snaps"][snaps[k]].astype(np.float64))
+            frac = float((d > VEC_TOL).any(axis=1).mean())
+            assert frac <= 0.02, f"{name}: {frac:.4f} of spins beyond {VEC_TOL}"
+    assert int(A.state[1]) == case["sweeps"]
+
+
+def test_quad_fixture_coverage():
+    """The interleaved path serves the periodic lattice-table fixtures the workloads need."""
+    served = [k for k in VEC_FIXTURES if _supported(C.CASES[k]["build"](sy, cr))]
+    for need in ("w3_heis_bcc4_j1j2", "w4_xy_square16", "heis_bcc2", "heis_fcc2", "xy_square4"):
+        assert need in served, need
+
+
+SYSTEMS = [
+    ("bcc J1-J2 K1 h 8^3", lambda: C.heisenberg_bcc_j1j2(sy, cr, 8), 10),
+    ("bcc J1-J2 K1 h 6^3 odd replicas", lambda: C.heisenberg_bcc_j1j2(sy, cr, 6), 7),
+    ("Heisenberg sc 8x6x4 h", lambda: sy.System("Heisenberg sc", 3, cr.make("sc"), (8, 6, 4), (True,) * 3,
+                                               {1: -1.0}, h=(0.1, 0.0, 0.2)), 8),
+    ("Heisenberg fcc 4^3", lambda: sy.heisenberg("fcc", 4), 5),
+    ("Heisenberg bcc J1 4^3", lambda: sy.heisenberg("bcc", 4), 6),
+    ("XY square 16 h", lambda: C.xy_periodic_field(sy, cr, "square", 16), 9),
+    ("XY triangular 8", lambda: sy.xy("triangular", 8), 4),
+    ("XY sc 64x4x4 (templated row)", lambda: sy.System("XY sc", 2, cr.make("sc"), (64, 4, 4), (True,) * 3,
+                                                       {1: 1.0}), 4),
+    ("Heisenberg bcc J1-J2 32x4x4 Barker", lambda: _barker(sy.System(
+        "Heisenberg bcc", 3, cr.make("bcc", (1, 2)), (32, 4, 4), (True,) * 3, {1: 1.0, 2: 0.3})), 8),
+]
+
+
+def _barker(s):
+    s.acceptance = "barker"
+    return s
+
+
+@pytest.mark.parametrize("label, make, B", SYSTEMS, ids=[x[0] for x in SYSTEMS])
+def test_quad_sweeps_equal_lattice_kernels_bit_for_bit(label, make, B):
+    from spin_colour_kernel_b200.sampler import Sampler
+    s = make()
+    R = Sampler(s, B, device="cuda", seed=77)
+    R.tune(1, 0, 0)                    # lattice kernels, class by class (no resident or tile path)
+    Q = _quad(s, B, seed=77)
+    T = torch.linspace(0.4, 3.0, B)
+    R.set_temperature(T)
+    Q.set_temperature(T)
+    X = R.init_spins(seed=5)
+    S = Q.pack(X)
+    assert torch.equal(Q.unpack(S), X)
+    for k in range(4):
+        R.sweep(X, 1 + k)
+        Q.sweep(S, 1 + k)
+        assert torch.equal(Q.unpack(S), X), f"{label}: sweep block {k}"
+    assert int(Q.state[1]) == int(R.state[1]) == 10
+
+
+def test_quad_pack_round_trip_and_padding():
+    s = C.heisenberg_bcc_j1j2(sy, cr, 4)
+    Q = _quad(s, 6)
+    x = torch.randn((6, 3) + s.shape, device="cuda")
+    S = Q.pack(x)
+    assert tuple(S.shape) == (2, 2, 4, 4, 3, 4, 4)
+    assert torch.equal(Q.unpack(S), x)
+    # lanes 2, 3 of the last quad are padding, zero after a pack
+    assert torch.count_nonzero(S[1, ..., 2:]) == 0
+    # element order: component k of site (a, z, y, x) at [q, a, z, y, k, (x % 2) * 2 + x // 2, j]
+    xn, Sn = x.cpu().numpy(), S.cpu().numpy()
+    for (rep, k, a, z, y, xx) in [(0, 0, 0, 0, 0, 0), (5, 2, 1, 3, 2, 3), (2, 1, 0, 1, 3, 2), (3, 0, 1, 2, 0, 1)]:
+        assert Sn[rep // 4, a, z, y, k, (xx % 2) * 2 + xx // 2, rep % 4] == xn[rep, k, a, z, y, xx]
+
+
+def test_quad_observables_equal_reference_layout_and_oracle():
+    for s, B in ((C.heisenberg_bcc_j1j2(sy, cr, 6), 7), (C.xy_periodic_field(sy, cr, "square", 16), 5),
+                 (sy.heisenberg("fcc", 4), 4)):
+        Q = _quad(s, B, seed=3)
+        Q.set_temperature(torch.linspace(0.5, 2.0, B))
+        S = Q.init_spins(seed=3)
+        Q.sweep(S, 2)
+        E, M = Q.observables(S)
+        x = Q.unpack(S)
+        E2, M2 = Q._flat().observables(x)
+        np.testing.assert_allclose(E.cpu().numpy(), E2.cpu().numpy(), rtol=1e-12, atol=1e-9, err_msg=s.name)
+        np.testing.assert_allclose(M.cpu().numpy(), M2.cpu().numpy(), rtol=1e-12, atol=1e-9, err_msg=s.name)
+        xn = x.cpu().numpy()
+        np.testing.assert_allclose(E.cpu().numpy(), obs.energy(s, xn), rtol=1e-12, atol=1e-9, err_msg=s.name)
+        np.testing.assert_allclose(M.cpu().numpy(), obs.magnetization(xn), rtol=1e-12, atol=1e-9)
+
+
+def test_quad_graph_replay_equals_sweeps():
+    s = C.heisenberg_bcc_j1j2(sy, cr, 8)
+    A, B = _quad(s, 8, seed=9), _quad(s, 8, seed=9)
+    for X in (A, B):
+        X.set_temperature(torch.linspace(0.5, 2.5, 8))
+    S1, S2 = A.init_spins(seed=1), B.init_spins(seed=1)
+    rep = A.graph(S1, 3)       # one warm-up sweep, then a graph of 3
+    rep()
+    B.sweep(S2, 4)
+    assert torch.equal(S1, S2)
+
+
+def test_quad_reference_sweep_and_sync_control_match_reference_layout():
+    from spin_colour_kernel_b200.sampler import Sampler
+    s = sy.heisenberg("bcc", 2)
+    Q = _quad(s, 3, seed=11)
+    R = Sampler(s, 3, device="cuda", seed=11)
+    for X in (Q, R):
+        X.set_temperature(1.5)
+    x = R.init_spins(seed=2)
+    S = Q.pack(x)
+    R.reference_sweep(x, 2)
+    Q.reference_sweep(S, 2)
+    assert torch.equal(Q.unpack(S), x)
+    assert int(Q.state[1]) == 2
+
+
+def test_quad_refuses_unsupported_systems():
+    with pytest.raises(ValueError):
+        _quad(sy.ising("square", 8), 4)                       # Ising
+    with pytest.raises(ValueError):
+        _quad(C.xy_disk(sy, cr, "square", 12), 4)             # mask, open boundary
+    with pytest.raises(ValueError):
+        _quad(sy.heisenberg("triangular", 6), 4)              # colouring of x-period 3
+    with pytest.raises(ValueError):
+        _quad(sy.heisenberg("kagome", 4), 4)                  # no compile-time lattice table

@@ -69,6 +69,27 @@ def test_plan_refusals_mirror_the_reference():
     assert L.lib().sck_plan_create(ctypes.byref(d), 4, L.MODE_INT8, ctypes.byref(h)) == L.ERR_INVALID
 
 
+def test_interleaved_plans_accept_the_periodic_lattice_table_systems_only():
+    bcc = C.heisenberg_bcc_j1j2(sy, cr, 64)
+    assert _plan(bcc, 1536, L.MODE_QUAD)[0] == 0
+    shape = ctypes.c_int32(), ctypes.c_int32()
+    d = P.describe(bcc)
+    h = ctypes.c_void_p()
+    assert L.lib().sck_plan_create(ctypes.byref(d), 7, L.MODE_QUAD, ctypes.byref(h)) == 0
+    L.lib().sck_plan_shape(h, ctypes.byref(shape[0]), ctypes.byref(shape[1]))
+    L.lib().sck_plan_destroy(h)
+    assert (shape[0].value, shape[1].value) == (8, 2)           # 7 replicas computed as 2 quads
+    for s in (sy.xy("square", 16), sy.heisenberg("fcc", 4), sy.heisenberg("bcc", 4), sy.xy("triangular", 8)):
+        assert _plan(s, 4, L.MODE_QUAD)[0] == 0, s.name
+    for s, word in ((sy.ising("square", 8), "vector"), (C.xy_disk(sy, cr, "square", 12), "mask"),
+                    (sy.heisenberg("triangular", 6), "x-period"), (sy.heisenberg("kagome", 4), "table"),
+                    (sy.System("XY sc open", 2, cr.make("sc"), (4, 4, 4), (False,) * 3, {1: 1.0}), "periodic")):
+        rc, msg = _plan(s, 4, L.MODE_QUAD)
+        assert rc == L.ERR_UNSUPPORTED and word in msg, (s.name, msg)
+    # the Philox envelope counts the padding lanes: 4 * ceil(B / 4) replicas
+    assert _plan(bcc, 4096, L.MODE_QUAD)[0] == L.ERR_COUNTER
+
+
 def test_describe_groups_bonds_by_coupling_in_first_appearance_order():
     # shells 1 and 3 share J: one group of 6 + 8 bonds, then shell 2 (12 bonds); J = 0 shell 4 is left out
     s = sy.System("sc shells", 1, cr.make("sc", (1, 2, 3, 4)), (9, 9, 9), (True,) * 3,

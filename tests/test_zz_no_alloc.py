@@ -47,6 +47,10 @@ def _both(A, S, storage, batch):
     (lambda: sy.nanodot(Rd=2.5, L=3), L.MODE_F32, 3),
     (lambda: sy.ising("sc", 10), L.MODE_INT8, 40),
     (lambda: sy.ising("square", 12), L.MODE_PACKED, 70),
+    # the tiled FP64 path (rows of 16 sites, 16 rows: 4 bands per replica), at the scratch limit exactly:
+    # 4096 replicas x 4 blocks x 16 doubles = 2 MiB
+    (lambda: C.heisenberg_bcc_j1j2(sy, cr, 16), L.MODE_F32, 4096),
+    (lambda: C.heisenberg_bcc_j1j2(sy, cr, 8), L.MODE_QUAD, 10),
 ])
 def test_no_alloc_observables_equal_workspace_observables(make, storage, batch):
     if not torch.cuda.is_available():
@@ -55,7 +59,9 @@ def test_no_alloc_observables_equal_workspace_observables(make, storage, batch):
     from spin_colour_kernel_b200.sampler import Sampler
     build.build()
     s = make()
-    kw = {"packed": storage == L.MODE_PACKED}
+    kw = {"packed": storage == L.MODE_PACKED} if s.n == 1 else {}
+    if storage == L.MODE_QUAD:
+        kw["layout"] = "quad"
     A = Sampler(s, batch, device="cuda", seed=5, **kw)
     A.set_temperature(torch.linspace(0.5, 4.0, batch))
     S = A.init_spins(seed=1)
@@ -67,14 +73,19 @@ def test_no_alloc_observables_equal_workspace_observables(make, storage, batch):
 
 
 def test_no_alloc_observables_refuse_oversized_requests():
+    """A request whose partial sums exceed the fixed array is refused (the plan's batch allows it, so only the
+    size limit can reject it), and so is a batch beyond the plan's, before anything is launched."""
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
     from spin_colour_kernel_b200.sampler import Sampler
-    s = sy.ising("sc", 8)
-    A = Sampler(s, 16, device="cuda", seed=1, packed=False)
+    s = C.heisenberg_bcc_j1j2(sy, cr, 16)
+    A = Sampler(s, 4097, device="cuda", seed=1)
     S = A.init_spins(seed=1)
     buf = A._buffers(S)
-    E = torch.empty(20000, dtype=torch.float64, device="cuda")
-    rc = L.lib().sck_observables_noalloc(A._plan, ctypes.byref(buf), S.data_ptr(), L.MODE_INT8, 20000, E.data_ptr(),
+    E = torch.empty(4097, dtype=torch.float64, device="cuda")
+    rc = L.lib().sck_observables_noalloc(A._plan, ctypes.byref(buf), S.data_ptr(), L.MODE_F32, 4097, E.data_ptr(),
                                          None, A._stream())
     assert rc == L.ERR_INVALID and b"scratch" in L.lib().sck_last_error()
+    rc = L.lib().sck_observables_noalloc(A._plan, ctypes.byref(buf), S.data_ptr(), L.MODE_F32, 4098, E.data_ptr(),
+                                         None, A._stream())
+    assert rc == L.ERR_INVALID and b"plan's batch" in L.lib().sck_last_error()
