@@ -191,6 +191,20 @@ int sck_observables_workspace_size(const sck_plan* plan, int32_t batch, int64_t*
 int sck_observables(const sck_plan* plan, const sck_buffers* buf, const void* spins, int32_t storage,
                     int32_t batch, double* E, double* M, void* workspace, void* stream);
 
+/* A measure step: n_sweeps sweeps in place (as sck_sweep), then the FP64 observables of the configuration they
+ * leave, E[batch] and M[batch][b][n] for the plan's batch (Sampler.sweep followed by Sampler.energy /
+ * magnetization, sampler.py:234-345, fused). With interleaved storage (SCK_MODE_QUAD) on a colouring whose
+ * coupling groups never mix neighbours of earlier and later classes (every lattice-table system the
+ * interleaved plans take), the last sweep's class launches accumulate them as they go: each bond is counted
+ * once, by its later endpoint, when both its spins are final, so no pass re-reads the state. Each site's energy
+ * share is formed in float32 from the float32 local fields of the sweep and summed in FP64 (energies agree with
+ * sck_observables to float32 rounding of the shares, magnetizations to FP64 rounding); other plans run the
+ * sweeps and then the sck_observables pass (FP64 throughout). `workspace` holds
+ * sck_sweep_measure_workspace_size bytes; deterministic, fixed-order sums. No counterpart in the reference. */
+int sck_sweep_measure_workspace_size(const sck_plan* plan, int64_t* bytes);
+int sck_sweep_measure(const sck_plan* plan, const sck_buffers* buf, int32_t n_sweeps, double* E, double* M,
+                      void* workspace, void* stream);
+
 /* One observation of a measure step folded into FP64 accumulators: the reference's ladder runner
  * (simulate_state, simulate.py:338-353) observes every `every` sweeps and accumulates, per replica r,
  *   acc[0*batch + r] += E - E_ref[r],  acc[1*batch + r] += (E - E_ref[r])^2,

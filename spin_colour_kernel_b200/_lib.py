@@ -63,6 +63,8 @@ _SIGNATURES = {
     "sck_topological_charge": ([_vp, ctypes.POINTER(Buffers), _vp, _i32, _i32, _vp, _vp], _i32),
     "sck_observables_accumulate": ([_vp, ctypes.POINTER(Buffers), _vp, _i32, _i32, ctypes.c_double, _vp, _vp, _vp,
                                     _vp, _vp, _vp, _vp], _i32),
+    "sck_sweep_measure_workspace_size": ([_vp, ctypes.POINTER(_i64)], _i32),
+    "sck_sweep_measure": ([_vp, ctypes.POINTER(Buffers), _i32, _vp, _vp, _vp, _vp], _i32),
     "sck_observables_noalloc": ([_vp, ctypes.POINTER(Buffers), _vp, _i32, _i32, _vp, _vp, _vp], _i32),
     "sck_wait_timeouts": ([ctypes.POINTER(_i64)], _i32),
     "sck_pack": ([_vp, _vp, _vp, _vp], _i32),

@@ -598,6 +598,37 @@ int sck_observables(const sck_plan* plan, const sck_buffers* buf, const void* sp
   return launch_observables(plan, spins, storage, batch, buf->mask, buf->k1, E, M, workspace, (cudaStream_t)stream);
 }
 
+int sck_sweep_measure_workspace_size(const sck_plan* plan, int64_t* bytes) {
+  if (plan == nullptr || bytes == nullptr) return fail(SCK_ERR_INVALID, "null plan or output");
+  const int64_t obs = (int64_t)plan->batch * obs_blocks_per_rep(plan, plan->batch) * OBS_VALUES * (int64_t)sizeof(double);
+  const int64_t fused = plan->mode == SCK_MODE_QUAD ? (int64_t)quad_measure_workspace(plan) : 0;
+  *bytes = obs > fused ? obs : fused;
+  return SCK_OK;
+}
+
+int sck_sweep_measure(const sck_plan* plan, const sck_buffers* buf, int32_t n_sweeps, double* E, double* M,
+                      void* workspace, void* stream) {
+  int rc = check_buffers(plan, buf, true);
+  if (rc != SCK_OK) return rc;
+  if (n_sweeps < 1) return fail(SCK_ERR_INVALID, "a measure step needs at least one sweep");
+  if (workspace == nullptr) return fail(SCK_ERR_INVALID, "null workspace (see sck_sweep_measure_workspace_size)");
+  if (plan->batch > 65535) return fail(SCK_ERR_INVALID, "measure step: batch above 65535");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (plan->mode == SCK_MODE_QUAD && quad_measure_fused(plan)) {
+    if (n_sweeps > 1) {
+      rc = sck_sweep(plan, buf, n_sweeps - 1, stream);
+      if (rc != SCK_OK) return rc;
+    }
+    return launch_quad_measure_sweep(plan, buf, E, M, workspace, s);
+  }
+  rc = sck_sweep(plan, buf, n_sweeps, stream);
+  if (rc != SCK_OK) return rc;
+  const int storage = plan->mode == SCK_MODE_QUAD ? SCK_MODE_QUAD
+                      : (plan->mode == SCK_MODE_BITWISE || plan->mode == SCK_MODE_BITWISE_INDEP) ? SCK_MODE_PACKED
+                      : plan->mode;
+  return launch_observables(plan, buf->spins, storage, plan->batch, buf->mask, buf->k1, E, M, workspace, s);
+}
+
 int sck_observables_accumulate(const sck_plan* plan, const sck_buffers* buf, const void* spins, int32_t storage,
                                int32_t batch, double n_active, const double* E_ref, double* E, double* M,
                                double* acc, double* accv, void* workspace, void* stream) {

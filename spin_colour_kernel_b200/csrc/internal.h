@@ -164,6 +164,10 @@ bool quad_ok(const sck_plan* plan, std::string* why);
 int launch_quad_class(const sck_plan* plan, const sck_buffers* buf, int colour, int alpha, cudaStream_t s);
 int launch_quad_convert(const sck_plan* plan, float* flat, float4* quads, int to_flat, cudaStream_t s);
 int quad_obs_blocks(const sck_plan* plan);
+bool quad_measure_fused(const sck_plan* plan);
+size_t quad_measure_workspace(const sck_plan* plan);
+int launch_quad_measure_sweep(const sck_plan* plan, const sck_buffers* buf, double* E, double* M, void* workspace,
+                              cudaStream_t s);
 int launch_quad_observables(const sck_plan* plan, const void* spins, int batch, const float* k1, double* E, double* M,
                             void* workspace, cudaStream_t s);
 }  // namespace sck

@@ -33,6 +33,17 @@ struct QuadParams {
   const float* beta;     // 4 per quad
   const int64_t* state;
   int colour, alpha, sweep_offset, q0;
+  // measure sweeps (MEASURE kernels): the class's index in the sweep, the coupling groups whose bonds all reach
+  // classes updated earlier in the sweep, per-block FP64 partial sums [replica][class][block][1 + N]
+  int measure_ci, n_classes, blocks_x, B;
+  unsigned lower_groups;
+  double* partial;
+};
+
+// FP64 sums one thread adds to a measure sweep: per lane j, the site's energy share and its N components.
+template <int N>
+struct MeasureAcc {
+  double v[4][1 + N];
 };
 
 // Residue (0 .. P-1) along x of the class's sites in row (y, z) of the launch's sublattice, or -1 when the row
@@ -112,8 +123,12 @@ __device__ __forceinline__ float2 lo2(float4 v) { return make_float2(v.x, v.y); 
 __device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); }
 
 // One class site (row segment position h, residue ph, row (y, z), sublattice A) of the four replicas of quad q.
-template <class Lat, int A, int N, int P, int L1C>
-__device__ __forceinline__ void quad_site(const QuadParams& p, int q, int h, int ph, int y, int z, int32_t key) {
+// MEASURE: also the site's share of the energy of the configuration the sweep leaves, -s'.v_low - h.s' +
+// anisotropy(s') with v_low the coupling-group fields of the neighbours updated earlier in the sweep (each bond
+// is counted once, at its later endpoint, when both its spins are final), and its components s', added in FP64.
+template <class Lat, int A, int N, int P, int L1C, bool MEASURE>
+__device__ __forceinline__ void quad_site(const QuadParams& p, int q, int h, int ph, int y, int z, int32_t key,
+                                          MeasureAcc<N>& m) {
   const Geometry& g = p.g;
   const int L1 = L1C ? L1C : g.L1;
   float4* base = p.spins + (size_t)q * N * g.nsite;
@@ -124,9 +139,9 @@ __device__ __forceinline__ void quad_site(const QuadParams& p, int q, int h, int
   float4 s4[N];
 #pragma unroll
   for (int k = 0; k < N; ++k) s4[k] = base[own_e + k * L1];
-  float2 vl[N], vh[N];
+  float2 vl[N], vh[N], wl[N], wh[N];
 #pragma unroll
-  for (int k = 0; k < N; ++k) vl[k] = vh[k] = f2(0.0f);
+  for (int k = 0; k < N; ++k) vl[k] = vh[k] = wl[k] = wh[k] = f2(0.0f);
   static_for<0, Lat::groups>([&](auto gc) {
     constexpr int gi = decltype(gc)::value;
     using Rg = GroupRange<Lat, A, gi>;
@@ -148,6 +163,15 @@ __device__ __forceinline__ void quad_site(const QuadParams& p, int q, int h, int
     for (int k = 0; k < N; ++k) {
       vl[k] = __fadd2_rn(vl[k], __fmul2_rn(J, gl[k]));
       vh[k] = __fadd2_rn(vh[k], __fmul2_rn(J, gh[k]));
+    }
+    if constexpr (MEASURE) {
+      if ((p.lower_groups >> gi) & 1u) {
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+          wl[k] = __fadd2_rn(wl[k], __fmul2_rn(J, gl[k]));
+          wh[k] = __fadd2_rn(wh[k], __fmul2_rn(J, gh[k]));
+        }
+      }
     }
   });
 #pragma unroll
@@ -172,17 +196,57 @@ __device__ __forceinline__ void quad_site(const QuadParams& p, int q, int h, int
                    a0, a1);
   finish_values<N>(g.acceptance, cubic, f2(k1), p.k2, c0 + 2 * ns, c0 + 3 * ns, true, make_float2(b4.z, b4.w), key,
                    sh, vh, th, a2, a3);
+  float4 n4[N];
+#pragma unroll
+  for (int k = 0; k < N; ++k)
+    n4[k] = make_float4(a0 ? tl[k].x : s4[k].x, a1 ? tl[k].y : s4[k].y, a2 ? th[k].x : s4[k].z,
+                        a3 ? th[k].y : s4[k].w);
   if (a0 | a1 | a2 | a3) {
 #pragma unroll
-    for (int k = 0; k < N; ++k)
-      base[own_e + k * L1] = make_float4(a0 ? tl[k].x : s4[k].x, a1 ? tl[k].y : s4[k].y, a2 ? th[k].x : s4[k].z,
-                                         a3 ? th[k].y : s4[k].w);
+    for (int k = 0; k < N; ++k) base[own_e + k * L1] = n4[k];
+  }
+  if constexpr (MEASURE) {
+    // float32 share of the site in each lane, then FP64 sums
+    auto share = [&](float2 n0, float2 n1, float2 n2, const float2 (&w)[N]) {
+      const float2 nn[3] = {n0, n1, n2};
+      float2 bond = __fmul2_rn(nn[0], w[0]);
+#pragma unroll
+      for (int k = 1; k < N; ++k) bond = __fadd2_rn(bond, __fmul2_rn(nn[k], w[k]));
+      float2 e = make_float2(-bond.x, -bond.y);
+#pragma unroll
+      for (int k = 0; k < N; ++k)
+        if (p.hnz[k]) e = __fadd2_rn(e, __fmul2_rn(f2(-p.h[k]), nn[k]));
+      if (cubic) {
+        const float2 q01 = __fmul2_rn(nn[0], nn[1]), q02 = __fmul2_rn(nn[0], nn[2]), q12 = __fmul2_rn(nn[1], nn[2]);
+        const float2 tri = __fmul2_rn(q01, nn[2]);
+        const float2 quad = __fadd2_rn(__fadd2_rn(__fmul2_rn(q01, q01), __fmul2_rn(q02, q02)), __fmul2_rn(q12, q12));
+        e = __fadd2_rn(e, __fadd2_rn(__fmul2_rn(f2(k1), quad), __fmul2_rn(__fmul2_rn(f2(p.k2), tri), tri)));
+      }
+      return e;
+    };
+    const float2 el = share(lo2(n4[0]), lo2(n4[1 % N]), N == 3 ? lo2(n4[2 % N]) : f2(0.0f), wl);
+    const float2 eh = share(hi2(n4[0]), hi2(n4[1 % N]), N == 3 ? hi2(n4[2 % N]) : f2(0.0f), wh);
+    m.v[0][0] += (double)el.x;
+    m.v[1][0] += (double)el.y;
+    m.v[2][0] += (double)eh.x;
+    m.v[3][0] += (double)eh.y;
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      m.v[0][1 + k] += (double)n4[k].x;
+      m.v[1][1 + k] += (double)n4[k].y;
+      m.v[2][1 + k] += (double)n4[k].z;
+      m.v[3][1 + k] += (double)n4[k].w;
+    }
   }
 }
 
+template <int V>
+__device__ __forceinline__ void block_sum(double (&x)[V], double (*red)[8]);
+
 // Grid (ceil(L3 L2 L1 / P / 256), quads of this launch). Thread -> (row, position in the row's class segment).
-template <class Lat, int N, int P, int L1C>
-__global__ void __launch_bounds__(256) quad_class_kernel(const __grid_constant__ QuadParams p) {
+// At most 85 registers (three blocks of 256 threads per SM) for the sweep; 128 for measure launches.
+template <class Lat, int N, int P, int L1C, bool MEASURE>
+__global__ void __launch_bounds__(256, MEASURE ? 2 : 3) quad_class_kernel(const __grid_constant__ QuadParams p) {
   const Geometry& g = p.g;
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   uint32_t row, h;
@@ -193,17 +257,47 @@ __global__ void __launch_bounds__(256) quad_class_kernel(const __grid_constant__
     row = fdiv(t, p.fd_hp);
     h = t - row * (uint32_t)p.hp;
   }
-  if (row >= (uint32_t)(g.L3 * g.L2)) return;
-  const int z = (int)fdiv(row, p.fd_L2);
-  const int y = (int)row - z * g.L2;
-  const int ph = class_residue<P>(p, y, z);
-  if (ph < 0) return;
   const int q = p.q0 + (int)blockIdx.y;
-  const int32_t key = sweep_key_at(p.state, p.sweep_offset);
-  static_for<0, Lat::b>([&](auto ac) {
-    constexpr int a = decltype(ac)::value;
-    if (a == p.alpha) quad_site<Lat, a, N, P, L1C>(p, q, (int)h, ph, y, z, key);
-  });
+  MeasureAcc<N> m;
+  if constexpr (MEASURE) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int v = 0; v <= N; ++v) m.v[j][v] = 0.0;
+  }
+  if (row < (uint32_t)(g.L3 * g.L2)) {
+    const int z = (int)fdiv(row, p.fd_L2);
+    const int y = (int)row - z * g.L2;
+    const int ph = class_residue<P>(p, y, z);
+    if (ph >= 0) {
+      const int32_t key = sweep_key_at(p.state, p.sweep_offset);
+      static_for<0, Lat::b>([&](auto ac) {
+        constexpr int a = decltype(ac)::value;
+        if (a == p.alpha) quad_site<Lat, a, N, P, L1C, MEASURE>(p, q, (int)h, ph, y, z, key, m);
+      });
+    }
+  }
+  if constexpr (MEASURE) {
+    // every thread of the block reaches here: block sums in a fixed order, one partial per (replica, value)
+    __shared__ double red[4 * (1 + N)][8];
+    double x[4 * (1 + N)];
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int v = 0; v <= N; ++v) x[j * (1 + N) + v] = m.v[j][v];
+    block_sum<4 * (1 + N)>(x, red);
+    if (threadIdx.x < 4 * (1 + N)) {
+      const int j = threadIdx.x / (1 + N), v = threadIdx.x - j * (1 + N);
+      const int rep = 4 * q + j;
+      if (rep < p.B) {
+        double val = 0.0;
+#pragma unroll
+        for (int i = 0; i < 4 * (1 + N); ++i)
+          if (i == (int)threadIdx.x) val = x[i];
+        p.partial[(((size_t)rep * p.n_classes + p.measure_ci) * p.blocks_x + blockIdx.x) * (1 + N) + v] = val;
+      }
+    }
+  }
 }
 
 // ------------------------------------------------------------------------------------------ layout changes
@@ -434,7 +528,10 @@ static QuadParams quad_params(const sck_plan* plan, const sck_buffers* buf, int 
 
 template <class Lat, int N, int P, int L1C>
 static void launch_quad_t(const QuadParams& p, dim3 grid, cudaStream_t s) {
-  quad_class_kernel<Lat, N, P, L1C><<<grid, 256, 0, s>>>(p);
+  if (p.partial != nullptr)
+    quad_class_kernel<Lat, N, P, L1C, true><<<grid, 256, 0, s>>>(p);
+  else
+    quad_class_kernel<Lat, N, P, L1C, false><<<grid, 256, 0, s>>>(p);
 }
 
 template <class Lat, int N, int P>
@@ -468,20 +565,152 @@ static void launch_quad_grid(const sck_plan* plan, const QuadParams& p, dim3 gri
   }
 }
 
-// One class of every quad (sweep offset 0: the sweep state[1] names).
-int launch_quad_class(const sck_plan* plan, const sck_buffers* buf, int colour, int alpha, cudaStream_t s) {
-  QuadParams p = quad_params(plan, buf, colour, alpha);
-  const Geometry& g = plan->geom;
-  const uint32_t per = (uint32_t)g.L3 * g.L2 * p.hp;
+static int quad_blocks_x(const sck_plan* plan) {
+  const uint32_t per = (uint32_t)plan->geom.L3 * plan->geom.L2 * (plan->geom.L1 / plan->P);
+  return (int)((per + 255) / 256);
+}
+
+static int launch_quad_params(const sck_plan* plan, QuadParams& p, cudaStream_t s) {
   const int Q = plan->Bp / 4;
   for (int q0 = 0; q0 < Q; q0 += 65535) {
     p.q0 = q0;
     const int nq = Q - q0 < 65535 ? Q - q0 : 65535;
-    launch_quad_grid(plan, p, dim3((per + 255) / 256, (unsigned)nq), s);
+    launch_quad_grid(plan, p, dim3((unsigned)quad_blocks_x(plan), (unsigned)nq), s);
     const int rc = cuda_status(cudaGetLastError(), "interleaved class launch");
     if (rc != SCK_OK) return rc;
   }
   return SCK_OK;
+}
+
+// One class of every quad (sweep offset 0: the sweep state[1] names).
+int launch_quad_class(const sck_plan* plan, const sck_buffers* buf, int colour, int alpha, cudaStream_t s) {
+  QuadParams p = quad_params(plan, buf, colour, alpha);
+  return launch_quad_params(plan, p, s);
+}
+
+// ------------------------------------------------------------------------------------------ measure sweeps
+// The coupling groups of class ci's sublattice whose bonds all reach classes earlier in the sweep order, or
+// false when some group mixes earlier and later neighbours. For a linear colouring the neighbour's colour along
+// bond (alpha -> alpha2, delta) is the site's colour shifted by K delta + o_alpha2 - o_alpha in every factor,
+// the same for every site of the class, so the answer is one per (class, bond).
+static bool class_lower_groups(const sck_plan* plan, int ci, unsigned* mask) {
+  const sck_system_desc& d = plan->desc;
+  const Colouring& col = plan->col;
+  const int colour = d.classes[ci][0], alpha = d.classes[ci][1];
+  int digit[SCK_MAX_FACTORS] = {0, 0, 0, 0};
+  for (int r = col.r - 1, c = colour; r >= 0; --r) {
+    digit[r] = c % col.m[r];
+    c /= col.m[r];
+  }
+  const sck_sublattice& sub = d.sub[alpha];
+  unsigned out = 0;
+  int bi = 0;
+  for (int gi = 0; gi < sub.n_groups; ++gi) {
+    int lower = 0, later = 0;
+    for (; bi < sub.group_end[gi]; ++bi) {
+      const sck_bond& bd = sub.bonds[bi];
+      int c2 = 0;
+      for (int r = 0; r < col.r; ++r) {
+        long long v = digit[r] + (long long)col.K[r][0] * bd.d[0] + (long long)col.K[r][1] * bd.d[1] +
+                      (long long)col.K[r][2] * bd.d[2] + col.o[bd.alpha2][r] - col.o[alpha][r];
+        v %= col.m[r];
+        if (v < 0) v += col.m[r];
+        c2 = c2 * col.m[r] + (int)v;
+      }
+      int idx = -1;
+      for (int j = 0; j < d.n_classes; ++j)
+        if (d.classes[j][0] == c2 && d.classes[j][1] == bd.alpha2) idx = j;
+      if (idx < 0 || idx == ci) return false;   // a neighbour in no class, or in its own class: not a colouring
+      (idx < ci ? lower : later) += 1;
+    }
+    if (lower && later) return false;
+    if (lower) out |= 1u << gi;
+  }
+  *mask = out;
+  return true;
+}
+
+bool quad_measure_fused(const sck_plan* plan) {
+  if (plan->desc.n_classes > 64) return false;
+  unsigned m = 0;
+  for (int ci = 0; ci < plan->desc.n_classes; ++ci)
+    if (!class_lower_groups(plan, ci, &m)) return false;
+  return true;
+}
+
+size_t quad_measure_workspace(const sck_plan* plan) {
+  const size_t fused = (size_t)plan->batch * plan->desc.n_classes * quad_blocks_x(plan) * (1 + plan->geom.n);
+  const size_t exact = (size_t)plan->batch * quad_obs_blocks(plan) * OBS_VALUES;
+  return (fused > exact ? fused : exact) * sizeof(double);
+}
+
+struct MeasureFinishParams {
+  int n_classes, blocks_x, n, b;
+  int cls_alpha[64];
+};
+
+// E[r] = sum of every class's and block's energy shares, M[r][alpha][k] = sum over the classes of sublattice
+// alpha; one block per replica, fixed-order sums.
+__global__ void __launch_bounds__(128) quad_measure_finish(const double* __restrict__ partial,
+                                                           const __grid_constant__ MeasureFinishParams f,
+                                                           double* __restrict__ E, double* __restrict__ M) {
+  const int rep = blockIdx.x;
+  const int V = 1 + f.n;
+  const int per = f.n_classes * f.blocks_x;
+  double acc[1 + SCK_MAX_BASIS * 3];
+#pragma unroll
+  for (int i = 0; i < 1 + SCK_MAX_BASIS * 3; ++i) acc[i] = 0.0;
+  const double* src = partial + (size_t)rep * per * V;
+  for (int i = threadIdx.x; i < per; i += blockDim.x) {
+    const int a = f.cls_alpha[i / f.blocks_x];
+    acc[0] += src[(size_t)i * V];
+#pragma unroll
+    for (int aa = 0; aa < SCK_MAX_BASIS; ++aa)
+      if (aa == a)
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+          if (k < f.n) acc[1 + aa * 3 + k] += src[(size_t)i * V + 1 + k];
+  }
+  __shared__ double red[1 + SCK_MAX_BASIS * 3][8];
+  block_sum<1 + SCK_MAX_BASIS * 3>(acc, red);
+  if (threadIdx.x == 0) {
+    if (E != nullptr) E[rep] = acc[0];
+    if (M != nullptr)
+      for (int a = 0; a < f.b; ++a)
+        for (int k = 0; k < f.n; ++k) M[((size_t)rep * f.b + a) * f.n + k] = acc[1 + a * 3 + k];
+  }
+}
+
+// One sweep whose class launches also accumulate the FP64 observables of the configuration it leaves (E and M
+// of the first plan->batch replicas), then the counter advance. Needs quad_measure_fused(plan).
+int launch_quad_measure_sweep(const sck_plan* plan, const sck_buffers* buf, double* E, double* M, void* workspace,
+                              cudaStream_t s) {
+  const int C = plan->desc.n_classes;
+  for (int ci = 0; ci < C; ++ci) {
+    QuadParams p = quad_params(plan, buf, plan->desc.classes[ci][0], plan->desc.classes[ci][1]);
+    if (!class_lower_groups(plan, ci, &p.lower_groups)) {
+      set_error("measure sweep: a coupling group mixes earlier and later classes");
+      return SCK_ERR_UNSUPPORTED;
+    }
+    p.measure_ci = ci;
+    p.n_classes = C;
+    p.blocks_x = quad_blocks_x(plan);
+    p.B = plan->batch;
+    p.partial = (double*)workspace;
+    const int rc = launch_quad_params(plan, p, s);
+    if (rc != SCK_OK) return rc;
+  }
+  int rc = launch_advance(buf->state, 1, s);
+  if (rc != SCK_OK) return rc;
+  MeasureFinishParams f;
+  memset(&f, 0, sizeof(f));
+  f.n_classes = C;
+  f.blocks_x = quad_blocks_x(plan);
+  f.n = plan->geom.n;
+  f.b = plan->geom.b;
+  for (int ci = 0; ci < C; ++ci) f.cls_alpha[ci] = plan->desc.classes[ci][1];
+  quad_measure_finish<<<plan->batch, 128, 0, s>>>((const double*)workspace, f, E, M);
+  return cuda_status(cudaGetLastError(), "measure sweep finish");
 }
 
 // Reference layout <-> interleaved storage: to_flat = 0 packs `flat` (B x N x sites floats) into `quads`,

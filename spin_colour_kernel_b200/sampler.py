@@ -504,6 +504,29 @@ class Sampler:
                                                    _ptr(Q), self._stream()))
         return Q
 
+    def sweep_measure(self, S: torch.Tensor, n: int = 1, E: torch.Tensor | None = None,
+                      M: torch.Tensor | None = None):
+        """A measure step: n sweeps in place, then the FP64 energy (B,) and magnetization (B, b, n) of the state
+        they leave (include/sck.h, sck_sweep_measure). With the 'quad' layout the last sweep accumulates them as it
+        updates (float32 site shares, FP64 sums); otherwise it is sweep + observables. Graph-safe with
+        preallocated outputs once the first call has sized the workspace."""
+        self._check(S)
+        s = self.sys
+        if E is None:
+            E = torch.empty(self.B, dtype=torch.float64, device=self.device)
+        if M is None:
+            M = torch.empty((self.B, s.b, s.n), dtype=torch.float64, device=self.device)
+        ws = getattr(self, "_measure_ws", None)
+        if ws is None:
+            nbytes = ctypes.c_int64()
+            L.check(L.lib().sck_sweep_measure_workspace_size(self._plan, ctypes.byref(nbytes)))
+            ws = self._measure_ws = torch.empty(max(1, nbytes.value // 8), dtype=torch.float64, device=self.device)
+        buf = self._buffers(S)
+        with torch.cuda.device(self.device):
+            L.check(L.lib().sck_sweep_measure(self._plan, ctypes.byref(buf), int(n), _ptr(E), _ptr(M), _ptr(ws),
+                                              self._stream()))
+        return E, M
+
     def energy(self, S: torch.Tensor) -> torch.Tensor:
         """Total energy per replica, float64."""
         return self.observables(S)[0]

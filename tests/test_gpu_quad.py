@@ -194,3 +194,58 @@ def test_quad_refuses_unsupported_systems():
         _quad(sy.heisenberg("triangular", 6), 4)              # colouring of x-period 3
     with pytest.raises(ValueError):
         _quad(sy.heisenberg("kagome", 4), 4)                  # no compile-time lattice table
+
+
+@pytest.mark.parametrize("make, B", [(lambda: C.heisenberg_bcc_j1j2(sy, cr, 8), 10),
+                                     (lambda: C.xy_periodic_field(sy, cr, "square", 16), 6),
+                                     (lambda: sy.heisenberg("fcc", 4), 4),
+                                     (lambda: sy.heisenberg("bcc", 4), 8)])
+def test_measure_sweep_equals_sweep_then_observables(make, B):
+    """The fused measure step leaves the same chain as plain sweeps, and its observables equal the FP64 pass on
+    the state it leaves: magnetizations to FP64 rounding, energies to the float32 rounding of the site shares."""
+    s = make()
+    A, R = _quad(s, B, seed=13), _quad(s, B, seed=13)
+    for X in (A, R):
+        X.set_temperature(torch.linspace(0.6, 2.6, B))
+    S1, S2 = A.init_spins(seed=4), R.init_spins(seed=4)
+    for n in (1, 3):
+        E, M = A.sweep_measure(S1, n)
+        R.sweep(S2, n)
+        assert torch.equal(S1, S2)
+        E2, M2 = R.observables(S2)
+        np.testing.assert_allclose(M.cpu().numpy(), M2.cpu().numpy(), rtol=1e-11, atol=1e-9, err_msg=s.name)
+        np.testing.assert_allclose(E.cpu().numpy(), E2.cpu().numpy(), rtol=2e-6, atol=1e-5 * s.n_active,
+                                   err_msg=s.name)
+    assert int(A.state[1]) == int(R.state[1]) == 4
+
+
+def test_measure_sweep_graph_capture():
+    s = C.heisenberg_bcc_j1j2(sy, cr, 8)
+    A = _quad(s, 8, seed=2)
+    A.set_temperature(torch.linspace(0.5, 2.5, 8))
+    S = A.init_spins(seed=1)
+    E = torch.empty(8, dtype=torch.float64, device="cuda")
+    M = torch.empty((8, 2, 3), dtype=torch.float64, device="cuda")
+    A.sweep_measure(S, 1, E, M)                          # first call: sizes the workspace
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        A.sweep_measure(S, 2, E, M)
+    g.replay()
+    E2, M2 = A.observables(S)
+    np.testing.assert_allclose(E.cpu().numpy(), E2.cpu().numpy(), rtol=2e-6)
+    np.testing.assert_allclose(M.cpu().numpy(), M2.cpu().numpy(), rtol=1e-11, atol=1e-9)
+    assert int(A.state[1]) == 3
+
+
+def test_measure_step_of_reference_layout_is_sweep_then_observables():
+    from spin_colour_kernel_b200.sampler import Sampler
+    s = C.xy_periodic_field(sy, cr, "square", 16)
+    A, R = Sampler(s, 5, device="cuda", seed=3), Sampler(s, 5, device="cuda", seed=3)
+    for X in (A, R):
+        X.set_temperature(0.8)
+    S1, S2 = A.init_spins(seed=2), R.init_spins(seed=2)
+    E, M = A.sweep_measure(S1, 2)
+    R.sweep(S2, 2)
+    E2, M2 = R.observables(S2)
+    assert torch.equal(S1, S2) and torch.equal(E, E2) and torch.equal(M, M2)
