@@ -213,6 +213,73 @@ def reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def reference_triton_arm(args, rank, world):
+    """The reference's own GPU path on this B200: its generated Triton class kernels, driven through its public
+    Sampler (Sampler(...).graph(S, k) replays timed with CUDA events, as its exp_perf.rate times them), from the
+    unmodified package installed in baseline/_ref; none of this repository's kernels is loaded. Same workload as
+    the default arm (Heisenberg bcc 64^3 x 2, J1-J2, K1, h_z, 1,536 replicas at 24 temperatures; spins uniform on
+    the sphere drawn on the device). Prints the `unavailable` line with the reason when the package or its Triton
+    compilation is missing here."""
+    if rank != 0:
+        return
+    import tempfile
+    ref = ROOT / "baseline" / "_ref"
+    base = {"impl": "reference-triton", "metric": "spin-update attempts/ns", "unit": "attempts/ns"}
+    if not (ref / "Spin_Colour_Kernel").is_dir():
+        print(json.dumps({**base, "unavailable": "reference not installed in baseline/_ref"}), flush=True)
+        return
+    os.environ.setdefault("SCK_CACHE", tempfile.mkdtemp(prefix="sck_ref_cache_"))
+    sys.path.insert(0, str(ref))
+    try:
+        from Spin_Colour_Kernel import crystals as rcr
+        from Spin_Colour_Kernel import system as rsy
+        from Spin_Colour_Kernel.sampler import Sampler as RefSampler
+        device = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+        torch.cuda.set_device(device)
+        L, B = args.L, args.replicas
+        s = rsy.System("Heisenberg bcc J1-J2", 3, rcr.make("bcc", (1, 2)), (L, L, L), (True,) * 3, {1: 1.0, 2: 0.3},
+                       h=(0.0, 0.0, 0.1), cubic_k1=np.full((2, L, L, L), 0.05, np.float32))
+        A = RefSampler(s, B, device, 1234)
+        A.set_temperature(torch.linspace(0.5, 2.5, 24).repeat_interleave(-(-B // 24))[:B])
+        g = torch.Generator(device=device).manual_seed(2)
+        S = torch.randn((B, 3) + s.shape, device=device, generator=g)
+        S = (S / S.norm(dim=1, keepdim=True)).contiguous()
+        replay = A.graph(S, 1)
+        for _ in range(max(1, args.warmup)):
+            replay()
+        torch.cuda.synchronize(device)
+        clocks = ClockSampler(device.index)
+        clocks.start()
+        time.sleep(0.25)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            replay()
+        e1.record()
+        torch.cuda.synchronize(device)
+        clk = clocks.stop()
+        ms = e0.elapsed_time(e1)
+    except Exception as exc:                     # no Triton for this GPU, a compile failure, ...
+        print(json.dumps({**base, "unavailable": f"{type(exc).__name__}: {str(exc).splitlines()[0][:200]}"}),
+              flush=True)
+        return
+    value = B * s.n_active * args.steps / (ms * 1e6)
+    peak, kind = hbm_peak()
+    achieved = value * 24.0
+    loaded = sorted({m.__name__.split(".")[0] for m in list(sys.modules.values()) if m is not None and
+                     getattr(m, "__name__", "").startswith(("spin_colour_kernel_b200", "Spin_Colour_Kernel"))})
+    line = {**base, "value": value, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"heisenberg-bcc-{L}^3x2-J1J2-K1-hz", "replicas": B, "sites": s.nsite,
+                       "path": "reference Sampler.graph(S, 1) replays (generated Triton class kernels)",
+                       "python_packages_loaded": loaded},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "note": f"algorithmic 24 B/attempt over the replay; peak {kind}"},
+            "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
 def ragged(args, rank, world, device):
     """96 XY systems of uneven size and mask in one batch, sweeps captured in a CUDA graph of 100 sweeps (or
     of K when K is not a multiple of 100); one step = one sweep of every system."""
@@ -377,10 +444,15 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--workload", default="heisenberg-bcc", choices=sorted(BYTES_PER_ATTEMPT))
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-triton"],
+                    help="ours; reference = the reference's CPU arithmetic on the host cores; reference-triton = "
+                         "the reference's own Triton kernels on this GPU (installed in baseline/_ref)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--L", type=int, default=64, help="heisenberg-bcc cells per axis (profiling runs use less)")
     ap.add_argument("--replicas", type=int, default=1536, help="heisenberg-bcc replicas")
+    ap.add_argument("--group", type=int, default=None,
+                    help="interleaved layout: replicas per group of the class-skewed L2 pipeline (0 = class by class)")
+    ap.add_argument("--skew", type=int, default=2, help="interleaved layout: class skew of the pipeline")
     ap.add_argument("--layout", default="quad", choices=["quad", "reference"],
                     help="heisenberg-bcc resident storage: interleaved quads (default) or the reference layout")
     ap.add_argument("--path", default="auto",
@@ -403,6 +475,9 @@ def main():
     if args.impl == "reference":
         reference_arm(args, rank, world)
         return
+    if args.impl == "reference-triton":
+        reference_triton_arm(args, rank, world)
+        return
     import datetime
     if dist:
         import torch.distributed as tdist
@@ -422,7 +497,9 @@ def main():
     s, A, S, T, cfg = make_workload(args.workload, rank, device, args.L, args.replicas, args.layout)
     budget = int((args.l2_mb or 0) * (1 << 20))
     if A.quad:
-        pass                               # one kernel family: the interleaved class kernels
+        if args.group:
+            A.pipeline(args.group, args.skew)
+        cfg["pipeline"] = {"group": A.path()["group"], "skew": args.skew if args.group else None}
     elif args.path in ("tile", "segment", "row", "lattice", "generic"):
         A.tune({"tile": 3, "segment": 2, "row": 2, "lattice": 1, "generic": 0}[args.path], budget, RESIDENT_LIMIT)
     elif args.path == "autotune":
@@ -439,8 +516,8 @@ def main():
     # the K timed steps are one call sweep(S, K): the library sees the whole sequence (a resident launch runs all
     # K sweeps on-chip, the L2 pipeline overlaps consecutive sweeps), as a user running K sweeps would call it
     K = args.steps
-    if path["resident"]:
-        launches = 1
+    if path["resident"] or (A.quad and groups):
+        launches = 1                       # one resident launch, or one pipeline launch, per call of K sweeps
     elif groups:
         launches = K * groups + C - 1
     else:

@@ -162,6 +162,25 @@ int sck_plan_tune(sck_plan* plan, int32_t specialised, int64_t l2_budget_bytes, 
 int sck_plan_path(const sck_plan* plan, int32_t* specialised, int64_t* l2_budget_bytes, int32_t* group,
                   int32_t* resident);
 
+/* The class-skewed L2 pipeline of interleaved storage (SCK_MODE_QUAD plans; no counterpart in the reference,
+ * whose sweeps launch class by class). Class-by-class launches read the whole state once per class; the pipeline
+ * cuts the quads into groups of group_replicas / 4 quads and runs the classes of a group back to back, so that
+ * its later classes find the group in L2. Class c of unit u (sweep-major groups) runs at position skew u + c:
+ * skew = the class count runs the groups one after another, skew 1 overlaps the most groups (and needs the
+ * largest L2 working set, about classes / skew + 1 groups). One launch carries a whole sck_sweep call; the
+ * chain is identical to class-by-class launches. group_replicas = 0 returns to class-by-class launches. Set-up
+ * (not capturable): allocates the ticket and completion counters on the current device and a host-mapped flag.
+ * Errors: SCK_ERR_UNSUPPORTED for other plans; SCK_ERR_INVALID for a group that is not whole quads, a skew that
+ * does not divide the class count, or too few groups for the skew (skew x groups must reach the class count).
+ *
+ * The pipeline's blocks wait for the class they follow with an iteration limit (sck_plan_set_wait_limit, default
+ * 2^20 polls, about a second); a block whose wait gives up leaves its sites unchanged and raises the plan's flag.
+ * sck_plan_wait_status synchronises `stream` and returns SCK_ERR_TIMEOUT (clearing the flag) when a wait of this
+ * plan gave up since the last status read; until then sck_sweep of the plan refuses with SCK_ERR_TIMEOUT. */
+int sck_plan_pipeline(sck_plan* plan, int32_t group_replicas, int32_t skew);
+int sck_plan_set_wait_limit(sck_plan* plan, int64_t polls);
+int sck_plan_wait_status(sck_plan* plan, void* stream);
+
 /* One class launch: every site of class (colour, alpha) of every replica, read from `src`, written to
  * `buf->spins` (src may equal buf->spins). colour < 0 with sync != 0 is the synchronous control (every site of
  * the sublattice from `src`). Replaces kernel[grid](...) of generator.py:191 / bitwise.py:278. */

@@ -52,6 +52,9 @@ _SIGNATURES = {
     "sck_plan_table_size": ([_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i32), ctypes.POINTER(_i32)], _i32),
     "sck_plan_shape": ([_vp, ctypes.POINTER(_i32), ctypes.POINTER(_i32)], _i32),
     "sck_plan_tune": ([_vp, _i32, _i64, _i64], _i32),
+    "sck_plan_pipeline": ([_vp, _i32, _i32], _i32),
+    "sck_plan_set_wait_limit": ([_vp, _i64], _i32),
+    "sck_plan_wait_status": ([_vp, _vp], _i32),
     "sck_plan_path": ([_vp, ctypes.POINTER(_i32), ctypes.POINTER(_i64), ctypes.POINTER(_i32),
                        ctypes.POINTER(_i32)], _i32),
     "sck_class_update": ([_vp, ctypes.POINTER(Buffers), _vp, _i32, _i32, _i32, _vp], _i32),

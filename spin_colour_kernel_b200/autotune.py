@@ -1,10 +1,14 @@
 """Autotuner of the sweep's execution path.
 
-The chain a Sampler produces does not depend on how its sweeps are executed, only the speed does. The knobs of
-the plan (`sck_plan_tune`) are: the specialised lattice kernels on or off, and the L2 budget of the group
-pipeline (0 = class by class over all replicas). `autotune(sampler, S)` times every candidate on a scratch copy
-of the spins with CUDA events, keeps the fastest, restores the sweep counter, and caches the choice per
-(system, batch, mode, device) in a JSON file (`$SCK_TUNE_CACHE`, default ~/.cache/spin_colour_kernel_b200/).
+The chain a Sampler produces does not depend on how its sweeps are executed, only the speed does. For the
+reference layout the knobs of the plan (`sck_plan_tune`) are: the kernel level (generic, lattice, segment, tile),
+the L2 budget of the group pipeline (0 = class by class over all replicas) and the resident limit. For the
+interleaved ('quad') layout they are the class schedule of `sck_plan_pipeline`: class-by-class launches, or the
+L2 pipeline with groups of 4, 8, 16 or 32 replicas and every class skew that divides the class count (the order
+in which the classes of different groups run; a group's own classes always run in sweep order, so the chain is
+unchanged). `autotune(sampler, S)` times every candidate on a scratch copy of the spins with CUDA events, keeps
+the fastest, restores the sweep counter, and caches the choice per (system, batch, mode, device) in a JSON file
+(`$SCK_TUNE_CACHE`, default ~/.cache/spin_colour_kernel_b200/).
 """
 
 from __future__ import annotations
@@ -52,8 +56,59 @@ def _store(d: dict) -> None:
 RESIDENT_LIMIT = 200 << 10
 
 
+QUAD_GROUPS = (4, 8, 16, 32)
+
+
+def quad_candidates(sampler):
+    """(group replicas, skew) pairs of the interleaved layout: (0, 1) = class by class."""
+    C = len(sampler.classes)
+    Q = sampler.Q
+    out = [(0, 1)]
+    for g in QUAD_GROUPS:
+        ngroups = -(-Q // min(g // 4, Q))
+        for d in range(1, C + 1):
+            if C % d == 0 and C <= 8 and d * ngroups >= C:
+                out.append((g, d))
+    return out
+
+
+def _time(sampler, work, sweeps):
+    sampler.sweep(work, 1)                         # warm-up
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stream = torch.cuda.current_stream(sampler.device)
+    a.record(stream)
+    sampler.sweep(work, sweeps)
+    b.record(stream)
+    torch.cuda.synchronize(sampler.device)
+    return a.elapsed_time(b) / sweeps
+
+
+def _autotune_quad(sampler, S, sweeps, use_cache, key, cache):
+    if key in cache:
+        c = cache[key]
+        sampler.pipeline(c["group"], c["skew"])
+        return dict(c, cached=True)
+    saved = sampler.state.clone()
+    work = S.clone()
+    results = []
+    for g, d in quad_candidates(sampler):
+        sampler.pipeline(g, d)
+        results.append((_time(sampler, work, sweeps), g, d))
+    sampler.check_waits()
+    sampler.state.copy_(saved)
+    del work
+    ms, g, d = min(results, key=lambda r: r[0])
+    sampler.pipeline(g, d)
+    choice = {"layout": "quad", "group": g, "skew": d, "ms_per_sweep": ms,
+              "tried": [{"group": r[1], "skew": r[2], "ms": r[0]} for r in results]}
+    if use_cache:
+        cache[key] = choice
+        _store(cache)
+    return dict(choice, cached=False)
+
+
 def candidates(sampler):
-    """(specialised, l2_budget, resident_limit) triples worth timing for this sampler."""
+    """(specialised, l2_budget, resident_limit) triples worth timing for this sampler (reference layout)."""
     out = [(0, 0, 0), (0, 0, RESIDENT_LIMIT)]
     kind = sampler.tune(2, 0, 0)["specialised"] // 100
     for level in range(1, kind + 1):
@@ -65,6 +120,8 @@ def autotune(sampler, S: torch.Tensor, sweeps: int = 3, use_cache: bool = True) 
     """Pick and apply the fastest path for this sampler; returns {"specialised", "l2_budget", "ms", ...}."""
     key = system_key(sampler)
     cache = _load() if use_cache else {}
+    if getattr(sampler, "quad", False):
+        return _autotune_quad(sampler, S, sweeps, use_cache, key, cache)
     if key in cache:
         c = cache[key]
         sampler.tune(c["level"], c["l2_budget"], c["resident_limit"])
@@ -79,14 +136,7 @@ def autotune(sampler, S: torch.Tensor, sweeps: int = 3, use_cache: bool = True) 
         if sig in seen:
             continue
         seen.add(sig)
-        sampler.sweep(work, 1)                         # warm-up
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        stream = torch.cuda.current_stream(sampler.device)
-        a.record(stream)
-        sampler.sweep(work, sweeps)
-        b.record(stream)
-        torch.cuda.synchronize(sampler.device)
-        results.append((a.elapsed_time(b) / sweeps, spec, budget, resident, p))
+        results.append((_time(sampler, work, sweeps), spec, budget, resident, p))
     sampler.state.copy_(saved)
     del work
     ms, spec, budget, resident, p = min(results, key=lambda r: r[0])
@@ -106,4 +156,4 @@ def ms_table(results) -> str:
     return "\n".join(f"spec={r['specialised']} group={r['group']}: {r['ms']:.3f} ms" for r in rows)
 
 
-__all__ = ["autotune", "candidates", "system_key", "ms_table"]
+__all__ = ["autotune", "candidates", "quad_candidates", "system_key", "ms_table"]

@@ -354,6 +354,7 @@ int sck_plan_create(const sck_system_desc* d, int32_t batch, int32_t mode, sck_p
     }
   }
   p->kernel_kind = 1;
+  p->wait_limit = 1u << 20;
   p->l2_budget = 0;
   p->resident_limit = kResidentDefault;
   *out = p;
@@ -400,12 +401,87 @@ int sck_plan_path(const sck_plan* plan, int32_t* specialised, int64_t* l2_budget
     *specialised = plan->spec ? kind * 100 + plan->spec : 0;
   }
   if (l2_budget_bytes) *l2_budget_bytes = plan->l2_budget;
-  if (group) *group = pipeline_group(plan);
+  if (group) *group = plan->mode == SCK_MODE_QUAD ? 4 * plan->quad_group : pipeline_group(plan);
   if (resident) *resident = use_resident(plan) ? 1 : 0;
   return SCK_OK;
 }
 
+int sck_plan_pipeline(sck_plan* plan, int32_t group_replicas, int32_t skew) {
+  if (plan == nullptr) return fail(SCK_ERR_INVALID, "null plan");
+  if (plan->mode != SCK_MODE_QUAD)
+    return fail(SCK_ERR_UNSUPPORTED, "the class-skewed pipeline runs interleaved storage (SCK_MODE_QUAD); "
+                                     "other plans take an L2 budget in sck_plan_tune");
+  if (group_replicas == 0) {
+    plan->quad_group = 0;
+    return SCK_OK;
+  }
+  const int C = plan->desc.n_classes;
+  if (group_replicas < 0 || group_replicas % 4 != 0)
+    return fail(SCK_ERR_INVALID, "pipeline groups hold whole quads: a positive multiple of 4 replicas");
+  if (skew < 1 || skew > C || C % skew != 0 || C > 8)
+    return fail(SCK_ERR_INVALID, "the skew must divide the class count (" + std::to_string(C) + ", at most 8)");
+  const int Q = plan->Bp / 4;
+  const int group = group_replicas / 4 < Q ? group_replicas / 4 : Q;
+  const int ngroups = (Q + group - 1) / group;
+  if ((long long)skew * ngroups <= C - 1)
+    return fail(SCK_ERR_INVALID, "too few replica groups for this skew: a group's next sweep would follow its own "
+                                 "last class too closely (need skew x groups >= classes)");
+  int dev = 0;
+  int rc = cuda_status(cudaGetDevice(&dev), "pipeline set-up");
+  if (rc != SCK_OK) return rc;
+  plan->quad_group = group;
+  const size_t need = quad_pipe_counter_bytes(plan);
+  if (plan->pipe_counters == nullptr || plan->pipe_bytes < need || plan->pipe_device != dev) {
+    if (plan->pipe_counters != nullptr) cudaFree(plan->pipe_counters);
+    plan->pipe_counters = nullptr;
+    plan->pipe_bytes = 0;
+    rc = cuda_status(cudaMalloc(&plan->pipe_counters, need), "pipeline counters");
+    if (rc != SCK_OK) {
+      plan->quad_group = 0;
+      return rc;
+    }
+    plan->pipe_bytes = need;
+    plan->pipe_device = dev;
+  }
+  if (plan->giveup_host == nullptr) {
+    rc = cuda_status(cudaHostAlloc((void**)&plan->giveup_host, sizeof(int), cudaHostAllocMapped), "pipeline flag");
+    if (rc != SCK_OK) {
+      plan->quad_group = 0;
+      return rc;
+    }
+    *plan->giveup_host = 0;
+    rc = cuda_status(cudaHostGetDevicePointer((void**)&plan->giveup_dev, plan->giveup_host, 0), "pipeline flag");
+    if (rc != SCK_OK) {
+      cudaFreeHost(plan->giveup_host);
+      plan->giveup_host = nullptr;
+      plan->quad_group = 0;
+      return rc;
+    }
+  }
+  plan->quad_skew = skew;
+  return SCK_OK;
+}
+
+int sck_plan_set_wait_limit(sck_plan* plan, int64_t polls) {
+  if (plan == nullptr || polls < 1 || polls > 0xFFFFFFFFll) return fail(SCK_ERR_INVALID, "polls must be 1 .. 2^32-1");
+  plan->wait_limit = (unsigned)polls;
+  return SCK_OK;
+}
+
+int sck_plan_wait_status(sck_plan* plan, void* stream) {
+  if (plan == nullptr) return fail(SCK_ERR_INVALID, "null plan");
+  if (plan->giveup_host == nullptr) return SCK_OK;
+  const int rc = cuda_status(cudaStreamSynchronize((cudaStream_t)stream), "wait status");
+  if (rc != SCK_OK) return rc;
+  if (*(volatile int*)plan->giveup_host) {
+    *(volatile int*)plan->giveup_host = 0;
+    return fail(SCK_ERR_TIMEOUT, "a pipeline wait gave up: the affected sites were left unchanged");
+  }
+  return SCK_OK;
+}
+
 int sck_plan_destroy(sck_plan* plan) {
+  if (plan != nullptr && plan->giveup_host != nullptr) cudaFreeHost(plan->giveup_host);
   if (plan != nullptr && plan->pipe_counters != nullptr) cudaFree(plan->pipe_counters);
   delete plan;
   return SCK_OK;
@@ -464,6 +540,18 @@ int sck_sweep(const sck_plan* plan, const sck_buffers* buf, int32_t n_sweeps, vo
   cudaStream_t s = (cudaStream_t)stream;
   if (n_sweeps == 0) return SCK_OK;
   if (plan->mode == SCK_MODE_QUAD) {
+    if (plan->giveup_host != nullptr && *(volatile int*)plan->giveup_host)
+      return fail(SCK_ERR_TIMEOUT, "an earlier pipeline wait of this plan gave up (read sck_plan_wait_status)");
+    if (plan->quad_group > 0) {
+      int dev = -1;
+      rc = cuda_status(cudaGetDevice(&dev), "interleaved pipeline");
+      if (rc != SCK_OK) return rc;
+      if (plan->pipe_device != dev)
+        return fail(SCK_ERR_INVALID, "the pipeline's counters belong to another device: call sck_plan_pipeline here");
+      rc = launch_quad_pipeline(plan, buf, n_sweeps, s, nullptr);
+      if (rc != SCK_OK) return rc;
+      return launch_advance(buf->state, n_sweeps, s);
+    }
     for (int k = 0; k < n_sweeps; ++k) {
       for (int i = 0; i < plan->desc.n_classes; ++i) {
         rc = launch_quad_class(plan, buf, plan->desc.classes[i][0], plan->desc.classes[i][1], s);
@@ -615,6 +703,16 @@ int sck_sweep_measure(const sck_plan* plan, const sck_buffers* buf, int32_t n_sw
   if (plan->batch > 65535) return fail(SCK_ERR_INVALID, "measure step: batch above 65535");
   cudaStream_t s = (cudaStream_t)stream;
   if (plan->mode == SCK_MODE_QUAD && quad_measure_fused(plan)) {
+    if (plan->quad_group > 0) {
+      if (plan->giveup_host != nullptr && *(volatile int*)plan->giveup_host)
+        return fail(SCK_ERR_TIMEOUT, "an earlier pipeline wait of this plan gave up (read sck_plan_wait_status)");
+      int dev = -1;
+      rc = cuda_status(cudaGetDevice(&dev), "interleaved pipeline");
+      if (rc != SCK_OK) return rc;
+      if (plan->pipe_device != dev)
+        return fail(SCK_ERR_INVALID, "the pipeline's counters belong to another device: call sck_plan_pipeline here");
+      return launch_quad_pipeline_measure(plan, buf, n_sweeps, E, M, workspace, s);
+    }
     if (n_sweeps > 1) {
       rc = sck_sweep(plan, buf, n_sweeps - 1, stream);
       if (rc != SCK_OK) return rc;

@@ -124,6 +124,10 @@ struct sck_plan {
   void* pipe_counters;       // device memory of the group pipeline's ticket and completion counters
   size_t pipe_bytes;
   int pipe_device;           // the device that holds them
+  int quad_group, quad_skew; // interleaved pipeline: quads per group (0 = class by class) and class skew
+  unsigned wait_limit;       // polls of a pipeline completion counter before a block gives up
+  int* giveup_host;          // host-mapped flag the pipeline raises when a wait gives up (host view)
+  int* giveup_dev;           //   and its device view
 };
 
 namespace sck {
@@ -166,6 +170,11 @@ int launch_quad_convert(const sck_plan* plan, float* flat, float4* quads, int to
 int quad_obs_blocks(const sck_plan* plan);
 bool quad_measure_fused(const sck_plan* plan);
 size_t quad_measure_workspace(const sck_plan* plan);
+size_t quad_pipe_counter_bytes(const sck_plan* plan);
+int launch_quad_pipeline(const sck_plan* plan, const sck_buffers* buf, int n_sweeps, cudaStream_t s,
+                         double* partial);
+int launch_quad_pipeline_measure(const sck_plan* plan, const sck_buffers* buf, int n_sweeps, double* E, double* M,
+                                 void* workspace, cudaStream_t s);
 int launch_quad_measure_sweep(const sck_plan* plan, const sck_buffers* buf, double* E, double* M, void* workspace,
                               cudaStream_t s);
 int launch_quad_observables(const sck_plan* plan, const void* spins, int batch, const float* k1, double* E, double* M,

@@ -49,12 +49,12 @@ struct MeasureAcc {
 // Residue (0 .. P-1) along x of the class's sites in row (y, z) of the launch's sublattice, or -1 when the row
 // holds none. The colour of a site is K c + o_alpha per factor (mixed radix); stepping x by one adds K[r][0].
 template <int P>
-__device__ __forceinline__ int class_residue(const QuadParams& p, int y, int z) {
+__device__ __forceinline__ int class_residue(const QuadParams& p, int colour, int alpha, int y, int z) {
   int gr[SCK_MAX_FACTORS];
 #pragma unroll
   for (int r = 0; r < SCK_MAX_FACTORS; ++r) {
     if (r < p.col.r) {
-      const uint32_t v = (uint32_t)(p.col.K[r][1] * y + p.col.K[r][2] * z + p.col.o[p.alpha][r]);
+      const uint32_t v = (uint32_t)(p.col.K[r][1] * y + p.col.K[r][2] * z + p.col.o[alpha][r]);
       gr[r] = (int)(v - fdiv(v, p.fd_m[r]) * (uint32_t)p.col.m[r]);
     }
   }
@@ -69,7 +69,7 @@ __device__ __forceinline__ int class_residue(const QuadParams& p, int y, int z) 
         if (gr[r] >= p.col.m[r]) gr[r] -= p.col.m[r];
       }
     }
-    if (idx == p.colour) return q;
+    if (idx == colour) return q;
   }
   return -1;
 }
@@ -268,7 +268,7 @@ __global__ void __launch_bounds__(256, MEASURE ? 2 : 3) quad_class_kernel(const 
   if (row < (uint32_t)(g.L3 * g.L2)) {
     const int z = (int)fdiv(row, p.fd_L2);
     const int y = (int)row - z * g.L2;
-    const int ph = class_residue<P>(p, y, z);
+    const int ph = class_residue<P>(p, p.colour, p.alpha, y, z);
     if (ph >= 0) {
       const int32_t key = sweep_key_at(p.state, p.sweep_offset);
       static_for<0, Lat::b>([&](auto ac) {
@@ -297,6 +297,164 @@ __global__ void __launch_bounds__(256, MEASURE ? 2 : 3) quad_class_kernel(const 
         p.partial[(((size_t)rep * p.n_classes + p.measure_ci) * p.blocks_x + blockIdx.x) * (1 + N) + v] = val;
       }
     }
+  }
+}
+
+// ------------------------------------------------------------------------------------------ L2 pipeline
+// Class-by-class launches read the whole state once per class (every class's neighbours span the other classes)
+// and write it once per sweep. The pipeline runs the classes of a group of quads back to back so that, after
+// the group's first read from HBM, its later classes find it in L2: one launch carries a whole call. Blocks take
+// tickets from a counter in the order they start. Units u = sweep-major groups; class ci of unit u sits at
+// position D u + ci (D, the skew, divides the class count C), so each position holds C / D tasks and about
+// C / D + 1 groups are in flight: D trades overlap between groups against the L2 working set. Within a position,
+// tasks run in increasing class order; a task is T tickets (quads of the group x site blocks of a class). Before
+// touching spins a block waits until every ticket of the task it follows has finished: class ci - 1 of its unit,
+// or class C - 1 of the same group's previous sweep. That task sits at an earlier position, so its tickets were
+// taken earlier by blocks that are running or done, and the wait ends. The waits poll with an iteration limit;
+// a block whose wait gives up skips its sites, counts itself done (so nothing waits forever) and raises the
+// plan's give-up flag, which sck_sweep reports as SCK_ERR_TIMEOUT.
+struct QuadPipeParams {
+  QuadParams p;
+  int C, D, group, ngroups, units, sweep_base, T, Q, blocks_x;
+  int cls[8][2];
+  unsigned* ticket;
+  unsigned* done;           // finished tickets per (group, class), summed over the launch's sweeps
+  unsigned wait_limit;      // polls of a completion counter before giving up
+  int* giveup;              // host-mapped flag, set (system scope) when a wait gives up
+  // measure step: the launch's last sweep also writes FP64 partial sums [replica][class][site block][1 + N]
+  double* partial;
+  unsigned lower_groups[8];
+  int B;
+};
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* a) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(a) : "memory");
+  return v;
+}
+
+struct PipeTask {
+  int go, has, q, ci, sweep, done_idx, chunk;
+};
+
+template <class Lat, int N, int P, int L1C, bool MEASURE>
+__global__ void __launch_bounds__(256, MEASURE ? 2 : 3) quad_pipe_kernel(const __grid_constant__ QuadPipeParams pp) {
+  __shared__ PipeTask s;
+  if (threadIdx.x == 0) {
+    const unsigned tk = atomicAdd(pp.ticket, 1u);
+    const unsigned per_pos = (unsigned)(pp.C / pp.D) * (unsigned)pp.T;
+    const unsigned pos = tk / per_pos;
+    const unsigned rem = tk - pos * per_pos;
+    const int i = (int)(rem / (unsigned)pp.T), j = (int)(rem - (unsigned)i * (unsigned)pp.T);
+    const int ci = (int)(pos % (unsigned)pp.D) + i * pp.D;
+    const int num = (int)pos - ci;
+    s.has = 0;
+    s.go = 0;
+    if (num >= 0 && num / pp.D < pp.units) {
+      const int u = num / pp.D;
+      const int sw = u / pp.ngroups, g = u - sw * pp.ngroups;
+      const int qi = j / pp.blocks_x;
+      s.has = 1;
+      s.q = g * pp.group + qi;
+      s.chunk = j - qi * pp.blocks_x;
+      s.ci = ci;
+      s.sweep = pp.sweep_base + sw;
+      s.done_idx = g * pp.C + ci;
+      const unsigned* dep = nullptr;
+      unsigned need = 0;
+      if (ci > 0) {
+        dep = pp.done + s.done_idx - 1;
+        need = (unsigned)(sw + 1) * (unsigned)pp.T;
+      } else if (sw > 0) {
+        dep = pp.done + g * pp.C + pp.C - 1;
+        need = (unsigned)sw * (unsigned)pp.T;
+      }
+      int go = 1;
+      if (dep != nullptr) {
+        unsigned polls = 0;
+        while (ld_acquire_gpu(dep) < need) {
+          if (++polls > pp.wait_limit) {
+            go = 0;
+            atomicExch_system(pp.giveup, 1);
+            break;
+          }
+          __nanosleep(64);
+        }
+      }
+      s.go = go && s.q < pp.Q;
+    }
+  }
+  __syncthreads();
+  if (!s.has) return;                                   // the pipeline's fill and drain: no task
+  // the measure step's partial sums: the launch's last sweep only (a block-uniform condition)
+  const bool measuring = MEASURE && s.sweep == pp.sweep_base + pp.units / pp.ngroups - 1;
+  MeasureAcc<N> m;
+  if constexpr (MEASURE) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int v = 0; v <= N; ++v) m.v[j][v] = 0.0;
+  }
+  if (s.go) {
+    const QuadParams& p = pp.p;
+    const Geometry& g = p.g;
+    const uint32_t t = (uint32_t)s.chunk * 256u + threadIdx.x;
+    uint32_t row, h;
+    if constexpr (L1C > 0) {
+      row = t / (uint32_t)(L1C / P);
+      h = t - row * (uint32_t)(L1C / P);
+    } else {
+      row = fdiv(t, p.fd_hp);
+      h = t - row * (uint32_t)p.hp;
+    }
+    if (row < (uint32_t)(g.L3 * g.L2)) {
+      const int colour = pp.cls[s.ci][0], alpha = pp.cls[s.ci][1];
+      const int z = (int)fdiv(row, p.fd_L2);
+      const int y = (int)row - z * g.L2;
+      const int ph = class_residue<P>(p, colour, alpha, y, z);
+      if (ph >= 0) {
+        const int32_t key = sweep_key_at(p.state, s.sweep);
+        static_for<0, Lat::b>([&](auto ac) {
+          constexpr int a = decltype(ac)::value;
+          if (a == alpha) {
+            if (measuring) {
+              QuadParams pm = p;
+              pm.lower_groups = pp.lower_groups[s.ci];
+              quad_site<Lat, a, N, P, L1C, MEASURE>(pm, s.q, (int)h, ph, y, z, key, m);
+            } else {
+              quad_site<Lat, a, N, P, L1C, false>(p, s.q, (int)h, ph, y, z, key, m);
+            }
+          }
+        });
+      }
+    }
+  }
+  if constexpr (MEASURE) {
+    if (measuring) {
+      __shared__ double red[4 * (1 + N)][8];
+      double x[4 * (1 + N)];
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int v = 0; v <= N; ++v) x[j * (1 + N) + v] = m.v[j][v];
+      block_sum<4 * (1 + N)>(x, red);
+      if (threadIdx.x < 4 * (1 + N) && s.q < pp.Q) {
+        const int j = threadIdx.x / (1 + N), v = threadIdx.x - j * (1 + N);
+        const int rep = 4 * s.q + j;
+        if (rep < pp.B) {
+          double val = 0.0;
+#pragma unroll
+          for (int i = 0; i < 4 * (1 + N); ++i)
+            if (i == (int)threadIdx.x) val = x[i];
+          pp.partial[(((size_t)rep * pp.C + s.ci) * pp.blocks_x + s.chunk) * (1 + N) + v] = val;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(pp.done + s.done_idx, 1u);   // finished (or given up): later tasks of this group may start
   }
 }
 
@@ -683,6 +841,8 @@ __global__ void __launch_bounds__(128) quad_measure_finish(const double* __restr
 
 // One sweep whose class launches also accumulate the FP64 observables of the configuration it leaves (E and M
 // of the first plan->batch replicas), then the counter advance. Needs quad_measure_fused(plan).
+static int launch_measure_finish(const sck_plan* plan, const void* workspace, double* E, double* M, cudaStream_t s);
+
 int launch_quad_measure_sweep(const sck_plan* plan, const sck_buffers* buf, double* E, double* M, void* workspace,
                               cudaStream_t s) {
   const int C = plan->desc.n_classes;
@@ -700,8 +860,13 @@ int launch_quad_measure_sweep(const sck_plan* plan, const sck_buffers* buf, doub
     const int rc = launch_quad_params(plan, p, s);
     if (rc != SCK_OK) return rc;
   }
-  int rc = launch_advance(buf->state, 1, s);
+  const int rc = launch_advance(buf->state, 1, s);
   if (rc != SCK_OK) return rc;
+  return launch_measure_finish(plan, workspace, E, M, s);
+}
+
+static int launch_measure_finish(const sck_plan* plan, const void* workspace, double* E, double* M, cudaStream_t s) {
+  const int C = plan->desc.n_classes;
   MeasureFinishParams f;
   memset(&f, 0, sizeof(f));
   f.n_classes = C;
@@ -784,6 +949,113 @@ int launch_quad_observables(const sck_plan* plan, const void* spins, int batch, 
   const int rc = cuda_status(cudaGetLastError(), "interleaved observables");
   if (rc != SCK_OK) return rc;
   return launch_observables_finish(p.partial, batch, p.blocks_per_quad, plan->geom.b, plan->geom.n, E, M, s);
+}
+
+// ---------------------------------------------------------------------------------------- pipeline host
+size_t quad_pipe_counter_bytes(const sck_plan* plan) {
+  const int Q = plan->Bp / 4;
+  const int ngroups = (Q + plan->quad_group - 1) / plan->quad_group;
+  return (size_t)(1 + ngroups * plan->desc.n_classes) * sizeof(unsigned);
+}
+
+template <class Lat, int N, int P, int L1C>
+static void launch_pipe_t(const QuadPipeParams& pp, unsigned blocks, cudaStream_t s) {
+  if (pp.partial != nullptr)
+    quad_pipe_kernel<Lat, N, P, L1C, true><<<blocks, 256, 0, s>>>(pp);
+  else
+    quad_pipe_kernel<Lat, N, P, L1C, false><<<blocks, 256, 0, s>>>(pp);
+}
+
+template <class Lat, int N, int P>
+static void launch_pipe_l1(const QuadPipeParams& pp, unsigned blocks, cudaStream_t s) {
+  if (pp.p.g.L1 == 64) launch_pipe_t<Lat, N, P, 64>(pp, blocks, s);
+  else if (pp.p.g.L1 == 32) launch_pipe_t<Lat, N, P, 32>(pp, blocks, s);
+  else if (pp.p.g.L1 == 128) launch_pipe_t<Lat, N, P, 128>(pp, blocks, s);
+  else launch_pipe_t<Lat, N, P, 0>(pp, blocks, s);
+}
+
+template <class Lat>
+static void launch_pipe_lat(const sck_plan* plan, const QuadPipeParams& pp, unsigned blocks, cudaStream_t s) {
+  if (plan->geom.n == 2) {
+    if (plan->P == 1) launch_pipe_l1<Lat, 2, 1>(pp, blocks, s);
+    else launch_pipe_l1<Lat, 2, 2>(pp, blocks, s);
+  } else {
+    if (plan->P == 1) launch_pipe_l1<Lat, 3, 1>(pp, blocks, s);
+    else launch_pipe_l1<Lat, 3, 2>(pp, blocks, s);
+  }
+}
+
+// n sweeps of the pipeline (one launch per chunk of sweeps that keeps the ticket count below 2^30); state[1] is
+// advanced by the caller. The counters are zeroed before every launch. With `partial` (a measure step, which
+// needs quad_measure_fused), the last sweep also writes the measure sweep's partial sums.
+int launch_quad_pipeline(const sck_plan* plan, const sck_buffers* buf, int n_sweeps, cudaStream_t s,
+                         double* partial) {
+  if (plan->pipe_counters == nullptr || plan->giveup_dev == nullptr) {
+    set_error("the interleaved pipeline has no counters: call sck_plan_pipeline on this device");
+    return SCK_ERR_INVALID;
+  }
+  QuadPipeParams pp;
+  memset(&pp, 0, sizeof(pp));
+  pp.p = quad_params(plan, buf, 0, 0);
+  const int C = plan->desc.n_classes;
+  pp.C = C;
+  pp.D = plan->quad_skew;
+  pp.group = plan->quad_group;
+  pp.Q = plan->Bp / 4;
+  pp.ngroups = (pp.Q + pp.group - 1) / pp.group;
+  pp.blocks_x = quad_blocks_x(plan);
+  pp.T = pp.group * pp.blocks_x;
+  for (int ci = 0; ci < C; ++ci) {
+    pp.cls[ci][0] = plan->desc.classes[ci][0];
+    pp.cls[ci][1] = plan->desc.classes[ci][1];
+  }
+  pp.ticket = (unsigned*)plan->pipe_counters;
+  pp.done = pp.ticket + 1;
+  pp.wait_limit = plan->wait_limit;
+  pp.giveup = plan->giveup_dev;
+  pp.B = plan->batch;
+  if (partial != nullptr)
+    for (int ci = 0; ci < C; ++ci)
+      if (!class_lower_groups(plan, ci, &pp.lower_groups[ci])) {
+        set_error("measure sweep: a coupling group mixes earlier and later classes");
+        return SCK_ERR_UNSUPPORTED;
+      }
+  const long long per_pos = (long long)(C / pp.D) * pp.T;
+  const long long units_max = ((1ll << 30) / per_pos - C) / pp.D;
+  const long long sweeps_per_launch = units_max / pp.ngroups;
+  if (sweeps_per_launch < 1) return cuda_status(cudaErrorInvalidConfiguration, "interleaved pipeline: too many tickets");
+  const size_t bytes = quad_pipe_counter_bytes(plan);
+  for (int sw0 = 0; sw0 < n_sweeps; sw0 += (int)sweeps_per_launch) {
+    const int n = (int)((long long)(n_sweeps - sw0) < sweeps_per_launch ? n_sweeps - sw0 : sweeps_per_launch);
+    pp.units = n * pp.ngroups;
+    pp.sweep_base = sw0;
+    pp.partial = (partial != nullptr && sw0 + n == n_sweeps) ? partial : nullptr;
+    int rc = cuda_status(cudaMemsetAsync(plan->pipe_counters, 0, bytes, s), "interleaved pipeline counters");
+    if (rc != SCK_OK) return rc;
+    const long long positions = (long long)pp.D * (pp.units - 1) + C;
+    const unsigned blocks = (unsigned)(positions * per_pos);
+    switch (plan->spec) {
+      case Lat_square_1::id: launch_pipe_lat<Lat_square_1>(plan, pp, blocks, s); break;
+      case Lat_triangular_1::id: launch_pipe_lat<Lat_triangular_1>(plan, pp, blocks, s); break;
+      case Lat_sc_1::id: launch_pipe_lat<Lat_sc_1>(plan, pp, blocks, s); break;
+      case Lat_bcc_1::id: launch_pipe_lat<Lat_bcc_1>(plan, pp, blocks, s); break;
+      case Lat_bcc_1_2::id: launch_pipe_lat<Lat_bcc_1_2>(plan, pp, blocks, s); break;
+      default: launch_pipe_lat<Lat_fcc_1>(plan, pp, blocks, s); break;
+    }
+    rc = cuda_status(cudaGetLastError(), "interleaved pipeline launch");
+    if (rc != SCK_OK) return rc;
+  }
+  return SCK_OK;
+}
+
+// A measure step through the pipeline: n sweeps, the last one measured, the counter advance and the sums.
+int launch_quad_pipeline_measure(const sck_plan* plan, const sck_buffers* buf, int n_sweeps, double* E, double* M,
+                                 void* workspace, cudaStream_t s) {
+  int rc = launch_quad_pipeline(plan, buf, n_sweeps, s, (double*)workspace);
+  if (rc != SCK_OK) return rc;
+  rc = launch_advance(buf->state, n_sweeps, s);
+  if (rc != SCK_OK) return rc;
+  return launch_measure_finish(plan, workspace, E, M, s);
 }
 
 }  // namespace sck

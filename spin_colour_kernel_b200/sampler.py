@@ -158,6 +158,24 @@ class Sampler:
         L.check(L.lib().sck_plan_tune(self._plan, level, int(l2_budget), int(resident_limit)))
         return self.path()
 
+    def pipeline(self, group: int, skew: int = 2):
+        """Interleaved ('quad') layout only: run sweeps through the class-skewed L2 pipeline with groups of
+        `group` replicas (a multiple of 4; 0 returns to class-by-class launches), class c of group-unit u at
+        position skew * u + c (include/sck.h, sck_plan_pipeline). The chain does not depend on it."""
+        with torch.cuda.device(self.device):
+            L.check(L.lib().sck_plan_pipeline(self._plan, int(group), int(skew)))
+        return self.path()
+
+    def set_wait_limit(self, polls: int):
+        """Polls of a pipeline completion counter before a block gives up (failure-detection tests shorten it)."""
+        L.check(L.lib().sck_plan_set_wait_limit(self._plan, int(polls)))
+
+    def check_waits(self):
+        """Synchronise the current stream and raise SckError (SCK_ERR_TIMEOUT) when a pipeline wait of this
+        sampler gave up since the last check (its sites were left unchanged); clears the condition."""
+        with torch.cuda.device(self.device):
+            L.check(L.lib().sck_plan_wait_status(self._plan, self._stream()))
+
     def path(self) -> dict:
         """The sweep path: specialised table id (0 = generic), budget, pipeline group, resident or not."""
         sp, bud, grp, res = ctypes.c_int32(), ctypes.c_int64(), ctypes.c_int32(), ctypes.c_int32()

@@ -249,3 +249,120 @@ def test_measure_step_of_reference_layout_is_sweep_then_observables():
     R.sweep(S2, 2)
     E2, M2 = R.observables(S2)
     assert torch.equal(S1, S2) and torch.equal(E, E2) and torch.equal(M, M2)
+
+
+PIPE_CASES = [
+    ("bcc J1-J2 8^3, 40 replicas, groups of 8, skew 1", lambda: C.heisenberg_bcc_j1j2(sy, cr, 8), 40, 8, 1),
+    ("bcc J1-J2 8^3, 38 replicas, groups of 12, skew 2", lambda: C.heisenberg_bcc_j1j2(sy, cr, 8), 38, 12, 2),
+    ("bcc J1-J2 8^3, 24 replicas, groups of 4, skew 4", lambda: C.heisenberg_bcc_j1j2(sy, cr, 8), 24, 4, 4),
+    ("bcc J1-J2 64x8x8, 16 replicas, groups of 4, skew 2", lambda: sy.System(
+        "Heisenberg bcc", 3, cr.make("bcc", (1, 2)), (64, 8, 8), (True,) * 3, {1: 1.0, 2: 0.3}), 16, 4, 2),
+    ("XY square 32 h, 20 replicas, groups of 4, skew 1", lambda: C.xy_periodic_field(sy, cr, "square", 32), 20, 4,
+     1),
+    ("Heisenberg fcc 4^3, 16 replicas, groups of 4, skew 2", lambda: sy.heisenberg("fcc", 4), 16, 4, 2),
+]
+
+
+@pytest.mark.parametrize("label, make, B, group, skew", PIPE_CASES, ids=[x[0] for x in PIPE_CASES])
+def test_pipeline_equals_class_by_class(label, make, B, group, skew):
+    """The class-skewed L2 pipeline only reorders independent work: spins identical to class-by-class launches,
+    over several calls of several sweeps (partial last groups, padding lanes, every skew that divides the class
+    count)."""
+    s = make()
+    A, R = _quad(s, B, seed=21), _quad(s, B, seed=21)
+    path = A.pipeline(group, skew)
+    assert path["group"] == group
+    for X in (A, R):
+        X.set_temperature(torch.linspace(0.5, 3.0, B))
+    S1, S2 = A.init_spins(seed=8), R.init_spins(seed=8)
+    for n in (1, 3, 2):
+        A.sweep(S1, n)
+        R.sweep(S2, n)
+        assert torch.equal(S1, S2), label
+    A.check_waits()
+    assert int(A.state[1]) == 6
+
+
+def test_pipeline_refuses_bad_groups_and_skews():
+    s = C.heisenberg_bcc_j1j2(sy, cr, 8)          # 4 classes
+    A = _quad(s, 16, seed=1)
+    for group, skew in ((6, 2), (8, 3), (16, 1), (-4, 2)):   # not whole quads, skew not dividing 4, too few groups
+        with pytest.raises(ValueError):
+            A.pipeline(group, skew)
+    from spin_colour_kernel_b200.sampler import Sampler
+    with pytest.raises(ValueError):
+        Sampler(s, 16, device="cuda").pipeline(8, 2)           # the reference layout takes an L2 budget instead
+
+
+def test_pipeline_wait_that_gives_up_reports_timeout():
+    """A wait limit shortened to one poll makes blocks give up instead of waiting for the class they follow: the
+    kernel returns normally (no trap, nothing hangs), the sweep's sites are partly left unchanged, and the plan
+    reports SCK_ERR_TIMEOUT: sck_sweep refuses until the status is read, the status read clears it, and with the
+    default limit restored the pipeline again equals class-by-class launches."""
+    from spin_colour_kernel_b200 import _lib as L
+    s = sy.System("Heisenberg bcc", 3, cr.make("bcc", (1, 2)), (32, 32, 16), (True,) * 3, {1: 1.0, 2: 0.3})
+    A = _quad(s, 32, seed=3)
+    A.pipeline(32, 4)                              # one group, classes strictly in sequence: every class waits
+    A.set_temperature(1.0)
+    S = A.init_spins(seed=1)
+    A.set_wait_limit(1)
+    A.sweep(S, 2)
+    torch.cuda.synchronize()
+    with pytest.raises(L.SckError) as e:
+        A.sweep(S, 1)                              # refused: an earlier wait of this plan gave up
+    assert e.value.code == L.ERR_TIMEOUT
+    with pytest.raises(L.SckError) as e:
+        A.check_waits()
+    assert e.value.code == L.ERR_TIMEOUT
+    A.check_waits()                                # cleared
+    A.set_wait_limit(1 << 20)
+    R = _quad(s, 32, seed=3)
+    R.set_temperature(1.0)
+    X = S.clone()
+    A.state.copy_(R.state)
+    A.sweep(S, 2)
+    R.sweep(X, 2)
+    A.check_waits()
+    assert torch.equal(S, X)
+
+
+@pytest.mark.parametrize("B, group, skew", [(24, 4, 2), (22, 4, 1), (16, 4, 4)])
+def test_pipeline_measure_step_equals_sweeps_then_observables(B, group, skew):
+    """A measure step through the pipeline (its last sweep accumulating the FP64 sums) leaves the chain of
+    class-by-class sweeps and returns the observables of the state it leaves."""
+    s = C.heisenberg_bcc_j1j2(sy, cr, 8)
+    A, R = _quad(s, B, seed=17), _quad(s, B, seed=17)
+    A.pipeline(group, skew)
+    for X in (A, R):
+        X.set_temperature(torch.linspace(0.5, 2.5, B))
+    S1, S2 = A.init_spins(seed=2), R.init_spins(seed=2)
+    for n in (1, 4):
+        E, M = A.sweep_measure(S1, n)
+        R.sweep(S2, n)
+        assert torch.equal(S1, S2)
+        E2, M2 = R.observables(S2)
+        np.testing.assert_allclose(M.cpu().numpy(), M2.cpu().numpy(), rtol=1e-11, atol=1e-9)
+        np.testing.assert_allclose(E.cpu().numpy(), E2.cpu().numpy(), rtol=2e-6, atol=1e-5 * s.n_active)
+    A.check_waits()
+
+
+def test_autotuned_schedule_is_bit_identical_and_cached(tmp_path, monkeypatch):
+    """The autotuner times class-by-class launches against every pipeline group and class skew, applies the
+    fastest, caches it per system, and the tuned path leaves the chain of the default path."""
+    from spin_colour_kernel_b200 import autotune as at
+    monkeypatch.setenv("SCK_TUNE_CACHE", str(tmp_path / "tune.json"))
+    s = C.heisenberg_bcc_j1j2(sy, cr, 16)
+    A, R = _quad(s, 64, seed=31), _quad(s, 64, seed=31)
+    for X in (A, R):
+        X.set_temperature(torch.linspace(0.5, 2.5, 64))
+    S1, S2 = A.init_spins(seed=1), R.init_spins(seed=1)
+    c = at.autotune(A, S1, sweeps=2)
+    assert not c["cached"] and len(c["tried"]) == len(at.quad_candidates(A)) > 4
+    assert int(A.state[1]) == 0                        # the counter is restored
+    A.sweep(S1, 3)
+    R.sweep(S2, 3)
+    assert torch.equal(S1, S2)
+    B = _quad(s, 64, seed=31)
+    c2 = at.autotune(B, B.init_spins(seed=1))
+    assert c2["cached"] and (c2["group"], c2["skew"]) == (c["group"], c["skew"])
+    assert B.path()["group"] == c["group"]
