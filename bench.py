@@ -271,7 +271,7 @@ def reference_triton_arm(args, rank, world):
     line = {**base, "value": value, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"heisenberg-bcc-{L}^3x2-J1J2-K1-hz", "replicas": B, "sites": s.nsite,
+            "config": {"workload": f"heisenberg-bcc-{L}^3x2-J1J2-K1-hz", "replicas": B, "sites": 2 * L ** 3,
                        "path": "reference Sampler.graph(S, 1) replays (generated Triton class kernels)",
                        "python_packages_loaded": loaded},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

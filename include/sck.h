@@ -173,10 +173,14 @@ int sck_plan_path(const sck_plan* plan, int32_t* specialised, int64_t* l2_budget
  * Errors: SCK_ERR_UNSUPPORTED for other plans; SCK_ERR_INVALID for a group that is not whole quads, a skew that
  * does not divide the class count, or too few groups for the skew (skew x groups must reach the class count).
  *
- * The pipeline's blocks wait for the class they follow with an iteration limit (sck_plan_set_wait_limit, default
- * 2^20 polls, about a second); a block whose wait gives up leaves its sites unchanged and raises the plan's flag.
- * sck_plan_wait_status synchronises `stream` and returns SCK_ERR_TIMEOUT (clearing the flag) when a wait of this
- * plan gave up since the last status read; until then sck_sweep of the plan refuses with SCK_ERR_TIMEOUT. */
+ * Bounded waits. Every device-side wait of a plan's kernels has an iteration limit (sck_plan_set_wait_limit,
+ * default 2^20 polls, about a second; 0 makes every wait that is not already satisfied give up at once, which
+ * failure-detection tests use): the pipelines' blocks waiting for the class they follow (this call and the
+ * L2 budget of sck_plan_tune) and the tile kernels waiting for their bulk copies (sck_plan_tune level 3). A block
+ * whose wait gives up leaves its sites unchanged and raises the plan's host-mapped flag (allocated when such a
+ * path is chosen). sck_plan_wait_status synchronises `stream` and returns SCK_ERR_TIMEOUT (clearing the flag)
+ * when a wait of this plan gave up since the last status read; until then sck_sweep and sck_sweep_measure of the
+ * plan refuse with SCK_ERR_TIMEOUT. */
 int sck_plan_pipeline(sck_plan* plan, int32_t group_replicas, int32_t skew);
 int sck_plan_set_wait_limit(sck_plan* plan, int64_t polls);
 int sck_plan_wait_status(sck_plan* plan, void* stream);

@@ -2,8 +2,10 @@
  *
  * No counterpart in the reference, which has no learned part. A masked autoregressive MLP (MADE) proposes a joint
  * update of a 4x4x4 block of spins conditioned on its 96 boundary spins; the proposal's exact density enters a
- * Metropolis-Hastings ratio, so the Boltzmann distribution is kept. Blocks are coloured by the parities of their
- * block coordinates (8 colours); a colour step updates every block of one colour in every replica at once.
+ * Metropolis-Hastings ratio, so the Boltzmann distribution is kept. A colour step updates every block of one
+ * parity class of the block coordinates (code px + 2 py + 4 pz) in every replica at once; the host orders these
+ * classes by the block colouring it finds with the site colouring's search (8 colours: blocks touching at a
+ * face, an edge or a corner differ).
  *
  * Conventions as in sck.h: caller-owned device buffers, every call asynchronous on the stream passed as void*,
  * no allocation and no synchronisation inside a call, 0 or a negative SCK_ERR_* status with sck_last_error().
@@ -74,6 +76,15 @@ int sck_made_train_step(void* params, float* adam, int32_t groups, const uint16_
 int sck_made_colour_step(const void* params, int32_t groups, int8_t* spins, int32_t R, int32_t L, const float* beta,
                          int32_t colour, int64_t seed, int32_t round, int32_t* accepted, void* record,
                          void* stream);
+
+/* Bounded waits. The tensor-core forward GEMM (training and sck_made_forward, 128-row batches) waits on its
+ * stages' mbarriers with an iteration limit (default 2^22 polls; sck_made_set_wait_limit sets it on the current
+ * device, synchronously; 0 makes every stage wait give up at once, for failure-detection tests). A block whose
+ * wait gives up waits for its products in flight, leaves its output rows unwritten and counts itself;
+ * sck_made_wait_status synchronises `stream` and returns SCK_ERR_TIMEOUT when a wait on the current device gave
+ * up since its last status read. */
+int sck_made_set_wait_limit(int64_t polls);
+int sck_made_wait_status(void* stream);
 
 #ifdef __cplusplus
 }

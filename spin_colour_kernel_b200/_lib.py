@@ -89,6 +89,8 @@ _SIGNATURES = {
     "sck_made_grads": ([_vp, _i32, _vp, _i32, _vp, _vp, _vp, _vp], _i32),
     "sck_made_train_step": ([_vp, _vp, _i32, _vp, _i32, _f32, _f32, _f32, _f32, _i32, _vp, _vp, _vp], _i32),
     "sck_made_colour_step": ([_vp, _i32, _vp, _i32, _i32, _vp, _i32, _i64, _i32, _vp, _vp, _vp], _i32),
+    "sck_made_set_wait_limit": ([_i64], _i32),
+    "sck_made_wait_status": ([_vp], _i32),
 }
 
 EXPORTS = tuple(_SIGNATURES)

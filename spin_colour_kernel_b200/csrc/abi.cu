@@ -62,6 +62,8 @@ static Common make_common(const sck_plan* plan, const sck_buffers* buf, const vo
   c.beta = buf->beta;
   c.table = buf->table;
   c.state = buf->state;
+  c.giveup = plan->giveup_dev;
+  c.wait_limit = plan->wait_limit;
   c.fd_bx = make_fastdiv((uint32_t)c.bx);
   c.fd_L1 = make_fastdiv((uint32_t)c.g.L1);
   c.fd_L2 = make_fastdiv((uint32_t)c.g.L2);
@@ -361,6 +363,27 @@ int sck_plan_create(const sck_system_desc* d, int32_t batch, int32_t mode, sck_p
   return SCK_OK;
 }
 
+// The plan's give-up flag: 4 bytes of mapped, portable pinned host memory that kernels with bounded waits (the
+// tile kernels' bulk-copy waits, the group pipelines' completion-counter waits) raise when a wait gives up.
+// Allocated once, on the first choice of such a path, never inside a sweep.
+static int ensure_giveup_flag(sck_plan* plan) {
+  if (plan->giveup_host != nullptr) return SCK_OK;
+  int rc = cuda_status(cudaHostAlloc((void**)&plan->giveup_host, sizeof(int),
+                                     cudaHostAllocMapped | cudaHostAllocPortable), "give-up flag");
+  if (rc != SCK_OK) {
+    plan->giveup_host = nullptr;
+    return rc;
+  }
+  *plan->giveup_host = 0;
+  rc = cuda_status(cudaHostGetDevicePointer((void**)&plan->giveup_dev, plan->giveup_host, 0), "give-up flag");
+  if (rc != SCK_OK) {
+    cudaFreeHost(plan->giveup_host);
+    plan->giveup_host = nullptr;
+    plan->giveup_dev = nullptr;
+  }
+  return rc;
+}
+
 int sck_plan_tune(sck_plan* plan, int32_t specialised, int64_t l2_budget_bytes, int64_t resident_limit_bytes) {
   if (plan == nullptr || l2_budget_bytes < 0 || resident_limit_bytes < 0)
     return fail(SCK_ERR_INVALID, "null plan or negative budget");
@@ -369,6 +392,10 @@ int sck_plan_tune(sck_plan* plan, int32_t specialised, int64_t l2_budget_bytes, 
   plan->kernel_kind = specialised >= 3 ? 3 : (specialised >= 2 ? 2 : 1);
   plan->l2_budget = l2_budget_bytes;
   plan->resident_limit = resident_limit_bytes;
+  if (plan->kernel_kind == 3 || pipeline_group(plan) > 0) {
+    const int rc = ensure_giveup_flag(plan);
+    if (rc != SCK_OK) return rc;
+  }
   // the group pipeline's counters live on the current device, allocated here (never inside a sweep)
   const int group = pipeline_group(plan);
   if (group > 0 && !use_resident(plan)) {
@@ -443,27 +470,17 @@ int sck_plan_pipeline(sck_plan* plan, int32_t group_replicas, int32_t skew) {
     plan->pipe_bytes = need;
     plan->pipe_device = dev;
   }
-  if (plan->giveup_host == nullptr) {
-    rc = cuda_status(cudaHostAlloc((void**)&plan->giveup_host, sizeof(int), cudaHostAllocMapped), "pipeline flag");
-    if (rc != SCK_OK) {
-      plan->quad_group = 0;
-      return rc;
-    }
-    *plan->giveup_host = 0;
-    rc = cuda_status(cudaHostGetDevicePointer((void**)&plan->giveup_dev, plan->giveup_host, 0), "pipeline flag");
-    if (rc != SCK_OK) {
-      cudaFreeHost(plan->giveup_host);
-      plan->giveup_host = nullptr;
-      plan->quad_group = 0;
-      return rc;
-    }
+  rc = ensure_giveup_flag(plan);
+  if (rc != SCK_OK) {
+    plan->quad_group = 0;
+    return rc;
   }
   plan->quad_skew = skew;
   return SCK_OK;
 }
 
 int sck_plan_set_wait_limit(sck_plan* plan, int64_t polls) {
-  if (plan == nullptr || polls < 1 || polls > 0xFFFFFFFFll) return fail(SCK_ERR_INVALID, "polls must be 1 .. 2^32-1");
+  if (plan == nullptr || polls < 0 || polls > 0xFFFFFFFFll) return fail(SCK_ERR_INVALID, "polls must be 0 .. 2^32-1");
   plan->wait_limit = (unsigned)polls;
   return SCK_OK;
 }
@@ -475,7 +492,8 @@ int sck_plan_wait_status(sck_plan* plan, void* stream) {
   if (rc != SCK_OK) return rc;
   if (*(volatile int*)plan->giveup_host) {
     *(volatile int*)plan->giveup_host = 0;
-    return fail(SCK_ERR_TIMEOUT, "a pipeline wait gave up: the affected sites were left unchanged");
+    return fail(SCK_ERR_TIMEOUT, "a bounded wait of this plan's kernels gave up: the affected sites were left "
+                                 "unchanged");
   }
   return SCK_OK;
 }
@@ -539,9 +557,9 @@ int sck_sweep(const sck_plan* plan, const sck_buffers* buf, int32_t n_sweeps, vo
   if (n_sweeps < 0) return fail(SCK_ERR_INVALID, "negative sweep count");
   cudaStream_t s = (cudaStream_t)stream;
   if (n_sweeps == 0) return SCK_OK;
+  if (plan->giveup_host != nullptr && *(volatile int*)plan->giveup_host)
+    return fail(SCK_ERR_TIMEOUT, "an earlier bounded wait of this plan gave up (read sck_plan_wait_status)");
   if (plan->mode == SCK_MODE_QUAD) {
-    if (plan->giveup_host != nullptr && *(volatile int*)plan->giveup_host)
-      return fail(SCK_ERR_TIMEOUT, "an earlier pipeline wait of this plan gave up (read sck_plan_wait_status)");
     if (plan->quad_group > 0) {
       int dev = -1;
       rc = cuda_status(cudaGetDevice(&dev), "interleaved pipeline");
@@ -702,10 +720,10 @@ int sck_sweep_measure(const sck_plan* plan, const sck_buffers* buf, int32_t n_sw
   if (workspace == nullptr) return fail(SCK_ERR_INVALID, "null workspace (see sck_sweep_measure_workspace_size)");
   if (plan->batch > 65535) return fail(SCK_ERR_INVALID, "measure step: batch above 65535");
   cudaStream_t s = (cudaStream_t)stream;
+  if (plan->giveup_host != nullptr && *(volatile int*)plan->giveup_host)
+    return fail(SCK_ERR_TIMEOUT, "an earlier bounded wait of this plan gave up (read sck_plan_wait_status)");
   if (plan->mode == SCK_MODE_QUAD && quad_measure_fused(plan)) {
     if (plan->quad_group > 0) {
-      if (plan->giveup_host != nullptr && *(volatile int*)plan->giveup_host)
-        return fail(SCK_ERR_TIMEOUT, "an earlier pipeline wait of this plan gave up (read sck_plan_wait_status)");
       int dev = -1;
       rc = cuda_status(cudaGetDevice(&dev), "interleaved pipeline");
       if (rc != SCK_OK) return rc;

@@ -200,7 +200,6 @@ __global__ void __launch_bounds__(256) spec_task_kernel(const __grid_constant__ 
 // as class launches are, tasks of different groups overlap freely, and a group's state is read from HBM once
 // per sweep while its C classes pass over it from L2.
 constexpr int kStreamSiteBlocks = 1;                 // site blocks of 256 threads per ticket
-constexpr unsigned kStreamWaitLimit = 1u << 22;      // polls of a completion counter before giving up
 static __device__ unsigned long long g_stream_wait_timeouts;
 
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* a) {
@@ -253,9 +252,10 @@ __global__ void __launch_bounds__(256, 5) stream_kernel(const __grid_constant__ 
       if (dep != nullptr) {
         unsigned polls = 0;
         while (ld_acquire_u32(dep) < need) {
-          if (++polls > kStreamWaitLimit) {
+          if (++polls > p.c.wait_limit) {
             go = 0;
             atomicAdd(&g_stream_wait_timeouts, 1ull);
+            if (p.c.giveup != nullptr) atomicExch_system(p.c.giveup, 1);
             break;
           }
           __nanosleep(100);

@@ -30,6 +30,8 @@ struct Common {
   const float* beta;
   const void* table;
   const int64_t* state;
+  int* giveup;       // the plan's host-mapped flag, raised (system scope) when a bounded wait gives up; may be null
+  unsigned wait_limit;  // polls of a bounded wait before it gives up
   FastDiv fd_bx, fd_L1, fd_L2, fd_m[SCK_MAX_FACTORS];
 };
 
@@ -126,7 +128,7 @@ struct sck_plan {
   int pipe_device;           // the device that holds them
   int quad_group, quad_skew; // interleaved pipeline: quads per group (0 = class by class) and class skew
   unsigned wait_limit;       // polls of a pipeline completion counter before a block gives up
-  int* giveup_host;          // host-mapped flag the pipeline raises when a wait gives up (host view)
+  int* giveup_host;          // host-mapped flag a kernel raises when a bounded wait gives up (host view)
   int* giveup_dev;           //   and its device view
 };
 
@@ -143,7 +145,8 @@ int launch_bitwise_sequential(const sck_plan* plan, const Common& c, cudaStream_
 int obs_blocks_per_rep(const sck_plan* plan, int batch);
 int obs_launch_blocks(const sck_plan* plan, int storage, int batch);
 int check_observables_request(const sck_plan* plan, int storage, int batch);
-int made_wait_timeouts(unsigned long long* count);   // bounded waits of the learned proposal's kernels that gave up
+int made_wait_timeouts(unsigned long long* count);
+int made_set_wait_limit(long long polls);   // polls before the tensor-core GEMM's stage waits give up   // bounded waits of the learned proposal's kernels that gave up
 int launch_observables(const sck_plan* plan, const void* spins, int storage, int batch, const int8_t* mask,
                        const float* k1, double* E, double* M, void* workspace, cudaStream_t s);
 int launch_observables_finish(const double* partial, int B, int blocks_per_rep, int b, int n, double* E, double* M,

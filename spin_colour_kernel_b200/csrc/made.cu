@@ -240,6 +240,9 @@ constexpr int UKC = 32;     // K per staged chunk (two K16 MMAs)
 constexpr long long kUmmaWaitLimit = 1ll << 22;
 
 static __device__ unsigned long long g_made_wait_timeouts;
+// polls of a stage's mbarrier before the forward GEMM gives up (sck_made_set_wait_limit; the drain after a give-up
+// always keeps kUmmaWaitLimit, so that no product is in flight when the block frees its tensor memory)
+static __device__ long long g_made_wait_limit = kUmmaWaitLimit;
 
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
   uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
@@ -310,8 +313,8 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(GemmArgs g) {
     const uint32_t mb = b ? mb1 : mb0;
     long long polls = 0;
     bool done = false;
-    while (!(done = umma_try_wait(mb, ph[b])) && ++polls < kUmmaWaitLimit) {
-    }
+    const long long limit = g_made_wait_limit;
+    while (polls < limit && !(done = umma_try_wait(mb, ph[b]))) ++polls;
     ph[b] ^= 1u;
     return !__syncthreads_or(!done);
   };
@@ -406,6 +409,10 @@ constexpr int umma_smem() { return 2 * (UM + N) * UKC * 2 + 16 + 16; }
 
 int made_wait_timeouts(unsigned long long* v) {
   return cuda_status(cudaMemcpyFromSymbol(v, made::g_made_wait_timeouts, sizeof(*v)), "learned wait timeouts");
+}
+
+int made_set_wait_limit(long long polls) {
+  return cuda_status(cudaMemcpyToSymbol(made::g_made_wait_limit, &polls, sizeof(polls)), "learned wait limit");
 }
 
 namespace made {
@@ -1041,6 +1048,31 @@ static int made_fail(int code, const char* msg) {
 static bool groups_ok(int G) { return G == 16 || G == 64; }
 
 extern "C" {
+
+int sck_made_set_wait_limit(int64_t polls) {
+  if (polls < 0) return made_fail(SCK_ERR_INVALID, "polls must not be negative");
+  return made_set_wait_limit((long long)polls);
+}
+
+int sck_made_wait_status(void* stream) {
+  // give-ups counted on the current device since its last status read
+  static unsigned long long seen[64];
+  int dev = 0;
+  int rc = cuda_status(cudaGetDevice(&dev), "learned wait status");
+  if (rc != SCK_OK) return rc;
+  rc = cuda_status(cudaStreamSynchronize((cudaStream_t)stream), "learned wait status");
+  if (rc != SCK_OK) return rc;
+  unsigned long long now = 0;
+  rc = made_wait_timeouts(&now);
+  if (rc != SCK_OK) return rc;
+  if (dev < 0 || dev >= 64) return SCK_OK;
+  if (now != seen[dev]) {
+    seen[dev] = now;
+    return made_fail(SCK_ERR_TIMEOUT, "a bounded wait of the learned proposal's tensor-core GEMM gave up: its "
+                                      "output rows were left unwritten");
+  }
+  return SCK_OK;
+}
 
 int sck_made_sizes(int32_t groups, int32_t batch, int64_t* param_bytes, int64_t* adam_bytes, int64_t* train_bytes) {
   if (!groups_ok(groups)) return made_fail(SCK_ERR_INVALID, "groups must be 16 or 64");

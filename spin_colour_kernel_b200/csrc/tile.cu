@@ -17,7 +17,7 @@ namespace sck {
 
 constexpr int BR_Y = 4;       // rows per brick
 constexpr int TILE_PAD = 4;   // floats before x = 0 in a shared row: x = -1 sits at TILE_PAD - 1
-constexpr long long kBrickWaitLimit = 1ll << 22;   // mbarrier polls before a brick gives up
+constexpr long long kBrickWaitLimit = 1ll << 22;   // mbarrier polls of the drain after a brick gave up
 
 template <class Lat, int N, int L1T, int BZ>
 struct BrickDims {
@@ -154,12 +154,14 @@ __global__ void __launch_bounds__(256) brick_class_kernel(const __grid_constant_
   }
   long long polls = 0;
   bool ready = false;
-  while (!(ready = mbar_try_wait(mbar, 0)) && ++polls < kBrickWaitLimit) {
-  }
+  while (polls < (long long)c.wait_limit && !(ready = mbar_try_wait(mbar, 0))) ++polls;
   if (__syncthreads_or(!ready)) {
-    // gave up (every thread of the block agrees): count it, wait (bounded again) for the copies still in
-    // flight, leave the brick unchanged
-    if (threadIdx.x == 0) atomicAdd(&g_wait_timeouts, 1ull);
+    // gave up (every thread of the block agrees): count it, raise the plan's flag, wait (bounded again, with the
+    // full limit) for the copies still in flight, leave the brick unchanged
+    if (threadIdx.x == 0) {
+      atomicAdd(&g_wait_timeouts, 1ull);
+      if (c.giveup != nullptr) atomicExch_system(c.giveup, 1);
+    }
     for (long long i = 0; i < kBrickWaitLimit && !mbar_try_wait(mbar, 0); ++i) {
     }
     return;

@@ -3,9 +3,12 @@
 No counterpart in the reference. A masked autoregressive MLP (MADE: 160 -> 256 -> 256 -> 256 -> 64, ReLU,
 bfloat16 weights and activations, FP32 accumulation on tensor cores) proposes a joint update of a 4x4x4 block
 conditioned on its 96 boundary spins; the proposal's exact density enters a Metropolis-Hastings ratio, so the
-chain keeps the Boltzmann distribution whatever the network has learned. Blocks are coloured by the parities of
-their block coordinates (8 colours); `round` runs the 8 colour steps, after which the caller interleaves plain
-colour sweeps (`Sampler.sweep`) on the same int8 spins.
+chain keeps the Boltzmann distribution whatever the network has learned. Blocks are coloured the way the sites of
+a system are: `block_colouring` runs the colouring search on the graph of blocks (two blocks interact when they
+touch at a face, an edge or a corner), verifies it bond by bond on the periodic block box and certifies it against
+the clique number; blocks of one colour share no bond and neither touches another's boundary, so a colour step
+updates them all at once. `round` runs one colour step per colour in the colouring's order, after which the caller
+interleaves plain colour sweeps (`Sampler.sweep`) on the same int8 spins.
 
 `BlockProposal.train` fits the network on block inputs gathered from configurations of the plain chain
 (`gather`), with the library's own forward and backward kernels and Adam. Everything runs on the GPU through
@@ -28,6 +31,38 @@ SHAPES = [((256, 160), (256,)), ((256, 256), (256,)), ((256, 256), (256,)), ((64
 
 def _ptr(t) -> int | None:
     return None if t is None else t.data_ptr()
+
+
+def block_colouring(nb: int):
+    """(colouring, parity code per colour) of the nb^3 periodic lattice of 4x4x4 blocks.
+
+    The block graph is the simple cubic lattice of blocks with its first three shells (face, edge and corner
+    neighbours), and its colouring is found by the same search as a system's site colouring
+    (`colouring.search`, first admissible linear colouring by increasing colour count), then checked bond by bond
+    on the box and against the clique number (the 2x2x2 cube of blocks is a clique of 8). The colour-step kernel
+    addresses the blocks of a class by the parities of their block coordinates, code px + 2 py + 4 pz; every
+    class must therefore be one parity coset, which is checked here."""
+    from . import colouring as co
+    from . import crystals as cr
+    if nb < 2 or nb % 2:
+        raise ValueError("the block lattice needs an even number of blocks per axis")
+    crystal = cr.make("sc", (1, 2, 3))
+    box, per = (nb, nb, nb), (True, True, True)
+    col = co.search(crystal, box, per)
+    if col is None or not co.verify_on_box(col, crystal, box, per):
+        raise ValueError("no verified block colouring of the block lattice")
+    if col.n_colours != co.clique_number(crystal):
+        raise ValueError(f"block colouring of {col.n_colours} colours is not optimal")
+    grid = col.colour_grid(0, box)                      # (z, y, x)
+    z, y, x = np.meshgrid(np.arange(nb), np.arange(nb), np.arange(nb), indexing="ij")
+    parity = (x % 2) + 2 * (y % 2) + 4 * (z % 2)
+    codes = []
+    for c in range(col.n_colours):
+        p = np.unique(parity[grid == c])
+        if p.size != 1 or np.any(grid[parity == p[0]] != c):
+            raise ValueError("a block colour class is not a parity class of the block coordinates")
+        codes.append(int(p[0]))
+    return col, codes
 
 
 def kaiming_params(seed: int = 0):
@@ -70,6 +105,7 @@ class BlockProposal:
         self.device = torch.device("cuda", dev.index if dev.index is not None else torch.cuda.current_device())
         self.L, self.R, self.groups = int(L), int(R), int(groups)
         self.nb = self.L // 4
+        self.block_colouring, self.colour_codes = block_colouring(self.nb)
         pb, ab = ctypes.c_int64(), ctypes.c_int64()
         abi.check(abi.lib().sck_made_sizes(self.groups, 64, ctypes.byref(pb), ctypes.byref(ab), None))
         self.params = torch.zeros(pb.value, dtype=torch.uint8, device=self.device)
@@ -124,7 +160,20 @@ class BlockProposal:
         with torch.cuda.device(self.device):
             abi.check(abi.lib().sck_made_forward(_ptr(self.params), self.groups, _ptr(x.contiguous()), n,
                                                  _ptr(logits), _ptr(logq), _ptr(self._workspace(n)), self._stream()))
+        self.check_waits()
         return logits, logq
+
+    def check_waits(self) -> None:
+        """Synchronise the current stream and raise SckError (SCK_ERR_TIMEOUT) when a bounded wait of the
+        tensor-core GEMM gave up on this device since the last check (its output rows were left unwritten)."""
+        with torch.cuda.device(self.device):
+            abi.check(abi.lib().sck_made_wait_status(self._stream()))
+
+    def set_wait_limit(self, polls: int) -> None:
+        """Polls of a GEMM stage's mbarrier before a block gives up, on this device (failure-detection tests
+        shorten it; the default is 2^22)."""
+        with torch.cuda.device(self.device):
+            abi.check(abi.lib().sck_made_set_wait_limit(int(polls)))
 
     def grads(self, x: torch.Tensor):
         """(loss, [(dW, db)] as float32 NumPy) of the mean negative log-density of rows x."""
@@ -161,12 +210,14 @@ class BlockProposal:
                 abi.check(abi.lib().sck_made_train_step(_ptr(self.params), _ptr(self.adam), self.groups, _ptr(xb),
                                                         batch, lr, betas[0], betas[1], eps, self.t,
                                                         _ptr(losses[i:i + 1]), _ptr(ws), self._stream()))
+        self.check_waits()
         return losses.cpu().numpy()
 
     # ------------------------------------------------------------------ sampling
     def colour_step(self, spins: torch.Tensor, beta: torch.Tensor, colour: int, seed: int, rnd: int,
                     accepted: torch.Tensor | None = None, record: torch.Tensor | None = None) -> None:
-        """One colour step in place on int8 spins of this proposal's R replicas (beta: FP32 per replica)."""
+        """One colour step in place on int8 spins of this proposal's R replicas (beta: FP32 per replica); `colour`
+        is the class's parity code (px + 2 py + 4 pz of its blocks' coordinates)."""
         with torch.cuda.device(self.device):
             abi.check(abi.lib().sck_made_colour_step(_ptr(self.params), self.groups, _ptr(spins), self.R, self.L,
                                                      _ptr(beta), int(colour), int(seed), int(rnd), _ptr(accepted),
@@ -174,9 +225,9 @@ class BlockProposal:
 
     def round(self, spins: torch.Tensor, beta: torch.Tensor, seed: int, rnd: int,
               accepted: torch.Tensor | None = None) -> None:
-        """The 8 colour steps of block round `rnd`."""
-        for c in range(8):
-            self.colour_step(spins, beta, c, seed, rnd, accepted)
+        """The colour steps of block round `rnd`, one per colour of the block colouring, in its order."""
+        for code in self.colour_codes:
+            self.colour_step(spins, beta, code, seed, rnd, accepted)
 
     def record_buffer(self) -> torch.Tensor:
         """A record buffer for colour_step: 80 bytes per (replica, block of the colour)."""

@@ -188,10 +188,14 @@ def test_colour_step_matches_oracle(groups, L):
     assert 0 < total_acc                      # some proposals are accepted at these temperatures
 
 
+ROUNDS = 1500
+
+
 def test_learned_rounds_keep_the_boltzmann_distribution():
-    """Plain sweeps alone and plain sweeps interleaved with learned rounds give the same mean energy and |M| on an
-    8^3 periodic lattice at T = 4.5115. The network is trained briefly on the plain chain's blocks, so proposals
-    are accepted often enough for the MH correction to matter."""
+    """Plain sweeps alone and plain sweeps interleaved with learned rounds give the same mean energy and |M|, within
+    2 sigma (sigma from tau_int of each series), on an 8^3 periodic lattice at T = 4.5115. The network is
+    trained briefly on the plain chain's blocks, so proposals are accepted often enough for the MH correction to
+    matter."""
     _need_gpu()
     from spin_colour_kernel_b200 import system as sy
     from spin_colour_kernel_b200.learned import BlockProposal
@@ -216,7 +220,7 @@ def test_learned_rounds_keep_the_boltzmann_distribution():
                 data.append(P.gather(S))
             P.train(torch.cat(data), steps=300, batch=2048, lr=2e-3)
         Es, Ms = [], []
-        for r in range(600):
+        for r in range(ROUNDS):
             if P is not None:
                 P.round(S, beta, seed=5, rnd=r, accepted=acc)
             A.sweep(S, 1)
@@ -232,8 +236,49 @@ def test_learned_rounds_keep_the_boltzmann_distribution():
             err = series.std() * np.sqrt(2 * tau / series.size)
             res[arm].append((mean, err))
         if P is not None:
-            res["acceptance"] = acc.sum().item() / (600 * R * (L // 4) ** 3)
+            res["acceptance"] = acc.sum().item() / (ROUNDS * R * (L // 4) ** 3)
     for k in range(2):
         (m1, e1), (m2, e2) = res["plain"][k], res["learned"][k]
-        assert abs(m1 - m2) < 4 * np.hypot(e1, e2), (k, res)
+        assert abs(m1 - m2) < 2 * np.hypot(e1, e2), (k, res)
     assert res["acceptance"] > 0.0
+
+
+def test_trained_network_decorrelates_faster_than_untrained():
+    """What training gains. On a 16^3 lattice at T = 4.5115, block rounds (one colour step per block colour,
+    then one plain sweep) with a network trained on the plain chain's blocks are accepted far more often and
+    decorrelate |M| faster (smaller tau_int, Sokal window over 128 chains) than the same rounds with the
+    untrained network, whose proposals are almost never accepted (its rounds are plain sweeps in all but name)."""
+    _need_gpu()
+    from spin_colour_kernel_b200 import stats
+    from spin_colour_kernel_b200 import system as sy
+    from spin_colour_kernel_b200.learned import BlockProposal
+    from spin_colour_kernel_b200.sampler import Sampler
+    L, R, T, K = 16, 128, 4.5115, 1500
+    s = sy.ising("sc", L)
+    A = Sampler(s, R, device="cuda", seed=31, packed=False)
+    A.set_temperature(torch.full((R,), T))
+    S = A.init_spins(seed=4)
+    A.sweep(S, 500)
+    beta = torch.full((R,), 1.0 / T, dtype=torch.float32, device="cuda")
+    trained = BlockProposal(L, R, groups=16, seed=9)
+    data = []
+    for _ in range(8):
+        A.sweep(S, 25)
+        data.append(trained.gather(S))
+    trained.train(torch.cat(data), steps=600, batch=4096, lr=2e-3)
+    untrained = BlockProposal(L, R, groups=16, seed=9)
+    out = {}
+    for name, P in (("trained", trained), ("untrained", untrained)):
+        X = S.clone()
+        acc = torch.zeros(R, dtype=torch.int32, device="cuda")
+        Ms = torch.empty((K, R), dtype=torch.float64, device="cuda")
+        for r in range(K):
+            P.round(X, beta, seed=13, rnd=r, accepted=acc)
+            A.sweep(X, 1)
+            _, M = A.observables(X)
+            Ms[r].copy_(M.reshape(R).abs())
+        series = Ms.cpu().numpy() / L ** 3
+        out[name] = (stats.integrated_tau(series), acc.sum().item() / (K * R * (L // 4) ** 3))
+    (tau_t, acc_t), (tau_u, acc_u) = out["trained"], out["untrained"]
+    assert acc_t > 0.1 and acc_t > 20 * acc_u, out
+    assert tau_t < 0.75 * tau_u, out

@@ -51,3 +51,25 @@ def test_parameter_flattening_round_trips_and_matches_the_oracle_shapes():
     for (W, b), (W2, b2) in zip(params, LP.unflatten(flat)):
         np.testing.assert_array_equal(W, W2)
         np.testing.assert_array_equal(b, b2)
+
+
+def test_block_colouring_is_searched_verified_and_names_parity_classes():
+    """The block colouring comes from the site colouring's own search on the block graph (face, edge and corner
+    neighbours): 8 colours, equal to the clique number, verified on the periodic box, and each colour is one
+    parity class of the block coordinates, whose code the colour-step kernel takes."""
+    from spin_colour_kernel_b200 import colouring as co
+    from spin_colour_kernel_b200 import crystals as cr
+    for nb in (2, 4, 16):
+        col, codes = LP.block_colouring(nb)
+        assert col.n_colours == 8 and sorted(codes) == list(range(8))
+        assert co.verify_on_box(col, cr.make("sc", (1, 2, 3)), (nb,) * 3, (True,) * 3)
+        grid = col.colour_grid(0, (nb,) * 3)
+        z, y, x = np.meshgrid(np.arange(nb), np.arange(nb), np.arange(nb), indexing="ij")
+        assert np.array_equal(np.asarray(codes)[grid], (x % 2) + 2 * (y % 2) + 4 * (z % 2))
+    for bad in (1, 3):
+        try:
+            LP.block_colouring(bad)
+        except ValueError:
+            pass
+        else:
+            raise AssertionError(f"nb={bad} accepted")
