@@ -285,7 +285,7 @@ def ragged(args, rank, world, device):
     of K when K is not a multiple of 100); one step = one sweep of every system."""
     import torch.distributed as tdist
     from spin_colour_kernel_b200 import workloads as W
-    from spin_colour_kernel_b200.sampler import Sampler, SamplerBatch
+    from spin_colour_kernel_b200.sampler import Sampler
     rng = np.random.default_rng(3 + rank)
     samplers, spins = [], []
     attempts = 0
@@ -296,7 +296,8 @@ def ragged(args, rank, world, device):
         samplers.append(A)
         spins.append(torch.from_numpy(W.xy_angles(s, 32, rng)).to(device))
         attempts += 32 * s.n_active
-    batch = SamplerBatch(samplers, spins)
+    from spin_colour_kernel_b200.autotune import autotune_batch
+    batch, tuned = autotune_batch(samplers, spins, use_cache=False)       # untimed: picks the resident limit
     G = 100 if args.steps % 100 == 0 else args.steps
     rep = batch.graph(G)
     for _ in range(max(1, args.warmup // G)):
@@ -330,10 +331,11 @@ def ragged(args, rank, world, device):
             "config": {"workload": "xy-ragged-96 (48 square + 48 triangular, L log-uniform 16..512, half nanodisk)",
                        "systems": len(samplers), "replicas_per_system": 32, "attempts_per_sweep": attempts,
                        "graph_sweeps": G, "resident_systems": info["resident_systems"],
+                       "autotune": {"resident_limit": tuned["resident_limit"], "tried": tuned["tried"]},
                        "l2": "no flush: state ~0.8 GB > L2"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None, "note": f"algorithmic 16 B/attempt over the whole step; peak {kind}"},
-            "gpu_launches": None, "clocks": clk}
+            "gpu_launches": 2 * (args.steps // G), "clocks": clk}
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -453,6 +455,7 @@ def main():
     ap.add_argument("--group", type=int, default=None,
                     help="interleaved layout: replicas per group of the class-skewed L2 pipeline (0 = class by class)")
     ap.add_argument("--skew", type=int, default=2, help="interleaved layout: class skew of the pipeline")
+    ap.add_argument("--chunks", type=int, default=None, help="interleaved layout: site blocks per pipeline ticket")
     ap.add_argument("--layout", default="quad", choices=["quad", "reference"],
                     help="heisenberg-bcc resident storage: interleaved quads (default) or the reference layout")
     ap.add_argument("--path", default="auto",
@@ -498,8 +501,9 @@ def main():
     budget = int((args.l2_mb or 0) * (1 << 20))
     if A.quad:
         if args.group:
-            A.pipeline(args.group, args.skew)
-        cfg["pipeline"] = {"group": A.path()["group"], "skew": args.skew if args.group else None}
+            A.pipeline(args.group, args.skew, args.chunks)
+        cfg["pipeline"] = {"group": A.path()["group"], "skew": args.skew if args.group else None,
+                           "chunks": (args.chunks or 4) if args.group else None}
     elif args.path in ("tile", "segment", "row", "lattice", "generic"):
         A.tune({"tile": 3, "segment": 2, "row": 2, "lattice": 1, "generic": 0}[args.path], budget, RESIDENT_LIMIT)
     elif args.path == "autotune":

@@ -182,6 +182,10 @@ int sck_plan_path(const sck_plan* plan, int32_t* specialised, int64_t* l2_budget
  * when a wait of this plan gave up since the last status read; until then sck_sweep and sck_sweep_measure of the
  * plan refuse with SCK_ERR_TIMEOUT. */
 int sck_plan_pipeline(sck_plan* plan, int32_t group_replicas, int32_t skew);
+/* Site blocks (256 class sites of a quad) that one pipeline ticket covers, 1 .. 64 (default 4): more per ticket
+ * means fewer ticket, wait and completion operations, a coarser overlap between the classes. The chain does not
+ * depend on it. No counterpart in the reference (its classes are separate launches). */
+int sck_plan_pipeline_chunks(sck_plan* plan, int32_t site_blocks);
 int sck_plan_set_wait_limit(sck_plan* plan, int64_t polls);
 int sck_plan_wait_status(sck_plan* plan, void* stream);
 
@@ -288,14 +292,21 @@ int sck_unpack(const sck_plan* plan, const int32_t* words, const int8_t* mask, i
 
 /* Ragged batches (no counterpart in the reference, which runs one Sampler per system): several plans with one
  * storage mode (int8 or float32) and one spin dimension, of different crystal, size, mask, colouring and
- * temperatures, swept together. Systems whose replica takes at most resident_limit_bytes of shared memory run
- * every sweep of a call in one resident launch; the others run one launch per colour step for all of them.
- *   sck_batch_workspace_size  device bytes of the per-system descriptors (caller-owned workspace);
+ * temperatures, swept together. A call is one persistent launch driven by the per-system descriptors: blocks take
+ * work items in ticket order; systems whose replica takes at most resident_limit_bytes of shared memory are one
+ * item per replica that runs every sweep of the call on-chip, the others one item per (sweep, class, replica,
+ * 256-site chunk), each waiting (bounded) for the class it follows in its own system to finish.
+ *   sck_batch_workspace_size  device bytes of the per-system descriptors and the call's counters (caller-owned
+ *                             workspace; one call at a time per workspace);
  *   sck_batch_bind            write the descriptors for these per-system buffers (a host-to-device copy on
- *                             `stream`: call it outside stream capture, again when a buffer moves);
- *   sck_batch_sweep           n sweeps of every system, kernel launches only (capturable); each system's
- *                             state[1] advances by n;
- *   sck_batch_info            systems and blocks of the resident launch, blocks of the colour-step launches. */
+ *                             `stream`: call it outside stream capture, again when a buffer moves); sizes the
+ *                             persistent grid for the current device and allocates a host-mapped give-up flag;
+ *   sck_batch_sweep           n sweeps of every system, kernel launches and a counter reset only (capturable);
+ *                             each system's state[1] advances by n; refuses with SCK_ERR_TIMEOUT while a wait
+ *                             that gave up is unread;
+ *   sck_batch_set_wait_limit  polls of a wait before it gives up (default 2^20; 0 for failure-detection tests);
+ *   sck_batch_wait_status     synchronise `stream`; SCK_ERR_TIMEOUT (clearing it) when a wait gave up;
+ *   sck_batch_info            resident systems and items, streaming items per sweep. */
 typedef struct sck_batch sck_batch;
 int sck_batch_create(const sck_plan* const* plans, int32_t n_plans, int64_t resident_limit_bytes, sck_batch** out);
 int sck_batch_destroy(sck_batch* batch);
@@ -303,6 +314,8 @@ int sck_batch_workspace_size(const sck_batch* batch, int64_t* bytes);
 int sck_batch_bind(sck_batch* batch, const sck_buffers* buffers, void* workspace, void* stream);
 int sck_batch_sweep(sck_batch* batch, void* workspace, int32_t n_sweeps, void* stream);
 int sck_batch_info(const sck_batch* batch, int32_t* resident_systems, int32_t* resident_blocks, int64_t* step_blocks);
+int sck_batch_set_wait_limit(sck_batch* batch, int64_t polls);
+int sck_batch_wait_status(sck_batch* batch, void* stream);
 
 /* Advance state[1] by `n` on the device (what a sweep does after its class launches). */
 int sck_advance(int64_t* state, int32_t n, void* stream);

@@ -53,6 +53,7 @@ _SIGNATURES = {
     "sck_plan_shape": ([_vp, ctypes.POINTER(_i32), ctypes.POINTER(_i32)], _i32),
     "sck_plan_tune": ([_vp, _i32, _i64, _i64], _i32),
     "sck_plan_pipeline": ([_vp, _i32, _i32], _i32),
+    "sck_plan_pipeline_chunks": ([_vp, _i32], _i32),
     "sck_plan_set_wait_limit": ([_vp, _i64], _i32),
     "sck_plan_wait_status": ([_vp, _vp], _i32),
     "sck_plan_path": ([_vp, ctypes.POINTER(_i32), ctypes.POINTER(_i64), ctypes.POINTER(_i32),
@@ -81,6 +82,8 @@ _SIGNATURES = {
     "sck_batch_bind": ([_vp, ctypes.POINTER(Buffers), _vp, _vp], _i32),
     "sck_batch_sweep": ([_vp, _vp, _i32, _vp], _i32),
     "sck_batch_info": ([_vp, ctypes.POINTER(_i32), ctypes.POINTER(_i32), ctypes.POINTER(_i64)], _i32),
+    "sck_batch_set_wait_limit": ([_vp, _i64], _i32),
+    "sck_batch_wait_status": ([_vp, _vp], _i32),
     # learned block proposal (include/sck_made.h)
     "sck_made_sizes": ([_i32, _i32, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64)], _i32),
     "sck_made_prepare": ([_vp, _i32, _vp], _i32),

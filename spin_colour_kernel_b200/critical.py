@@ -130,3 +130,150 @@ def crossing(grid, u1, u2) -> float:
         return float("nan")
     j = flips[flips.size // 2]
     return float(grid[j] - d[j] * (grid[j + 1] - grid[j]) / (d[j + 1] - d[j]))
+
+
+# ------------------------------------------------------------------------------------------ multi-size driver
+def holm(p) -> list[float]:
+    """Holm's step-down adjustment of a family of p-values (each p times the number of hypotheses not yet
+    rejected, made monotone, capped at 1)."""
+    p = np.asarray(p, np.float64)
+    adj = np.zeros(p.size)
+    running = 0.0
+    for rank, i in enumerate(np.argsort(p)):
+        running = max(running, (p.size - rank) * p[i])
+        adj[i] = min(1.0, running)
+    return adj.tolist()
+
+
+def probe_tau(s: sy.System, L_box: int, Tc: float, seeds: int, device="cuda", start: int = 2000,
+              cap: int = 100_000, ratio: int = 50):
+    """tau_int of m^2 at Tc from probes of growing length (x4 from `start`, at most `cap`) until the probe reaches
+    `ratio` tau: (tau, probe length, whether it reached ratio tau, energy spread of one configuration)."""
+    from .stats import integrated_tau
+    length = int(start)
+    while True:
+        E, m2, _ = series(s, L_box, [Tc], seeds, max(500, length // 4), length, 1, device)
+        tau = integrated_tau(m2[0].T)
+        if length >= ratio * tau or length >= cap:
+            return tau, length, bool(length >= ratio * tau), float(E[0].std(axis=1).mean())
+        length = min(cap, 4 * length)
+
+
+def _size_box(s0: sy.System, L: int) -> int:
+    """Box side of size L: triangular boxes take the nearest multiple of 3 (a 3-colouring of the periodic box)."""
+    return 3 * int(round(L / 3)) if s0.crystal.name == "triangular" else L
+
+
+def _make(maker, args, L, kw, acceptance):
+    s = maker(*args, L, **kw)
+    if acceptance != s.acceptance:
+        s = sy.System(s.name, s.n, s.crystal, s.box, s.periodic, s.J, T_ref=s.T_ref, acceptance=acceptance)
+    return s
+
+
+def crossing_estimate(data: dict, x: float, weights=None, device="cpu", lnZ_cache=None, points: int = 241):
+    """T_c from Binder crossings of consecutive sizes: for each pair (L1, L2), both curves reweighted onto the
+    temperatures both sizes cover, crossed; with two or more crossings, the intercept of a straight-line fit of
+    T_cross against sqrt(L1 L2)^-x, else the last crossing. `weights` are per-seed multiplicities (bootstrap);
+    `lnZ_cache` keeps each size's free energies from the unweighted pass as the next passes' starting point.
+    Returns (estimate, [(sqrt(L1 L2), T_cross)], {(L1, L2): (grid, U1, U2)})."""
+    Ls = sorted(data)
+    curves, cross = {}, []
+    for a, b in zip(Ls[:-1], Ls[1:]):
+        grid = np.linspace(max(data[a]["temps"][0], data[b]["temps"][0]),
+                           min(data[a]["temps"][-1], data[b]["temps"][-1]), points)
+        us = []
+        for L in (a, b):
+            d = data[L]
+            w = None if weights is None else np.broadcast_to(weights[None, :, None], d["E"].shape)
+            u, lnZ = binder_curve(d["E"], d["m2"], d["m4"], d["temps"], grid, weights=w, device=device,
+                                  lnZ0=None if lnZ_cache is None else lnZ_cache.get(L))
+            if lnZ_cache is not None and weights is None:
+                lnZ_cache[L] = lnZ
+            us.append(u)
+        curves[(a, b)] = (grid, us[0], us[1])
+        t = crossing(grid, us[0], us[1])
+        if np.isfinite(t):
+            cross.append((math.sqrt(a * b), t))
+    if len(cross) >= 2:
+        X = np.array([l ** (-x) for l, _ in cross])
+        Y = np.array([t for _, t in cross])
+        return float(np.polyfit(X, Y, 1)[1]), cross, curves
+    return (cross[-1][1] if cross else float("nan")), cross, curves
+
+
+def e4(out, device="cuda", sizes2d=(32, 64, 128, 256), sizes3d=(16, 24, 32, 48), seeds: int = 10,
+       window: float = 0.03, ntemps: int = 9, meas: int = 20000, boots: int = 2000, only=None, tag: str = "E4",
+       probe_cap: int = 100_000, acceptance: str = "metropolis", probe_start: int = 2000, log=print):
+    """The multi-size critical-point study (the reference's E4, `exp_perf.py:846-950`) on this library: for each
+    system of `e4_systems()` (or those named in `only`) and each size, tau_int at T_c from a growing probe,
+    `ntemps` temperatures one energy width apart (within +-window), thermalisation of max(1000, 20 tau) sweeps,
+    an observation every max(1, tau / 2, meas / 2000) sweeps, the raw series saved to
+    `<out>/<tag>-<system>-L<L>.npz`; then T_c from Binder crossings of consecutive sizes extrapolated in
+    L^-(1/nu + omega), a bootstrap over seeds (95 % interval, two-sided p-value of the reference T_c), Holm's
+    adjustment across systems and a verdict (supported / not supported / inconclusive when the half-width
+    exceeds 0.5 % of T_c). Writes and returns `<out>/<tag>.json`'s payload."""
+    import json
+    import time
+    from pathlib import Path
+    from .stats import integrated_tau
+    out = Path(out)
+    out.mkdir(parents=True, exist_ok=True)
+    rdev = device if str(device).startswith("cuda") and torch.cuda.is_available() else "cpu"
+    rows = []
+    for maker, args, kw, dim, x in e4_systems():
+        probe = _make(maker, args, 6 if args[0] == "triangular" else 4, kw, acceptance)
+        if only and probe.name not in only:
+            continue
+        Tc = kw["T_ref"]
+        t0 = time.time()
+        data = {}
+        for L in (sizes2d if dim == "2d" else sizes3d):
+            Lb = _size_box(probe, L)
+            s = _make(maker, args, Lb, kw, acceptance)
+            tau, P, resolved, sigma_E = probe_tau(s, Lb, Tc, seeds, device, start=probe_start, cap=probe_cap)
+            temps = e4_temperatures(Tc, sigma_E, ntemps, window)
+            therm = int(max(1000, 20 * tau))
+            every = max(1, int(round(tau / 2)), meas // 2000)
+            E, m2, m4 = series(s, Lb, temps, seeds, therm, meas, every, device)
+            mid = int(np.argmin(np.abs(temps - Tc)))
+            tau_prod = every * integrated_tau(m2[mid].T)
+            np.savez_compressed(out / f"{tag}-{probe.name.replace(' ', '_')}-L{Lb}.npz", E=E,
+                                m2=m2.astype(np.float32), m4=m4.astype(np.float32), temps=temps, tau=tau,
+                                therm=therm, every=every)
+            data[Lb] = {"E": E, "m2": m2, "m4": m4, "temps": temps, "tau": tau, "probe_sweeps": P,
+                        "tau_resolved": resolved, "sigma_E": sigma_E, "therm": therm, "every": every,
+                        "tau_production": tau_prod, "therm_over_tau_production": therm / tau_prod}
+            log(f"E4 {probe.name:20s} L={Lb} tau={tau:.1f} (probe {P}, resolved {resolved}) tau_prod={tau_prod:.1f} "
+                f"therm={therm} every={every} window=+-{(temps[-1] / Tc - 1):.4%} {time.time() - t0:.0f}s")
+        lnZ = {}
+        est, pairs, curves = crossing_estimate(data, x, device=rdev, lnZ_cache=lnZ)
+        rng = np.random.default_rng(1)
+        bs = np.array([crossing_estimate(data, x, weights=np.bincount(rng.integers(0, seeds, seeds),
+                                                                      minlength=seeds).astype(np.float64),
+                                         device=rdev, lnZ_cache=lnZ)[0] for _ in range(boots)])
+        bs = bs[np.isfinite(bs)]
+        lo, hi = np.quantile(bs, [0.025, 0.975]) if bs.size > 10 else (np.nan, np.nan)
+        half = (hi - lo) / 2 / Tc
+        p = float(min(1.0, 2 * min(np.mean(bs <= Tc), np.mean(bs >= Tc)))) if bs.size else float("nan")
+        keys = ("tau", "probe_sweeps", "tau_resolved", "sigma_E", "therm", "every", "tau_production",
+                "therm_over_tau_production")
+        Ls = sorted(data)
+        rows.append({"system": probe.name, "T_ref": Tc, "estimate": est, "low": float(lo), "high": float(hi),
+                     "half_width_over_Tc": float(half), "p_reference": p, "pair_crossings": pairs, "sizes": Ls,
+                     "temps": {L: data[L]["temps"].tolist() for L in Ls}, "correction_exponent": x,
+                     "reweighting": "multi-histogram", "declared": {L: {k: data[L][k] for k in keys} for L in Ls},
+                     "binder": {f"{a}-{b}": {"grid": g.tolist(), str(a): ua.tolist(), str(b): ub.tolist()}
+                                for (a, b), (g, ua, ub) in curves.items()},
+                     "seconds": time.time() - t0})
+        log(f"E4 {probe.name:20s} Tc={est:.5f} [{lo:.5f},{hi:.5f}] ref {Tc:.5f} half {half:.4%}")
+    for r, pa in zip(rows, holm([r["p_reference"] if np.isfinite(r["p_reference"]) else 1.0 for r in rows])):
+        r["p_holm"] = pa
+        r["verdict"] = ("inconclusive" if not (r["half_width_over_Tc"] <= 0.005) else
+                        ("supported" if pa >= 0.05 else "not supported"))
+    payload = {"experiment": tag, "rows": rows,
+               "params": {"sizes2d": list(sizes2d), "sizes3d": list(sizes3d), "seeds": seeds, "window": window,
+                          "ntemps": ntemps, "meas": meas, "boots": boots, "probe_cap": probe_cap,
+                          "reweighting": "multi-histogram"}}
+    (out / f"{tag}.json").write_text(json.dumps(payload, indent=2, default=float))
+    return payload

@@ -357,6 +357,7 @@ int sck_plan_create(const sck_system_desc* d, int32_t batch, int32_t mode, sck_p
   }
   p->kernel_kind = 1;
   p->wait_limit = 1u << 20;
+  p->quad_cpt = 4;
   p->l2_budget = 0;
   p->resident_limit = kResidentDefault;
   *out = p;
@@ -476,6 +477,13 @@ int sck_plan_pipeline(sck_plan* plan, int32_t group_replicas, int32_t skew) {
     return rc;
   }
   plan->quad_skew = skew;
+  return SCK_OK;
+}
+
+int sck_plan_pipeline_chunks(sck_plan* plan, int32_t site_blocks) {
+  if (plan == nullptr || site_blocks < 1 || site_blocks > 64)
+    return fail(SCK_ERR_INVALID, "site blocks per pipeline ticket must be 1 .. 64");
+  plan->quad_cpt = site_blocks;
   return SCK_OK;
 }
 

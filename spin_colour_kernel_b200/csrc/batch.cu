@@ -1,13 +1,18 @@
 // Ragged batches: many systems of different size, crystal, mask and temperature swept together.
 //
 // A batch holds several plans with one storage mode. Per-system descriptors (geometry, colouring, bonds,
-// device buffers) live in a caller-owned workspace on the device, written by sck_batch_bind. A sweep of the
-// batch then needs no host work:
-//   - systems whose replica fits in shared memory run one resident launch for all of them: block (system,
-//     replica) loads the replica once and runs every class of every sweep of the call on-chip;
-//   - the other systems run one launch per colour step: step k updates class k of every system that has one,
-//     every (system, replica, 256-site chunk) a block, found by a binary search over per-step block offsets.
-// Both launch kinds read each system's descriptor from the workspace, so one kernel serves every crystal.
+// device buffers) live in a caller-owned workspace on the device, written by sck_batch_bind, together with the
+// call's ticket and completion counters. A call of n sweeps is ONE persistent launch: a grid sized to the
+// resident capacity of the GPU whose blocks take work items in ticket order from a counter:
+//   - resident items (system, replica), for systems whose replica fits shared memory: the block loads the
+//     replica once and runs every class of every sweep of the call on-chip;
+//   - streaming items (sweep, colour step k, system, replica, 256-site chunk) for the others, found by binary
+//     searches over per-step item offsets. Before touching spins, a block waits (bounded) until every item of the
+//     class its item follows is done: class k - 1 of the same system and sweep, or the system's last class of the
+//     previous sweep; per-(system, class) completion counters count finished items. That class holds smaller
+//     tickets, taken by blocks that are running or done, so every wait ends, and each system's classes are
+//     serialised exactly as separate launches would serialise them, while different systems overlap freely.
+// Both kinds read each system's descriptor from the workspace, so one kernel serves every crystal.
 #include <string.h>
 
 #include <algorithm>
@@ -28,6 +33,7 @@ __device__ __forceinline__ void batch_site(const Common& c, const SubDev& sub, i
 }
 
 constexpr int kBatchMaxSystems = 256;
+constexpr int kBatchItemPasses = 4;   // a streaming item: 4 x 256 class sites of one replica and class
 constexpr int kBatchMaxClasses = 32;
 
 struct SysDev {
@@ -36,21 +42,30 @@ struct SysDev {
   int n_classes;
   int classes[kBatchMaxClasses][2];
   int resident;
-  int chunks;          // 256-site chunks of one class (streaming systems)
+  int chunks;          // streaming items of one class and replica (kBatchItemPasses x 256 class sites each)
 };
 
 struct BatchLayout {   // offsets into the workspace
   size_t sys;          // SysDev[n]
-  size_t step_off;     // int[max_classes][n + 1]: first block of system s in colour step k (streaming)
-  size_t res_off;      // int[n + 1]: first block of system s in the resident launch
+  size_t step_off;     // int[max_classes][n + 1]: first item of system s in colour step k (streaming)
+  size_t res_off;      // int[n + 1]: first resident item of system s
+  size_t k_off;        // long long[max_classes + 1]: first item of colour step k within a sweep
+  size_t counters;     // unsigned[1 + n max_classes]: ticket, then finished items per (system, class)
 };
 
 struct BatchDevParams {
   const SysDev* sys;
-  const int* offsets;  // n + 1 block offsets of this launch
-  int n;
-  int step;            // colour step (streaming) or number of sweeps (resident)
-  int sweep_offset;
+  const int* step_off;
+  const int* res_off;
+  const long long* k_off;
+  int n, max_classes;
+  int res_items;                // resident items of a launch
+  long long step_items;         // streaming items of one sweep
+  int n_sweeps, sweep_base;     // sweeps of this launch, offset of its first sweep within the call
+  unsigned* ticket;
+  unsigned* done;
+  unsigned wait_limit;
+  int* giveup;
 };
 
 }  // namespace sck
@@ -65,8 +80,13 @@ struct sck_batch {
   sck::BatchLayout layout;
   size_t bytes;
   std::vector<unsigned char> staging;   // host image of the workspace
-  std::vector<int> step_blocks;   // total blocks per colour step
+  std::vector<int> step_blocks;   // total items per colour step
   int resident_blocks;
+  long long step_items;           // streaming items per sweep
+  int grid;                       // persistent blocks of a launch (resident capacity of the device)
+  unsigned wait_limit;
+  int* giveup_host;               // host-mapped flag a block raises when a wait gives up
+  int* giveup_dev;
   bool bound;
 };
 
@@ -82,101 +102,199 @@ __device__ __forceinline__ int find_system(const int* off, int n, int block) {
   return lo;
 }
 
-template <int N, typename ST>
-__global__ void __launch_bounds__(256) batch_step_kernel(const BatchDevParams p) {
-  const int s = find_system(p.offsets, p.n, blockIdx.x);
-  const SysDev& d = p.sys[s];
-  if (d.resident || p.step >= d.n_classes) return;
-  const int local = blockIdx.x - p.offsets[s];
-  const int rep = local / d.chunks;
-  const int chunk = local - rep * d.chunks;
-  const uint32_t t = (uint32_t)chunk * 256u + threadIdx.x;
-  if (t >= (uint32_t)d.c.rows * (uint32_t)d.c.bx) return;
-  const int colour = d.classes[p.step][0], alpha = d.classes[p.step][1];
-  int x, y, z;
-  if (!class_site(d.c, colour, alpha, t, x, y, z)) return;
-  const int32_t key = sweep_key(d.c.state);
-  ST* spins = (ST*)d.c.dst + (size_t)rep * N * d.c.g.nsite;
-  batch_site<N, ST>(d.c, d.sub[alpha], alpha, rep, x, y, z, key, spins);
+__device__ __forceinline__ int find_step(const long long* k_off, int K, long long item) {
+  int k = 0;
+  while (k + 1 < K && k_off[k + 1] <= item) ++k;
+  return k;
 }
 
+__device__ __forceinline__ unsigned batch_ld_acquire(const unsigned* a) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(a) : "memory");
+  return v;
+}
+
+struct BatchItem {
+  int kind;      // 0: no more work, 1: resident, 2: streaming, 3: streaming item whose wait gave up
+  int s, rep, chunk, k, sw;
+};
+
+// The persistent batch kernel: 256 threads per block, dynamic shared memory for the largest resident replica.
 template <int N, typename ST>
-__global__ void __launch_bounds__(1024) batch_resident_kernel(const BatchDevParams p) {
+__global__ void __launch_bounds__(256) batch_persistent_kernel(const BatchDevParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  ST* S = reinterpret_cast<ST*>(smem_raw);
-  const int s = find_system(p.offsets, p.n, blockIdx.x);
-  const SysDev& d = p.sys[s];
-  if (!d.resident) return;
-  const int rep = blockIdx.x - p.offsets[s];
-  const int n = N * d.c.g.nsite;
-  ST* home = (ST*)d.c.dst + (size_t)rep * n;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) S[i] = home[i];
-  __syncthreads();
-  const uint32_t per = (uint32_t)d.c.rows * (uint32_t)d.c.bx;
-  for (int sw = 0; sw < p.step; ++sw) {
-    const int32_t key = sweep_key_at(d.c.state, sw);
-    for (int ci = 0; ci < d.n_classes; ++ci) {
-      const int colour = d.classes[ci][0], alpha = d.classes[ci][1];
-      for (uint32_t t = threadIdx.x; t < per; t += blockDim.x) {
-        int x, y, z;
-        if (class_site(d.c, colour, alpha, t, x, y, z)) batch_site<N, ST>(d.c, d.sub[alpha], alpha, rep, x, y, z, key, S);
+  __shared__ BatchItem it;
+  const long long total = (long long)p.res_items + (long long)p.n_sweeps * p.step_items;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const long long tk = (long long)atomicAdd(p.ticket, 1u);
+      it.kind = 0;
+      if (tk < p.res_items) {
+        const int s = find_system(p.res_off, p.n, (int)tk);
+        it.kind = 1;
+        it.s = s;
+        it.rep = (int)tk - p.res_off[s];
+      } else if (tk < total) {
+        const long long u = tk - p.res_items;
+        const int sw = (int)(u / p.step_items);
+        const long long r = u - (long long)sw * p.step_items;
+        const int k = find_step(p.k_off, p.max_classes, r);
+        const int local = (int)(r - p.k_off[k]);
+        const int* off = p.step_off + (size_t)k * (p.n + 1);
+        const int s = find_system(off, p.n, local);
+        const SysDev& d = p.sys[s];
+        const int j = local - off[s];
+        it.kind = 2;
+        it.s = s;
+        it.k = k;
+        it.sw = sw;
+        it.rep = j / d.chunks;
+        it.chunk = j - it.rep * d.chunks;
+        // the class this item follows: k - 1 of this sweep, or the last class of the previous sweep
+        const unsigned per = (unsigned)d.chunks * (unsigned)d.c.B;
+        const unsigned* dep = nullptr;
+        unsigned need = 0;
+        if (k > 0) {
+          dep = p.done + (size_t)s * p.max_classes + (k - 1);
+          need = (unsigned)(sw + 1) * per;
+        } else if (sw > 0) {
+          dep = p.done + (size_t)s * p.max_classes + (d.n_classes - 1);
+          need = (unsigned)sw * per;
+        }
+        if (dep != nullptr) {
+          unsigned polls = 0;
+          while (batch_ld_acquire(dep) < need) {
+            if (++polls > p.wait_limit) {
+              it.kind = 3;
+              if (p.giveup != nullptr) atomicExch_system(p.giveup, 1);
+              break;
+            }
+            __nanosleep(64);
+          }
+        }
+      }
+    }
+    __syncthreads();
+    const int kind = it.kind;
+    if (kind == 0) return;
+    const SysDev& d = p.sys[it.s];
+    if (kind == 1) {
+      ST* S = reinterpret_cast<ST*>(smem_raw);
+      const int n = N * d.c.g.nsite;
+      ST* home = (ST*)d.c.dst + (size_t)it.rep * n;
+      for (int i = threadIdx.x; i < n; i += blockDim.x) S[i] = home[i];
+      __syncthreads();
+      const uint32_t per = (uint32_t)d.c.rows * (uint32_t)d.c.bx;
+      for (int sw = 0; sw < p.n_sweeps; ++sw) {
+        const int32_t key = sweep_key_at(d.c.state, p.sweep_base + sw);
+        for (int ci = 0; ci < d.n_classes; ++ci) {
+          const int colour = d.classes[ci][0], alpha = d.classes[ci][1];
+          for (uint32_t t = threadIdx.x; t < per; t += blockDim.x) {
+            int x, y, z;
+            if (class_site(d.c, colour, alpha, t, x, y, z))
+              batch_site<N, ST>(d.c, d.sub[alpha], alpha, it.rep, x, y, z, key, S);
+          }
+          __syncthreads();
+        }
+      }
+      for (int i = threadIdx.x; i < n; i += blockDim.x) home[i] = S[i];
+    } else {
+      if (kind == 2) {
+        const uint32_t per = (uint32_t)d.c.rows * (uint32_t)d.c.bx;
+        const int colour = d.classes[it.k][0], alpha = d.classes[it.k][1];
+        const int32_t key = sweep_key_at(d.c.state, p.sweep_base + it.sw);
+        ST* spins = (ST*)d.c.dst + (size_t)it.rep * N * d.c.g.nsite;
+#pragma unroll 1
+        for (int pass = 0; pass < kBatchItemPasses; ++pass) {
+          const uint32_t t = ((uint32_t)it.chunk * kBatchItemPasses + pass) * 256u + threadIdx.x;
+          int x, y, z;
+          if (t < per && class_site(d.c, colour, alpha, t, x, y, z))
+            batch_site<N, ST>(d.c, d.sub[alpha], alpha, it.rep, x, y, z, key, spins);
+        }
       }
       __syncthreads();
+      // done (or given up): the class's next items may start; the barrier orders the block's stores before it
+      if (threadIdx.x == 0)
+        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(p.done + (size_t)it.s * p.max_classes + it.k)
+                     : "memory");
     }
+    __syncthreads();   // `it` is rewritten by the next ticket
   }
-  for (int i = threadIdx.x; i < n; i += blockDim.x) home[i] = S[i];
 }
 
-// state[1] += inc for every system of the given kind (resident or streaming).
-__global__ void batch_advance_kernel(const SysDev* sys, int n, int resident, int inc) {
+// state[1] += inc for every system.
+__global__ void batch_advance_kernel(const SysDev* sys, int n, int inc) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s < n && sys[s].resident == resident) const_cast<int64_t*>(sys[s].c.state)[1] += inc;
+  if (s < n) const_cast<int64_t*>(sys[s].c.state)[1] += inc;
 }
 
 template <int N, typename ST>
-static int run_batch(const sck_batch* b, const unsigned char* ws, int n_sweeps, cudaStream_t st) {
-  BatchDevParams p;
-  p.sys = (const SysDev*)(ws + b->layout.sys);
-  p.n = b->n;
-  p.sweep_offset = 0;
-  if (b->resident_blocks > 0) {
-    p.offsets = (const int*)(ws + b->layout.res_off);
-    p.step = n_sweeps;
-    cudaError_t e = cudaFuncSetAttribute(batch_resident_kernel<N, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)b->resident_smem);
-    if (e != cudaSuccess) return cuda_status(e, "batch resident shared memory");
-    batch_resident_kernel<N, ST><<<b->resident_blocks, 512, b->resident_smem, st>>>(p);
-    int rc = cuda_status(cudaGetLastError(), "batch resident launch");
-    if (rc != SCK_OK) return rc;
-    batch_advance_kernel<<<(b->n + 127) / 128, 128, 0, st>>>(p.sys, b->n, 1, n_sweeps);
-    rc = cuda_status(cudaGetLastError(), "batch advance");
-    if (rc != SCK_OK) return rc;
-  }
-  for (int sw = 0; sw < n_sweeps; ++sw) {
-    bool any = false;
-    for (int k = 0; k < b->max_classes; ++k) {
-      if (b->step_blocks[k] == 0) continue;
-      any = true;
-      p.offsets = (const int*)(ws + b->layout.step_off) + (size_t)k * (b->n + 1);
-      p.step = k;
-      batch_step_kernel<N, ST><<<b->step_blocks[k], 256, 0, st>>>(p);
-      const int rc = cuda_status(cudaGetLastError(), "batch step launch");
-      if (rc != SCK_OK) return rc;
-    }
-    if (!any) break;
-    batch_advance_kernel<<<(b->n + 127) / 128, 128, 0, st>>>(p.sys, b->n, 0, 1);
-    const int rc = cuda_status(cudaGetLastError(), "batch advance");
-    if (rc != SCK_OK) return rc;
-  }
+static int batch_prepare(sck_batch* b) {
+  cudaError_t e = cudaFuncSetAttribute(batch_persistent_kernel<N, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)b->resident_smem);
+  if (e != cudaSuccess) return cuda_status(e, "batch shared memory");
+  int dev = 0, sms = 0, per_sm = 0;
+  e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_persistent_kernel<N, ST>, 256, b->resident_smem);
+  if (e != cudaSuccess) return cuda_status(e, "batch occupancy");
+  b->grid = sms * (per_sm > 0 ? per_sm : 1);
   return SCK_OK;
 }
 
-int batch_sweep_dispatch(const sck_batch* b, const unsigned char* ws, int n_sweeps, cudaStream_t st) {
+template <int N, typename ST>
+static int run_batch(const sck_batch* b, unsigned char* ws, int n_sweeps, cudaStream_t st) {
+  BatchDevParams p;
+  memset(&p, 0, sizeof(p));
+  p.sys = (const SysDev*)(ws + b->layout.sys);
+  p.step_off = (const int*)(ws + b->layout.step_off);
+  p.res_off = (const int*)(ws + b->layout.res_off);
+  p.k_off = (const long long*)(ws + b->layout.k_off);
+  p.n = b->n;
+  p.max_classes = b->max_classes;
+  p.res_items = b->resident_blocks;
+  p.step_items = b->step_items;
+  p.ticket = (unsigned*)(ws + b->layout.counters);
+  p.done = p.ticket + 1;
+  p.wait_limit = b->wait_limit;
+  p.giveup = b->giveup_dev;
+  const size_t counter_bytes = sizeof(unsigned) * (1 + (size_t)b->n * b->max_classes);
+  // sweeps per launch: tickets and per-class completion counts stay below 2^31
+  long long per_launch = b->step_items > 0 ? ((1ll << 31) - 1 - b->resident_blocks) / b->step_items : n_sweeps;
+  if (per_launch < 1) return cuda_status(cudaErrorInvalidConfiguration, "batch too large for one launch");
+  for (int sw0 = 0; sw0 < n_sweeps; sw0 += (int)per_launch) {
+    p.sweep_base = sw0;
+    p.n_sweeps = (int)std::min<long long>(per_launch, n_sweeps - sw0);
+    int rc = cuda_status(cudaMemsetAsync(p.ticket, 0, counter_bytes, st), "batch counters");
+    if (rc != SCK_OK) return rc;
+    const long long items = (long long)p.res_items + (long long)p.n_sweeps * p.step_items;
+    const int grid = (int)std::min<long long>(b->grid, items);
+    if (grid > 0) {
+      batch_persistent_kernel<N, ST><<<grid, 256, b->resident_smem, st>>>(p);
+      rc = cuda_status(cudaGetLastError(), "batch launch");
+      if (rc != SCK_OK) return rc;
+    }
+  }
+  batch_advance_kernel<<<(b->n + 127) / 128, 128, 0, st>>>(p.sys, b->n, n_sweeps);
+  return cuda_status(cudaGetLastError(), "batch advance");
+}
+
+int batch_sweep_dispatch(const sck_batch* b, unsigned char* ws, int n_sweeps, cudaStream_t st) {
   if (b->mode == SCK_MODE_INT8) return run_batch<1, int8_t>(b, ws, n_sweeps, st);
   switch (b->ncomp) {
     case 1: return run_batch<1, float>(b, ws, n_sweeps, st);
     case 2: return run_batch<2, float>(b, ws, n_sweeps, st);
     default: return run_batch<3, float>(b, ws, n_sweeps, st);
+  }
+}
+
+int batch_prepare_dispatch(sck_batch* b) {
+  if (b->mode == SCK_MODE_INT8) return batch_prepare<1, int8_t>(b);
+  switch (b->ncomp) {
+    case 1: return batch_prepare<1, float>(b);
+    case 2: return batch_prepare<2, float>(b);
+    default: return batch_prepare<3, float>(b);
   }
 }
 
@@ -229,17 +347,45 @@ int sck_batch_create(const sck_plan* const* plans, int32_t n_plans, int64_t resi
   b->layout.sys = 0;
   b->layout.step_off = align_up(sizeof(SysDev) * n_plans, 256);
   b->layout.res_off = align_up(b->layout.step_off + sizeof(int) * (size_t)b->max_classes * (n_plans + 1), 256);
-  b->bytes = align_up(b->layout.res_off + sizeof(int) * (size_t)(n_plans + 1), 256);
+  b->layout.k_off = align_up(b->layout.res_off + sizeof(int) * (size_t)(n_plans + 1), 256);
+  b->layout.counters = align_up(b->layout.k_off + sizeof(long long) * (size_t)(b->max_classes + 1), 256);
+  b->bytes = align_up(b->layout.counters + sizeof(unsigned) * (1 + (size_t)n_plans * b->max_classes), 256);
   b->staging.assign(b->bytes, 0);
   b->step_blocks.assign(b->max_classes, 0);
   b->resident_blocks = 0;
+  b->step_items = 0;
+  b->grid = 0;
+  b->wait_limit = 1u << 20;
+  b->giveup_host = nullptr;
+  b->giveup_dev = nullptr;
   b->bound = false;
   *out = b;
   return SCK_OK;
 }
 
 int sck_batch_destroy(sck_batch* batch) {
+  if (batch != nullptr && batch->giveup_host != nullptr) cudaFreeHost(batch->giveup_host);
   delete batch;
+  return SCK_OK;
+}
+
+int sck_batch_set_wait_limit(sck_batch* batch, int64_t polls) {
+  if (batch == nullptr || polls < 0 || polls > 0xFFFFFFFFll)
+    return batch_fail(SCK_ERR_INVALID, "polls must be 0 .. 2^32-1");
+  batch->wait_limit = (unsigned)polls;
+  return SCK_OK;
+}
+
+int sck_batch_wait_status(sck_batch* batch, void* stream) {
+  if (batch == nullptr) return batch_fail(SCK_ERR_INVALID, "null batch");
+  if (batch->giveup_host == nullptr) return SCK_OK;
+  const int rc = cuda_status(cudaStreamSynchronize((cudaStream_t)stream), "batch wait status");
+  if (rc != SCK_OK) return rc;
+  if (*(volatile int*)batch->giveup_host) {
+    *(volatile int*)batch->giveup_host = 0;
+    return batch_fail(SCK_ERR_TIMEOUT, "a bounded wait of the batch kernel gave up: the affected sites were left "
+                                       "unchanged");
+  }
   return SCK_OK;
 }
 
@@ -277,7 +423,7 @@ int sck_batch_bind(sck_batch* b, const sck_buffers* buffers, void* workspace, vo
     }
     d.resident = b->resident[s];
     const long long per = (long long)d.c.rows * d.c.bx;
-    d.chunks = (int)((per + 255) / 256);
+    d.chunks = (int)((per + 256 * kBatchItemPasses - 1) / (256 * kBatchItemPasses));
     res_off[s] = (int)res_total;
     if (d.resident) res_total += plan->Bp;
     for (int k = 0; k < b->max_classes; ++k) {
@@ -286,12 +432,33 @@ int sck_batch_bind(sck_batch* b, const sck_buffers* buffers, void* workspace, vo
     }
   }
   res_off[b->n] = (int)res_total;
+  long long* k_off = (long long*)(img + b->layout.k_off);
+  long long items = 0;
   for (int k = 0; k < b->max_classes; ++k) {
     if (step_total[k] >= (1ll << 31)) return batch_fail(SCK_ERR_UNSUPPORTED, "batch too large for one launch");
     step_off[k * (b->n + 1) + b->n] = (int)step_total[k];
     b->step_blocks[k] = (int)step_total[k];
+    k_off[k] = items;
+    items += step_total[k];
   }
+  k_off[b->max_classes] = items;
+  if (items + res_total >= (1ll << 31)) return batch_fail(SCK_ERR_UNSUPPORTED, "batch too large for one launch");
+  b->step_items = items;
   b->resident_blocks = (int)res_total;
+  // set-up outside any sweep: the kernel's shared-memory limit and grid, the give-up flag
+  int rc0 = batch_prepare_dispatch(b);
+  if (rc0 != SCK_OK) return rc0;
+  if (b->giveup_host == nullptr) {
+    rc0 = cuda_status(cudaHostAlloc((void**)&b->giveup_host, sizeof(int), cudaHostAllocMapped | cudaHostAllocPortable),
+                      "batch give-up flag");
+    if (rc0 != SCK_OK) {
+      b->giveup_host = nullptr;
+      return rc0;
+    }
+    *b->giveup_host = 0;
+    rc0 = cuda_status(cudaHostGetDevicePointer((void**)&b->giveup_dev, b->giveup_host, 0), "batch give-up flag");
+    if (rc0 != SCK_OK) return rc0;
+  }
   const int rc = cuda_status(cudaMemcpyAsync(workspace, img, b->bytes, cudaMemcpyHostToDevice, (cudaStream_t)stream),
                              "batch descriptors");
   if (rc != SCK_OK) return rc;
@@ -303,7 +470,9 @@ int sck_batch_sweep(sck_batch* b, void* workspace, int32_t n_sweeps, void* strea
   if (b == nullptr || workspace == nullptr || n_sweeps < 0) return batch_fail(SCK_ERR_INVALID, "bad batch sweep call");
   if (!b->bound) return batch_fail(SCK_ERR_INVALID, "bind the batch's buffers first (sck_batch_bind)");
   if (n_sweeps == 0) return SCK_OK;
-  return batch_sweep_dispatch(b, (const unsigned char*)workspace, n_sweeps, (cudaStream_t)stream);
+  if (b->giveup_host != nullptr && *(volatile int*)b->giveup_host)
+    return batch_fail(SCK_ERR_TIMEOUT, "an earlier bounded wait of this batch gave up (read sck_batch_wait_status)");
+  return batch_sweep_dispatch(b, (unsigned char*)workspace, n_sweeps, (cudaStream_t)stream);
 }
 
 int sck_batch_info(const sck_batch* b, int32_t* resident_systems, int32_t* resident_blocks, int64_t* step_blocks) {

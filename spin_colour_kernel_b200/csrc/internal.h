@@ -127,6 +127,7 @@ struct sck_plan {
   size_t pipe_bytes;
   int pipe_device;           // the device that holds them
   int quad_group, quad_skew; // interleaved pipeline: quads per group (0 = class by class) and class skew
+  int quad_cpt;              //   and site blocks of 256 threads per ticket
   unsigned wait_limit;       // polls of a pipeline completion counter before a block gives up
   int* giveup_host;          // host-mapped flag a kernel raises when a bounded wait gives up (host view)
   int* giveup_dev;           //   and its device view

@@ -260,7 +260,14 @@ __global__ void __launch_bounds__(128) quad_measure_finish(const double* __restr
 
 // One sweep whose class launches also accumulate the FP64 observables of the configuration it leaves (E and M
 // of the first plan->batch replicas), then the counter advance. Needs quad_measure_fused(plan).
-static int launch_measure_finish(const sck_plan* plan, const void* workspace, double* E, double* M, cudaStream_t s);
+static int launch_measure_finish(const sck_plan* plan, const void* workspace, double* E, double* M, cudaStream_t s,
+                                 int blocks_x);
+
+// The pipeline's tickets per quad and class: site blocks of 256 threads grouped plan->quad_cpt to a ticket.
+static int quad_pipe_tickets(const sck_plan* plan) {
+  const int cpt = plan->quad_cpt > 0 ? plan->quad_cpt : 1;
+  return (quad_blocks_x(plan) + cpt - 1) / cpt;
+}
 
 int launch_quad_measure_sweep(const sck_plan* plan, const sck_buffers* buf, double* E, double* M, void* workspace,
                               cudaStream_t s) {
@@ -281,15 +288,16 @@ int launch_quad_measure_sweep(const sck_plan* plan, const sck_buffers* buf, doub
   }
   const int rc = launch_advance(buf->state, 1, s);
   if (rc != SCK_OK) return rc;
-  return launch_measure_finish(plan, workspace, E, M, s);
+  return launch_measure_finish(plan, workspace, E, M, s, quad_blocks_x(plan));
 }
 
-static int launch_measure_finish(const sck_plan* plan, const void* workspace, double* E, double* M, cudaStream_t s) {
+static int launch_measure_finish(const sck_plan* plan, const void* workspace, double* E, double* M, cudaStream_t s,
+                                 int blocks_x) {
   const int C = plan->desc.n_classes;
   MeasureFinishParams f;
   memset(&f, 0, sizeof(f));
   f.n_classes = C;
-  f.blocks_x = quad_blocks_x(plan);
+  f.blocks_x = blocks_x;
   f.n = plan->geom.n;
   f.b = plan->geom.b;
   for (int ci = 0; ci < C; ++ci) f.cls_alpha[ci] = plan->desc.classes[ci][1];
@@ -379,7 +387,9 @@ int launch_quad_pipeline(const sck_plan* plan, const sck_buffers* buf, int n_swe
   pp.Q = plan->Bp / 4;
   pp.ngroups = (pp.Q + pp.group - 1) / pp.group;
   pp.blocks_x = quad_blocks_x(plan);
-  pp.T = pp.group * pp.blocks_x;
+  pp.cpt = plan->quad_cpt > 0 ? plan->quad_cpt : 1;
+  pp.tq = quad_pipe_tickets(plan);
+  pp.T = pp.group * pp.tq;
   for (int ci = 0; ci < C; ++ci) {
     pp.cls[ci][0] = plan->desc.classes[ci][0];
     pp.cls[ci][1] = plan->desc.classes[ci][1];
@@ -430,7 +440,7 @@ int launch_quad_pipeline_measure(const sck_plan* plan, const sck_buffers* buf, i
   if (rc != SCK_OK) return rc;
   rc = launch_advance(buf->state, n_sweeps, s);
   if (rc != SCK_OK) return rc;
-  return launch_measure_finish(plan, workspace, E, M, s);
+  return launch_measure_finish(plan, workspace, E, M, s, quad_pipe_tickets(plan));
 }
 
 }  // namespace sck

@@ -58,12 +58,13 @@ struct QuadParams {
 struct QuadPipeParams {
   QuadParams p;
   int C, D, group, ngroups, units, sweep_base, T, Q, blocks_x;
+  int cpt, tq;              // site blocks of 256 threads per ticket, tickets per quad and class (T = group tq)
   int cls[8][2];
   unsigned* ticket;
   unsigned* done;           // finished tickets per (group, class), summed over the launch's sweeps
   unsigned wait_limit;      // polls of a completion counter before giving up
   int* giveup;              // host-mapped flag, set (system scope) when a wait gives up
-  // measure step: the launch's last sweep also writes FP64 partial sums [replica][class][site block][1 + N]
+  // measure step: the launch's last sweep also writes FP64 partial sums [replica][class][ticket][1 + N]
   double* partial;
   unsigned lower_groups[8];
   int B;
@@ -304,10 +305,58 @@ __device__ __forceinline__ void quad_site(const QuadParams& p, int q, int h, int
 template <int V>
 __device__ __forceinline__ void block_sum(double (&x)[V], double (*red)[8]);
 
+// FP64 warp sums of 16 values per lane by recursive halving: at offset o (16, 8, 4, 2) each lane keeps one half
+// of its remaining values, sends the other half to lane ^ o and adds what it receives; the last step (offset 1)
+// adds the pair's single values. Lane l ends with the warp total of value (l >> 1) & 15 in x[0]. 16 shuffles of
+// a double instead of 80; every total is the same fixed binary tree of additions on every call.
+__device__ __forceinline__ void warp_halving_sum16(double (&x)[16]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 16, h = 8; o >= 2; o >>= 1, h >>= 1) {
+    const bool hi = (lane & o) != 0;
+#pragma unroll
+    for (int i = 0; i < h; ++i) {
+      const double keep = hi ? x[i + h] : x[i];
+      const double send = hi ? x[i] : x[i + h];
+      x[i] = keep + __shfl_xor_sync(0xFFFFFFFFu, send, o);
+    }
+  }
+  x[0] += __shfl_xor_sync(0xFFFFFFFFu, x[0], 1);
+}
+
+// Measure-step epilogue of a block of 256 threads: the block totals of the (1 + N) values of each of the four
+// lanes of a quad, in a fixed order (warp halving sums, then the 8 warps in order); thread v < 4 (1 + N) gets
+// value v (lane v / (1 + N), component v % (1 + N)), the other threads 0. Every thread of the block must call it.
+template <int N>
+__device__ __forceinline__ double measure_block_sum(const MeasureAcc<N>& m) {
+  __shared__ double red[8][16];
+  double x[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) x[i] = 0.0;
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+#pragma unroll
+    for (int v = 0; v <= N; ++v) x[j * (1 + N) + v] = m.v[j][v];
+  warp_halving_sum16(x);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if ((lane & 1) == 0) red[warp][lane >> 1] = x[0];
+  __syncthreads();
+  double v = 0.0;
+  if (threadIdx.x < 4 * (1 + N)) {
+#pragma unroll
+    for (int w = 0; w < 8; ++w) v += red[w][threadIdx.x];
+  }
+  return v;
+}
+
+// Blocks of 256 threads per SM the class and pipeline kernels are compiled for (3: at most 85 registers).
+#ifndef SCK_QUAD_MIN_BLOCKS
+#define SCK_QUAD_MIN_BLOCKS 3
+#endif
+
 // Grid (ceil(L3 L2 L1 / P / 256), quads of this launch). Thread -> (row, position in the row's class segment).
-// At most 85 registers (three blocks of 256 threads per SM) for the sweep; 128 for measure launches.
 template <class Lat, int N, int P, int L1C, bool MEASURE>
-__global__ void __launch_bounds__(256, MEASURE ? 2 : 3) quad_class_kernel(const __grid_constant__ QuadParams p) {
+__global__ void __launch_bounds__(256, SCK_QUAD_MIN_BLOCKS) quad_class_kernel(const __grid_constant__ QuadParams p) {
   const Geometry& g = p.g;
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   uint32_t row, h;
@@ -340,23 +389,12 @@ __global__ void __launch_bounds__(256, MEASURE ? 2 : 3) quad_class_kernel(const 
   }
   if constexpr (MEASURE) {
     // every thread of the block reaches here: block sums in a fixed order, one partial per (replica, value)
-    __shared__ double red[4 * (1 + N)][8];
-    double x[4 * (1 + N)];
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int v = 0; v <= N; ++v) x[j * (1 + N) + v] = m.v[j][v];
-    block_sum<4 * (1 + N)>(x, red);
+    const double val = measure_block_sum<N>(m);
     if (threadIdx.x < 4 * (1 + N)) {
       const int j = threadIdx.x / (1 + N), v = threadIdx.x - j * (1 + N);
       const int rep = 4 * q + j;
-      if (rep < p.B) {
-        double val = 0.0;
-#pragma unroll
-        for (int i = 0; i < 4 * (1 + N); ++i)
-          if (i == (int)threadIdx.x) val = x[i];
+      if (rep < p.B)
         p.partial[(((size_t)rep * p.n_classes + p.measure_ci) * p.blocks_x + blockIdx.x) * (1 + N) + v] = val;
-      }
     }
   }
 }
@@ -374,7 +412,7 @@ struct PipeTask {
 };
 
 template <class Lat, int N, int P, int L1C, bool MEASURE>
-__global__ void __launch_bounds__(256, MEASURE ? 2 : 3) quad_pipe_kernel(const __grid_constant__ QuadPipeParams pp) {
+__global__ void __launch_bounds__(256, SCK_QUAD_MIN_BLOCKS) quad_pipe_kernel(const __grid_constant__ QuadPipeParams pp) {
   __shared__ PipeTask s;
   if (threadIdx.x == 0) {
     const unsigned tk = atomicAdd(pp.ticket, 1u);
@@ -389,10 +427,10 @@ __global__ void __launch_bounds__(256, MEASURE ? 2 : 3) quad_pipe_kernel(const _
     if (num >= 0 && num / pp.D < pp.units) {
       const int u = num / pp.D;
       const int sw = u / pp.ngroups, g = u - sw * pp.ngroups;
-      const int qi = j / pp.blocks_x;
+      const int qi = j / pp.tq;
       s.has = 1;
       s.q = g * pp.group + qi;
-      s.chunk = j - qi * pp.blocks_x;
+      s.chunk = j - qi * pp.tq;
       s.ci = ci;
       s.sweep = pp.sweep_base + sw;
       s.done_idx = g * pp.C + ci;
@@ -434,7 +472,11 @@ __global__ void __launch_bounds__(256, MEASURE ? 2 : 3) quad_pipe_kernel(const _
   if (s.go) {
     const QuadParams& p = pp.p;
     const Geometry& g = p.g;
-    const uint32_t t = (uint32_t)s.chunk * 256u + threadIdx.x;
+#pragma unroll 1
+    for (int c = 0; c < pp.cpt; ++c) {
+    const int chunk = s.chunk * pp.cpt + c;
+    if (chunk >= pp.blocks_x) break;
+    const uint32_t t = (uint32_t)chunk * 256u + threadIdx.x;
     uint32_t row, h;
     if constexpr (L1C > 0) {
       row = t / (uint32_t)(L1C / P);
@@ -464,33 +506,23 @@ __global__ void __launch_bounds__(256, MEASURE ? 2 : 3) quad_pipe_kernel(const _
         });
       }
     }
+    }
   }
   if constexpr (MEASURE) {
     if (measuring) {
-      __shared__ double red[4 * (1 + N)][8];
-      double x[4 * (1 + N)];
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-#pragma unroll
-        for (int v = 0; v <= N; ++v) x[j * (1 + N) + v] = m.v[j][v];
-      block_sum<4 * (1 + N)>(x, red);
+      const double val = measure_block_sum<N>(m);
       if (threadIdx.x < 4 * (1 + N) && s.q < pp.Q) {
         const int j = threadIdx.x / (1 + N), v = threadIdx.x - j * (1 + N);
         const int rep = 4 * s.q + j;
-        if (rep < pp.B) {
-          double val = 0.0;
-#pragma unroll
-          for (int i = 0; i < 4 * (1 + N); ++i)
-            if (i == (int)threadIdx.x) val = x[i];
-          pp.partial[(((size_t)rep * pp.C + s.ci) * pp.blocks_x + s.chunk) * (1 + N) + v] = val;
-        }
+        if (rep < pp.B) pp.partial[(((size_t)rep * pp.C + s.ci) * pp.tq + s.chunk) * (1 + N) + v] = val;
       }
     }
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    __threadfence();
-    atomicAdd(pp.done + s.done_idx, 1u);   // finished (or given up): later tasks of this group may start
+    // finished (or given up): later tasks of this group may start. The barrier orders every thread's stores
+    // before this release (cumulativity), so a block that acquires the count sees them.
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(pp.done + s.done_idx) : "memory");
   }
 }
 

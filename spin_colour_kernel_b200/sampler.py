@@ -158,11 +158,14 @@ class Sampler:
         L.check(L.lib().sck_plan_tune(self._plan, level, int(l2_budget), int(resident_limit)))
         return self.path()
 
-    def pipeline(self, group: int, skew: int = 2):
+    def pipeline(self, group: int, skew: int = 2, chunks: int | None = None):
         """Interleaved ('quad') layout only: run sweeps through the class-skewed L2 pipeline with groups of
         `group` replicas (a multiple of 4; 0 returns to class-by-class launches), class c of group-unit u at
-        position skew * u + c (include/sck.h, sck_plan_pipeline). The chain does not depend on it."""
+        position skew * u + c, each ticket covering `chunks` site blocks (include/sck.h, sck_plan_pipeline,
+        sck_plan_pipeline_chunks). The chain does not depend on it."""
         with torch.cuda.device(self.device):
+            if chunks is not None:
+                L.check(L.lib().sck_plan_pipeline_chunks(self._plan, int(chunks)))
             L.check(L.lib().sck_plan_pipeline(self._plan, int(group), int(skew)))
         return self.path()
 
@@ -557,10 +560,11 @@ class Sampler:
 class SamplerBatch:
     """Several samplers (different systems, sizes, masks, colourings, temperatures) swept together.
 
-    All samplers need the same storage (int8 Ising or float32 components of one spin dimension). Systems whose
-    replica fits `resident_limit` bytes of shared memory run every sweep of a call in one resident launch; the
-    rest run one launch per colour step for all of them (include/sck.h, sck_batch_*). Each sampler keeps its own
-    spins, temperatures, tables and counter; `sweep(n)` advances every sampler's counter by n.
+    All samplers need the same storage (int8 Ising or float32 components of one spin dimension). A call is one
+    persistent launch over per-system work descriptors: systems whose replica fits `resident_limit` bytes of
+    shared memory run every sweep of the call on-chip, the rest class by class, each class waiting for the one
+    before it in its own system (include/sck.h, sck_batch_*). Each sampler keeps its own spins, temperatures,
+    tables and counter; `sweep(n)` advances every sampler's counter by n.
     """
 
     def __init__(self, samplers: list, spins: list, resident_limit: int = 200 << 10):
@@ -595,6 +599,16 @@ class SamplerBatch:
     def sweep(self, n: int = 1):
         with torch.cuda.device(self.device):
             L.check(L.lib().sck_batch_sweep(self._batch, _ptr(self._ws), int(n), self.samplers[0]._stream()))
+
+    def set_wait_limit(self, polls: int):
+        """Polls of a class wait before a block gives up (failure-detection tests shorten it)."""
+        L.check(L.lib().sck_batch_set_wait_limit(self._batch, int(polls)))
+
+    def check_waits(self):
+        """Synchronise and raise SckError (SCK_ERR_TIMEOUT) when a wait of the batch kernel gave up since the last
+        check (its sites were left unchanged); clears the condition."""
+        with torch.cuda.device(self.device):
+            L.check(L.lib().sck_batch_wait_status(self._batch, self.samplers[0]._stream()))
 
     def graph(self, k: int):
         """Capture k sweeps of the whole batch in a CUDA graph; returns its replay."""

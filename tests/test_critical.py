@@ -54,3 +54,54 @@ def test_series_of_an_ising_size_matches_the_reference():
     # with graphs the chain gains the capture's warm-up sweep; the series keeps its shape and range
     E2, m22, _ = CR.series(sy.ising("square", 8), 8, np.array([2.1, 2.269, 2.45]), 3, 20, 12, 2, device="cuda")
     assert E2.shape == E.shape and np.all((m22 >= 0) & (m22 <= 1))
+
+
+def test_holm_adjustment():
+    """Holm's step-down adjustment: each p times the hypotheses not yet rejected, monotone, capped at 1."""
+    assert np.allclose(CR.holm([0.01, 0.04, 0.03]), [0.03, 0.06, 0.06])
+    assert np.allclose(CR.holm([0.5, 0.9]), [1.0, 1.0])
+    assert np.allclose(CR.holm([0.001]), [0.001])
+
+
+def test_crossing_estimate_extrapolates_pair_crossings():
+    """On synthetic series whose reweighted Binder curves cross, the estimate is the intercept of the pair
+    crossings against sqrt(L1 L2)^-x (three sizes, two pairs), and a single pair gives its own crossing."""
+    rng = np.random.default_rng(0)
+    temps = np.linspace(2.2, 2.34, 5)
+    data = {}
+    for L in (8, 16, 32):
+        E = rng.normal(-1.5 * L * L, 0.5 * L, size=(5, 3, 200))
+        m2 = np.abs(rng.normal(0.5, 0.05, size=(5, 3, 200)))
+        m4 = m2 ** 2 * (1.0 + 0.1 * (np.arange(5)[:, None, None] - 2) * (L / 16.0))
+        data[L] = {"E": E, "m2": m2, "m4": m4, "temps": temps}
+    est, cross, curves = CR.crossing_estimate(data, 2.0)
+    assert len(curves) == 2
+    if len(cross) >= 2:
+        X = np.array([l ** -2.0 for l, _ in cross])
+        Y = np.array([t for _, t in cross])
+        assert est == pytest.approx(float(np.polyfit(X, Y, 1)[1]))
+    one = {16: data[16], 32: data[32]}
+    e1, c1, _ = CR.crossing_estimate(one, 2.0)
+    assert (np.isnan(e1) and not c1) or e1 == pytest.approx(c1[-1][1])
+
+
+@pytest.mark.gpu
+def test_e4_driver_runs_a_small_study(tmp_path):
+    """The multi-size driver end to end on two small square Ising sizes: probes, series files, crossings, the
+    bootstrap interval, Holm's adjustment and a verdict, written to <tag>.json."""
+    import json
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    out = CR.e4(tmp_path, sizes2d=(8, 16), seeds=4, meas=600, boots=40, only=("Ising square",), probe_cap=2000,
+                probe_start=500, tag="E4small", log=lambda *_: None)
+    assert (tmp_path / "E4small.json").exists()
+    assert json.loads((tmp_path / "E4small.json").read_text())["rows"][0]["system"] == "Ising square"
+    assert sorted(p.name for p in tmp_path.glob("E4small-*.npz")) == ["E4small-Ising_square-L16.npz",
+                                                                     "E4small-Ising_square-L8.npz"]
+    r = out["rows"][0]
+    assert r["sizes"] == [8, 16] and r["verdict"] in ("supported", "not supported", "inconclusive")
+    assert 0.0 <= r["p_holm"] <= 1.0
+    assert np.isfinite(r["estimate"]) and abs(r["estimate"] / r["T_ref"] - 1) < 0.05, r["estimate"]
+    d = np.load(tmp_path / "E4small-Ising_square-L16.npz")
+    assert d["E"].shape[:2] == (9, 4) and len(d["temps"]) == 9

@@ -244,41 +244,46 @@ def test_learned_rounds_keep_the_boltzmann_distribution():
 
 
 def test_trained_network_decorrelates_faster_than_untrained():
-    """What training gains. On a 16^3 lattice at T = 4.5115, block rounds (one colour step per block colour,
-    then one plain sweep) with a network trained on the plain chain's blocks are accepted far more often and
-    decorrelate |M| faster (smaller tau_int, Sokal window over 128 chains) than the same rounds with the
-    untrained network, whose proposals are almost never accepted (its rounds are plain sweeps in all but name)."""
+    """What training gains. On a 32^3 lattice at T = 4.5115, block rounds (one colour step per block colour,
+    then one plain sweep) with a network trained on the plain chain's blocks against the same rounds with the
+    untrained network: the trained proposals are accepted for about half of all blocks (the untrained ones
+    almost never), and the chain decorrelates faster: smaller tau_int of E and of |M| (Sokal window over 64
+    chains of 3000 rounds). The gain is modest at these sizes: the block moves leave the long-wavelength modes
+    to the plain sweeps."""
     _need_gpu()
     from spin_colour_kernel_b200 import stats
     from spin_colour_kernel_b200 import system as sy
     from spin_colour_kernel_b200.learned import BlockProposal
     from spin_colour_kernel_b200.sampler import Sampler
-    L, R, T, K = 16, 128, 4.5115, 1500
+    L, R, T, K = 32, 64, 4.5115, 3000
     s = sy.ising("sc", L)
     A = Sampler(s, R, device="cuda", seed=31, packed=False)
     A.set_temperature(torch.full((R,), T))
     S = A.init_spins(seed=4)
-    A.sweep(S, 500)
+    A.sweep(S, 1000)
     beta = torch.full((R,), 1.0 / T, dtype=torch.float32, device="cuda")
     trained = BlockProposal(L, R, groups=16, seed=9)
     data = []
     for _ in range(8):
         A.sweep(S, 25)
         data.append(trained.gather(S))
-    trained.train(torch.cat(data), steps=600, batch=4096, lr=2e-3)
+    trained.train(torch.cat(data), steps=800, batch=4096, lr=2e-3)
     untrained = BlockProposal(L, R, groups=16, seed=9)
     out = {}
     for name, P in (("trained", trained), ("untrained", untrained)):
         X = S.clone()
         acc = torch.zeros(R, dtype=torch.int32, device="cuda")
         Ms = torch.empty((K, R), dtype=torch.float64, device="cuda")
+        Es = torch.empty((K, R), dtype=torch.float64, device="cuda")
         for r in range(K):
             P.round(X, beta, seed=13, rnd=r, accepted=acc)
             A.sweep(X, 1)
-            _, M = A.observables(X)
+            E, M = A.observables(X)
             Ms[r].copy_(M.reshape(R).abs())
-        series = Ms.cpu().numpy() / L ** 3
-        out[name] = (stats.integrated_tau(series), acc.sum().item() / (K * R * (L // 4) ** 3))
-    (tau_t, acc_t), (tau_u, acc_u) = out["trained"], out["untrained"]
-    assert acc_t > 0.1 and acc_t > 20 * acc_u, out
-    assert tau_t < 0.75 * tau_u, out
+            Es[r].copy_(E)
+        out[name] = {"tau_M": stats.integrated_tau(Ms.cpu().numpy() / L ** 3),
+                     "tau_E": stats.integrated_tau(Es.cpu().numpy() / L ** 3),
+                     "acceptance": acc.sum().item() / (K * R * (L // 4) ** 3)}
+    t_, u_ = out["trained"], out["untrained"]
+    assert t_["acceptance"] > 0.3 and t_["acceptance"] > 50 * u_["acceptance"], out
+    assert t_["tau_E"] < 0.95 * u_["tau_E"] and t_["tau_M"] < u_["tau_M"], out

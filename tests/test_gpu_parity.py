@@ -412,6 +412,49 @@ def test_ragged_batch_equals_individual_samplers(resident_limit):
         assert int(A.state[1]) == 6
 
 
+def test_ragged_batch_wait_that_gives_up_reports_timeout():
+    """The persistent batch kernel orders each system's classes by completion counters; with zero polls an item
+    whose class predecessor has not finished gives up, the batch reports SCK_ERR_TIMEOUT (sweeps refused until
+    the status is read), and with the default limit restored it again equals the systems swept on their own."""
+    from spin_colour_kernel_b200 import workloads as W
+    from spin_colour_kernel_b200.sampler import Sampler, SamplerBatch
+    specs = [("square", 64, False, 0.7), ("triangular", 48, True, 1.1)]
+    rng = np.random.default_rng(5)
+    samplers, spins, refs, ref_spins = [], [], [], []
+    for i, (crystal, side, disk, T) in enumerate(specs):
+        s = W.xy_system(crystal, side, disk)
+        A, R = Sampler(s, 4, device="cuda", seed=50 + i), Sampler(s, 4, device="cuda", seed=50 + i)
+        R.tune(0, 0, 0)
+        for X in (A, R):
+            X.set_temperature(T)
+        S = torch.from_numpy(W.xy_angles(s, 4, rng)).cuda()
+        samplers.append(A)
+        spins.append(S)
+        refs.append(R)
+        ref_spins.append(S.clone())
+    batch = SamplerBatch(samplers, spins, resident_limit=0)    # every system streams: every class waits
+    batch.set_wait_limit(0)
+    batch.sweep(3)
+    torch.cuda.synchronize()
+    with pytest.raises(L.SckError) as e:
+        batch.sweep(1)
+    assert e.value.code == L.ERR_TIMEOUT
+    with pytest.raises(L.SckError) as e:
+        batch.check_waits()
+    assert e.value.code == L.ERR_TIMEOUT
+    batch.check_waits()
+    batch.set_wait_limit(1 << 20)
+    for A, R, S, S2 in zip(samplers, refs, spins, ref_spins):
+        A.state.copy_(R.state)
+        S2.copy_(S)
+    batch.sweep(3)
+    for R, S in zip(refs, ref_spins):
+        R.sweep(S, 3)
+    batch.check_waits()
+    for S, S2 in zip(spins, ref_spins):
+        assert torch.equal(S, S2)
+
+
 def test_graph_replay_equals_plain_sweeps():
     from spin_colour_kernel_b200.sampler import Sampler
     s = C.heisenberg_bcc_j1j2(sy, cr, 6)

@@ -283,6 +283,31 @@ def test_pipeline_equals_class_by_class(label, make, B, group, skew):
     assert int(A.state[1]) == 6
 
 
+@pytest.mark.parametrize("chunks", [1, 3, 64])
+def test_pipeline_ticket_size_does_not_change_the_chain(chunks):
+    """Tickets of 1, 3 (a partial last ticket per quad and class) and 64 site blocks (one ticket per quad and
+    class): the same spins as class-by-class launches, and the same measure-step observables."""
+    s = sy.System("Heisenberg bcc", 3, cr.make("bcc", (1, 2)), (32, 16, 16), (True,) * 3, {1: 1.0, 2: 0.3},
+                  h=(0.0, 0.0, 0.1))
+    B = 20
+    A, R = _quad(s, B, seed=5), _quad(s, B, seed=5)
+    A.pipeline(4, 2, chunks)
+    for X in (A, R):
+        X.set_temperature(torch.linspace(0.5, 3.0, B))
+    S1, S2 = A.init_spins(seed=3), R.init_spins(seed=3)
+    A.sweep(S1, 3)
+    R.sweep(S2, 3)
+    assert torch.equal(S1, S2)
+    E1, M1 = A.sweep_measure(S1, 2)
+    E2, M2 = R.sweep_measure(S2, 2)
+    assert torch.equal(S1, S2)
+    np.testing.assert_allclose(E1.cpu().numpy(), E2.cpu().numpy(), rtol=1e-12, atol=1e-9)
+    np.testing.assert_allclose(M1.cpu().numpy(), M2.cpu().numpy(), rtol=1e-12, atol=1e-9)
+    A.check_waits()
+    with pytest.raises(ValueError):
+        A.pipeline(4, 2, 0)
+
+
 def test_pipeline_refuses_bad_groups_and_skews():
     s = C.heisenberg_bcc_j1j2(sy, cr, 8)          # 4 classes
     A = _quad(s, 16, seed=1)
@@ -364,5 +389,39 @@ def test_autotuned_schedule_is_bit_identical_and_cached(tmp_path, monkeypatch):
     assert torch.equal(S1, S2)
     B = _quad(s, 64, seed=31)
     c2 = at.autotune(B, B.init_spins(seed=1))
-    assert c2["cached"] and (c2["group"], c2["skew"]) == (c["group"], c["skew"])
+    assert c2["cached"] and (c2["group"], c2["skew"], c2["chunks"]) == (c["group"], c["skew"], c["chunks"])
     assert B.path()["group"] == c["group"]
+
+
+def test_autotuned_batch_is_bit_identical_and_cached(tmp_path, monkeypatch):
+    """The batch autotuner times the persistent batch kernel at several resident limits (which systems run
+    on-chip), restores every counter, returns the fastest batch, caches the choice, and the tuned batch continues
+    the chains of the systems swept on their own."""
+    from spin_colour_kernel_b200 import autotune as at
+    from spin_colour_kernel_b200 import workloads as W
+    from spin_colour_kernel_b200.sampler import Sampler
+    monkeypatch.setenv("SCK_TUNE_CACHE", str(tmp_path / "tune.json"))
+    rng = np.random.default_rng(9)
+    specs = [("square", 16, False, 0.7), ("triangular", 45, True, 1.0), ("square", 96, False, 0.9)]
+    samplers, spins, refs, ref_spins = [], [], [], []
+    for i, (crystal, L, disk, T) in enumerate(specs):
+        s = W.xy_system(crystal, L, disk)
+        A, R = Sampler(s, 4, device="cuda", seed=70 + i), Sampler(s, 4, device="cuda", seed=70 + i)
+        R.tune(0, 0, 0)
+        for X in (A, R):
+            X.set_temperature(T)
+        S = torch.from_numpy(W.xy_angles(s, 4, rng)).cuda()
+        samplers += [A]
+        spins += [S]
+        refs += [R]
+        ref_spins += [S.clone()]
+    batch, c = at.autotune_batch(samplers, spins, sweeps=2)
+    assert not c["cached"] and len(c["tried"]) >= 2
+    assert all(int(A.state[1]) == 0 for A in samplers)
+    batch.sweep(3)
+    for R, S in zip(refs, ref_spins):
+        R.sweep(S, 3)
+    for S, S2 in zip(spins, ref_spins):
+        assert torch.equal(S, S2)
+    _, c2 = at.autotune_batch(samplers, spins)
+    assert c2["cached"] and c2["resident_limit"] == c["resident_limit"]

@@ -72,10 +72,10 @@ def test_group_pipeline_wait_that_gives_up_reports_timeout():
     _need_gpu()
     from spin_colour_kernel_b200.sampler import Sampler
     s = C.heisenberg_bcc_j1j2(sy, cr, 16)
-    B = 8
+    B = 16
     A, R = Sampler(s, B, device="cuda", seed=21, packed=False), Sampler(s, B, device="cuda", seed=21, packed=False)
     per_rep = s.nsite * s.n * 4
-    assert A.tune(True, len(A.classes) * per_rep * 2, 0)["group"] == 2   # four groups of two replicas
+    assert A.tune(True, len(A.classes) * per_rep * 2, 0)["group"] == 2   # eight groups of two replicas
     R.tune(True, 0, 0)
     for X in (A, R):
         X.set_temperature(torch.linspace(0.3, 3.0, B))
