@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "site.cuh"
+#include "spec_site.cuh"
 
 namespace sck {
 
@@ -42,7 +43,10 @@ struct SysDev {
   int n_classes;
   int classes[kBatchMaxClasses][2];
   int resident;
-  int chunks;          // streaming items of one class and replica (kBatchItemPasses x 256 class sites each)
+  int chunks;          // streaming items of one class and replica slot (kBatchItemPasses x 256 class sites each)
+  int rpi;             // replicas per streaming item: 2 for vector models (a pair in packed float32x2), 1 Ising
+  int spec, per;       // compile-time lattice table of the system (0: generic site update), periodic wrap
+  float J[SCK_MAX_BASIS][SCK_MAX_GROUPS];
 };
 
 struct BatchLayout {   // offsets into the workspace
@@ -114,6 +118,33 @@ __device__ __forceinline__ unsigned batch_ld_acquire(const unsigned* a) {
   return v;
 }
 
+// The site update of a streaming item: the specialised lattice update (the lattice kernels' arithmetic, a
+// replica pair per thread for vector models) for systems on the square, triangular or simple cubic table, else
+// the generic update of each replica of the slot.
+template <class Lat, int N, typename ST>
+__device__ __forceinline__ void batch_spec_site(const SysDev& d, int rep0, int x, int y, int z, int32_t key) {
+  auto run = [&](auto per_c) {
+    constexpr bool PER = decltype(per_c)::value;
+    if constexpr (N == 1)
+      ising_spec_site<Lat, 0, ST, PER>(d.c, rep0, x, y, z, key);
+    else
+      vec_spec_pair<Lat, 0, N, PER, 0>(d.c, d.J[0], rep0, rep0 + 1 < d.c.B, x, y, z, key);
+  };
+  if (d.per) run(std::true_type{});
+  else run(std::false_type{});
+}
+
+template <int N, typename ST>
+__device__ __forceinline__ void batch_stream_site(const SysDev& d, int alpha, int rep0, int x, int y, int z,
+                                                  int32_t key) {
+  if (d.spec == Lat_square_1::id) return batch_spec_site<Lat_square_1, N, ST>(d, rep0, x, y, z, key);
+  if (d.spec == Lat_triangular_1::id) return batch_spec_site<Lat_triangular_1, N, ST>(d, rep0, x, y, z, key);
+  if (d.spec == Lat_sc_1::id) return batch_spec_site<Lat_sc_1, N, ST>(d, rep0, x, y, z, key);
+  ST* base = (ST*)d.c.dst;
+  for (int r = rep0; r < rep0 + d.rpi && r < d.c.B; ++r)
+    batch_site<N, ST>(d.c, d.sub[alpha], alpha, r, x, y, z, key, base + (size_t)r * N * d.c.g.nsite);
+}
+
 struct BatchItem {
   int kind;      // 0: no more work, 1: resident, 2: streaming, 3: streaming item whose wait gave up
   int s, rep, chunk, k, sw;
@@ -151,7 +182,7 @@ __global__ void __launch_bounds__(256) batch_persistent_kernel(const BatchDevPar
         it.rep = j / d.chunks;
         it.chunk = j - it.rep * d.chunks;
         // the class this item follows: k - 1 of this sweep, or the last class of the previous sweep
-        const unsigned per = (unsigned)d.chunks * (unsigned)d.c.B;
+        const unsigned per = (unsigned)d.chunks * (unsigned)((d.c.B + d.rpi - 1) / d.rpi);
         const unsigned* dep = nullptr;
         unsigned need = 0;
         if (k > 0) {
@@ -203,13 +234,13 @@ __global__ void __launch_bounds__(256) batch_persistent_kernel(const BatchDevPar
         const uint32_t per = (uint32_t)d.c.rows * (uint32_t)d.c.bx;
         const int colour = d.classes[it.k][0], alpha = d.classes[it.k][1];
         const int32_t key = sweep_key_at(d.c.state, p.sweep_base + it.sw);
-        ST* spins = (ST*)d.c.dst + (size_t)it.rep * N * d.c.g.nsite;
+        const int rep0 = it.rep * d.rpi;
 #pragma unroll 1
         for (int pass = 0; pass < kBatchItemPasses; ++pass) {
           const uint32_t t = ((uint32_t)it.chunk * kBatchItemPasses + pass) * 256u + threadIdx.x;
           int x, y, z;
           if (t < per && class_site(d.c, colour, alpha, t, x, y, z))
-            batch_site<N, ST>(d.c, d.sub[alpha], alpha, it.rep, x, y, z, key, spins);
+            batch_stream_site<N, ST>(d, alpha, rep0, x, y, z, key);
         }
       }
       __syncthreads();
@@ -424,11 +455,19 @@ int sck_batch_bind(sck_batch* b, const sck_buffers* buffers, void* workspace, vo
     d.resident = b->resident[s];
     const long long per = (long long)d.c.rows * d.c.bx;
     d.chunks = (int)((per + 256 * kBatchItemPasses - 1) / (256 * kBatchItemPasses));
+    d.rpi = plan->geom.n == 1 ? 1 : 2;
+    const bool table = plan->spec == Lat_square_1::id || plan->spec == Lat_triangular_1::id ||
+                       plan->spec == Lat_sc_1::id;
+    d.spec = table ? plan->spec : 0;
+    d.per = table ? spec_periodic_box(plan) : 0;
+    for (int a = 0; a < SCK_MAX_BASIS; ++a)
+      for (int gi = 0; gi < SCK_MAX_GROUPS; ++gi) d.J[a][gi] = plan->sub[a].J[gi];
     res_off[s] = (int)res_total;
     if (d.resident) res_total += plan->Bp;
+    const long long slots = (plan->Bp + d.rpi - 1) / d.rpi;
     for (int k = 0; k < b->max_classes; ++k) {
       step_off[k * (b->n + 1) + s] = (int)step_total[k];
-      if (!d.resident && k < d.n_classes) step_total[k] += (long long)d.chunks * plan->Bp;
+      if (!d.resident && k < d.n_classes) step_total[k] += (long long)d.chunks * slots;
     }
   }
   res_off[b->n] = (int)res_total;

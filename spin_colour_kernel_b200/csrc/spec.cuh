@@ -183,6 +183,10 @@ __device__ __forceinline__ void finish_pair(const Common& c, int own, int rep0, 
                  make_float2(c.beta[rep0], c.beta[rep1]), key, s, v, t, acc0, acc1);
 }
 
+// 1 when the plan's compile-time lattice table applies with the branch-free periodic wrap (every axis periodic,
+// extents at least the table's reach), else 0 (fast_sweep.cu).
+int spec_periodic_box(const sck_plan* plan);
+
 // Segment kernels (segment.cu): eligibility and the task launch.
 bool seg_kernel_ok(const sck_plan* plan);
 int launch_seg_tasks(const sck_plan* plan, SpecParams& p, int ys, cudaStream_t s);

@@ -19,37 +19,37 @@ from .colouring import Colouring, search, seam_ok, verify_on_box
 @dataclass
 class System:
     name: str
-    n: int                                   # spin components: 1 Ising, 2 XY, 3 Heisenberg
+    n: int                                   # components per spin (Ising 1, XY 2, Heisenberg 3)
     crystal: cr.Crystal
-    box: tuple[int, ...]                     # (L1, L2[, L3]) cells
+    box: tuple[int, ...]                     # cells along each lattice axis, x first
     periodic: tuple[bool, ...]
-    J: dict[int, float]                      # isotropic exchange per shell
-    extra: dict[int, np.ndarray] = field(default_factory=dict)   # bond index -> extra n x n matrix (DMI ...)
-    h: tuple[float, ...] | None = None       # uniform field
-    cubic_k1: np.ndarray | None = None       # per-site cubic anisotropy K1, shape (b, L3, L2, L1)
-    cubic_k2: float = 0.0                    # (sx sy sz)^2 coefficient
-    mask: np.ndarray | None = None           # bool (b, L3, L2, L1); False = no spin
+    J: dict[int, float]                      # shell number -> scalar coupling
+    extra: dict[int, np.ndarray] = field(default_factory=dict)   # bond position -> added n x n coupling (e.g. DMI)
+    h: tuple[float, ...] | None = None       # external field, the same on every site
+    cubic_k1: np.ndarray | None = None       # K1 of the cubic anisotropy at every site, (b, L3, L2, L1)
+    cubic_k2: float = 0.0                    # K2, multiplying (sx sy sz)^2
+    mask: np.ndarray | None = None           # (b, L3, L2, L1) bool, True where a spin lives
     colouring: Colouring | None = None
-    T_ref: float | None = None               # reference critical temperature, when one exists
-    acceptance: str = "metropolis"           # "metropolis": u < exp(-beta dE); "barker": u (1 + exp(beta dE)) < 1
+    T_ref: float | None = None               # known critical temperature of the model, if any
+    acceptance: str = "metropolis"           # "metropolis" (u < exp(-beta dE)) or "barker" (u (1 + exp(beta dE)) < 1)
 
     def __post_init__(self):
         if self.n not in (1, 2, 3):
-            raise ValueError("n must be 1, 2 or 3")
+            raise ValueError("a spin has 1, 2 or 3 components (n)")
         if len(self.box) != self.crystal.D or len(self.periodic) != self.crystal.D:
-            raise ValueError("box and periodic must have one entry per lattice axis")
+            raise ValueError("box and periodic need as many entries as the crystal has axes")
         if self.cubic_k1 is not None and self.n != 3:
-            raise ValueError("cubic anisotropy needs n = 3")
+            raise ValueError("cubic anisotropy is defined for three-component spins only")
         if self.acceptance not in ("metropolis", "barker"):
-            raise ValueError("acceptance must be 'metropolis' or 'barker'")
+            raise ValueError("acceptance is 'metropolis' or 'barker'")
         if self.colouring is None:
             self.colouring = search(self.crystal, self.box, self.periodic)
             if self.colouring is None:
-                raise ValueError(f"{self.name}: no seam-compatible linear colouring for box {self.box}")
+                raise ValueError(f"{self.name}: the search found no linear colouring that closes across the seams of box {self.box}")
         if not seam_ok(self.colouring, self.box, self.periodic):
-            raise ValueError(f"{self.name}: colouring violates the seam condition on box {self.box}")
+            raise ValueError(f"{self.name}: the colouring does not close across the periodic seams of box {self.box}")
         if not verify_on_box(self.colouring, self.crystal, self.box, self.periodic):
-            raise ValueError(f"{self.name}: colouring is not admissible on the box")
+            raise ValueError(f"{self.name}: a bond of the box joins two sites of one colour")
 
     # ---------------------------------------------------------------- geometry
     @property
@@ -129,8 +129,8 @@ def nanodot(Rd: float = 18.30, L: int = 5, Jex=1.0, Kan1=0.177, Kan2=0.034, KanS
     N = 2 * half + 1
     xs = np.arange(-half, half + 1)
     xg, yg = np.meshgrid(xs, xs, indexing="xy")
-    disk = (xg ** 2 + yg ** 2) <= Rd ** 2                 # [y, x]
-    mask = np.broadcast_to(disk, (L, N, N)).copy()[None]  # (1, L, N, N)
+    disk = (xg ** 2 + yg ** 2) <= Rd ** 2                 # indexed [y, x]
+    mask = np.broadcast_to(disk, (L, N, N)).copy()[None]  # one sublattice, L layers of the disc
     # in-disc first neighbours per site: y and x wrap (the disc never reaches the edge), z is open
     count = np.zeros(mask.shape[1:], np.int64)
     m3 = mask[0]
@@ -166,7 +166,7 @@ def nanodot(Rd: float = 18.30, L: int = 5, Jex=1.0, Kan1=0.177, Kan2=0.034, KanS
                   mask=mask)
 
 
-# Reference critical temperatures (J = kB = 1).
+# Known critical temperatures in units J = kB = 1 (sources beside each value).
 TC = {
     "Ising square": 2.0 / np.log(1 + np.sqrt(2)),
     "Ising triangular": 4.0 / np.log(3.0),

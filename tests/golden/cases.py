@@ -173,3 +173,15 @@ RUN_CFG = dict(model="ising", crystal="square", box=[6, 6], periodic=[True, True
                shape="rho <= 2.6", states=[{"name": "a", "J": {"1": 1.0}}, {"name": "b", "J": {"1": 1.0}, "H": 0.2}],
                replicas=5, T_max=3.0, T_min=2.0, T_step=0.5, thermalization=3, measurement=3, measure_every=1,
                units="reduced", seed=1)
+
+
+def batch_twin_tune(R, resident_limit):
+    """Tune sampler R (of one system of a ragged batch) to the path that runs the batch's site update for it: the
+    generic resident kernel when the batch keeps the system on-chip, the lattice kernels when the system is on the
+    square, triangular or simple cubic table (the batch streams those with the lattice kernels' update), else
+    the generic class kernels."""
+    if R.sys.nsite * R.sys.n * 4 <= resident_limit:
+        return R.tune(0, 0, resident_limit)
+    if R.sys.crystal.name in ("square", "triangular", "sc") and R.tune(1, 0, 0)["specialised"] > 0:
+        return R.tune(1, 0, 0)
+    return R.tune(0, 0, 0)

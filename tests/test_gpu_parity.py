@@ -387,7 +387,7 @@ def test_ragged_batch_equals_individual_samplers(resident_limit):
         B = 3 + i % 2
         A = Sampler(s, B, device="cuda", seed=100 + i)
         R = Sampler(s, B, device="cuda", seed=100 + i)
-        R.tune(0, 0, resident_limit)
+        C.batch_twin_tune(R, resident_limit)
         for X in (A, R):
             X.set_temperature(T)
         S = torch.from_numpy(W.xy_angles(s, B, rng)).cuda()
@@ -424,7 +424,7 @@ def test_ragged_batch_wait_that_gives_up_reports_timeout():
     for i, (crystal, side, disk, T) in enumerate(specs):
         s = W.xy_system(crystal, side, disk)
         A, R = Sampler(s, 4, device="cuda", seed=50 + i), Sampler(s, 4, device="cuda", seed=50 + i)
-        R.tune(0, 0, 0)
+        C.batch_twin_tune(R, 0)
         for X in (A, R):
             X.set_temperature(T)
         S = torch.from_numpy(W.xy_angles(s, 4, rng)).cuda()

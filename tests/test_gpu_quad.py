@@ -407,7 +407,6 @@ def test_autotuned_batch_is_bit_identical_and_cached(tmp_path, monkeypatch):
     for i, (crystal, L, disk, T) in enumerate(specs):
         s = W.xy_system(crystal, L, disk)
         A, R = Sampler(s, 4, device="cuda", seed=70 + i), Sampler(s, 4, device="cuda", seed=70 + i)
-        R.tune(0, 0, 0)
         for X in (A, R):
             X.set_temperature(T)
         S = torch.from_numpy(W.xy_angles(s, 4, rng)).cuda()
@@ -417,6 +416,8 @@ def test_autotuned_batch_is_bit_identical_and_cached(tmp_path, monkeypatch):
         ref_spins += [S.clone()]
     batch, c = at.autotune_batch(samplers, spins, sweeps=2)
     assert not c["cached"] and len(c["tried"]) >= 2
+    for R in refs:
+        C.batch_twin_tune(R, c["resident_limit"])
     assert all(int(A.state[1]) == 0 for A in samplers)
     batch.sweep(3)
     for R, S in zip(refs, ref_spins):
