@@ -294,8 +294,8 @@ int sck_unpack(const sck_plan* plan, const int32_t* words, const int8_t* mask, i
  * storage mode (int8 or float32) and one spin dimension, of different crystal, size, mask, colouring and
  * temperatures, swept together. A call is one persistent launch driven by the per-system descriptors: blocks take
  * work items in ticket order; systems whose replica takes at most resident_limit_bytes of shared memory are one
- * item per replica that runs every sweep of the call on-chip, the others one item per (sweep, class, replica,
- * 256-site chunk), each waiting (bounded) for the class it follows in its own system to finish.
+ * item per replica that runs every sweep of the call on-chip, the others one item per (sweep, class, replica
+ * slot, 2,048-site chunk), each waiting (bounded) for the class it follows in its own system to finish.
  *   sck_batch_workspace_size  device bytes of the per-system descriptors and the call's counters (caller-owned
  *                             workspace; one call at a time per workspace);
  *   sck_batch_bind            write the descriptors for these per-system buffers (a host-to-device copy on

@@ -6,8 +6,8 @@
 // resident capacity of the GPU whose blocks take work items in ticket order from a counter:
 //   - resident items (system, replica), for systems whose replica fits shared memory: the block loads the
 //     replica once and runs every class of every sweep of the call on-chip;
-//   - streaming items (sweep, colour step k, system, replica, 256-site chunk) for the others, found by binary
-//     searches over per-step item offsets. Before touching spins, a block waits (bounded) until every item of the
+//   - streaming items (sweep, colour step k, system, replica slot, 2,048-site chunk) for the others, found by
+//     binary searches over per-step item offsets. Before touching spins, a block waits (bounded) until every item of the
 //     class its item follows is done: class k - 1 of the same system and sweep, or the system's last class of the
 //     previous sweep; per-(system, class) completion counters count finished items. That class holds smaller
 //     tickets, taken by blocks that are running or done, so every wait ends, and each system's classes are
@@ -34,7 +34,7 @@ __device__ __forceinline__ void batch_site(const Common& c, const SubDev& sub, i
 }
 
 constexpr int kBatchMaxSystems = 256;
-constexpr int kBatchItemPasses = 4;   // a streaming item: 4 x 256 class sites of one replica and class
+constexpr int kBatchItemPasses = 8;   // a streaming item: 8 x 256 class sites of one replica slot and class
 constexpr int kBatchMaxClasses = 32;
 
 struct SysDev {
@@ -150,9 +150,10 @@ struct BatchItem {
   int s, rep, chunk, k, sw;
 };
 
-// The persistent batch kernel: 256 threads per block, dynamic shared memory for the largest resident replica.
+// The persistent batch kernel: 256 threads per block (at most 64 registers: four blocks per SM when the
+// resident replicas allow), dynamic shared memory for the largest resident replica.
 template <int N, typename ST>
-__global__ void __launch_bounds__(256) batch_persistent_kernel(const BatchDevParams p) {
+__global__ void __launch_bounds__(256, 4) batch_persistent_kernel(const BatchDevParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ BatchItem it;
   const long long total = (long long)p.res_items + (long long)p.n_sweeps * p.step_items;

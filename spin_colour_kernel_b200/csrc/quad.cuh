@@ -353,10 +353,13 @@ __device__ __forceinline__ double measure_block_sum(const MeasureAcc<N>& m) {
 #ifndef SCK_QUAD_MIN_BLOCKS
 #define SCK_QUAD_MIN_BLOCKS 3
 #endif
+#ifndef SCK_QUAD_MEASURE_MIN_BLOCKS
+#define SCK_QUAD_MEASURE_MIN_BLOCKS 3
+#endif
 
 // Grid (ceil(L3 L2 L1 / P / 256), quads of this launch). Thread -> (row, position in the row's class segment).
 template <class Lat, int N, int P, int L1C, bool MEASURE>
-__global__ void __launch_bounds__(256, SCK_QUAD_MIN_BLOCKS) quad_class_kernel(const __grid_constant__ QuadParams p) {
+__global__ void __launch_bounds__(256, MEASURE ? SCK_QUAD_MEASURE_MIN_BLOCKS : SCK_QUAD_MIN_BLOCKS) quad_class_kernel(const __grid_constant__ QuadParams p) {
   const Geometry& g = p.g;
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   uint32_t row, h;
