@@ -142,6 +142,25 @@ __device__ __forceinline__ int wrap_once(int v, int L) {
   return v;
 }
 
+// Compile-time box extents of a kernel instantiation: L1C > 0 fixes the row length L1; L1C < 0 fixes a cubic
+// box of edge -L1C (a power of two: L1 = L2 = L3, so the y and z wraps are bit masks and every extent, plane
+// and site count is a constant); 0 leaves everything to the runtime geometry.
+template <int L1C>
+struct QDim {
+  static constexpr int E = L1C < 0 ? -L1C : L1C;
+  static constexpr bool cube = L1C < 0;
+  __device__ __forceinline__ static int L1(const Geometry& g) { return E ? E : g.L1; }
+  __device__ __forceinline__ static int L2(const Geometry& g) { return cube ? E : g.L2; }
+  __device__ __forceinline__ static int L3(const Geometry& g) { return cube ? E : g.L3; }
+  // v in [-1, L]: one step outside the box at most
+  __device__ __forceinline__ static int wrap_y(int v, const Geometry& g) {
+    return cube ? (v & (E - 1)) : wrap_once(v, g.L2);
+  }
+  __device__ __forceinline__ static int wrap_z(int v, const Geometry& g) {
+    return cube ? (v & (E - 1)) : wrap_once(v, g.L3);
+  }
+};
+
 // Float4 offsets (within one quad) of the rows and row positions around a site: rowo[dz][dy] for offsets
 // -R..R (periodic wrap), xo[dx] = the element of x + dx within its component row.
 template <class Lat, int N, int P, int L1C>
@@ -152,15 +171,16 @@ struct QuadAround {
   int plane_a;   // elements of one sublattice
 
   __device__ __forceinline__ QuadAround(const Geometry& g, int hp, int h, int ph, int y, int z) {
-    const int L1 = L1C ? L1C : g.L1;
-    const int HP = L1C ? L1C / P : hp;
+    using D = QDim<L1C>;
+    const int L1 = D::L1(g);
+    const int HP = D::E ? D::E / P : hp;
     const int RS = N * L1;
-    plane_a = g.L3 * g.L2 * RS;
+    plane_a = D::L3(g) * D::L2(g) * RS;
 #pragma unroll
     for (int dz = -R; dz <= R; ++dz) {
-      const int zz = Lat::dim == 3 ? wrap_once(z + dz, g.L3) : z;
+      const int zz = Lat::dim == 3 ? D::wrap_z(z + dz, g) : z;
 #pragma unroll
-      for (int dy = -R; dy <= R; ++dy) rowo[dz + R][dy + R] = (zz * g.L2 + wrap_once(y + dy, g.L2)) * RS;
+      for (int dy = -R; dy <= R; ++dy) rowo[dz + R][dy + R] = (zz * D::L2(g) + D::wrap_y(y + dy, g)) * RS;
     }
 #pragma unroll
     for (int dx = -R; dx <= R; ++dx) {
@@ -192,12 +212,15 @@ template <class Lat, int A, int N, int P, int L1C, bool MEASURE>
 __device__ __forceinline__ void quad_site(const QuadParams& p, int q, int h, int ph, int y, int z, int32_t key,
                                           MeasureAcc<N>& m) {
   const Geometry& g = p.g;
-  const int L1 = L1C ? L1C : g.L1;
-  float4* base = p.spins + (size_t)q * N * g.nsite;
+  using D = QDim<L1C>;
+  const int L1 = D::L1(g);
+  const int plane = D::cube ? D::E * D::E * D::E : g.plane;        // sites of one sublattice
+  const int nsite = D::cube ? Lat::b * plane : g.nsite;
+  float4* base = p.spins + (size_t)q * N * nsite;
   const QuadAround<Lat, N, P, L1C> nb(g, p.hp, h, ph, y, z);
   const int own_e = A * nb.plane_a + nb.rowo[Lat::reach][Lat::reach] + nb.xo[Lat::reach];
   const int x = h * P + ph;
-  const int own = A * g.plane + (z * g.L2 + y) * g.L1 + x;    // the reference's site index (Philox counter)
+  const int own = A * plane + (z * D::L2(g) + y) * L1 + x;    // the reference's site index (Philox counter)
   float4 s4[N];
 #pragma unroll
   for (int k = 0; k < N; ++k) s4[k] = base[own_e + k * L1];
@@ -251,8 +274,8 @@ __device__ __forceinline__ void quad_site(const QuadParams& p, int q, int h, int
   const bool cubic = N == 3 && g.has_cubic;
   const float k1 = cubic ? p.k1[own] : 0.0f;
   const float4 b4 = reinterpret_cast<const float4*>(p.beta)[q];
-  const uint32_t c0 = counter_of(4 * q, g.nsite, own);
-  const uint32_t ns = (uint32_t)g.nsite;
+  const uint32_t c0 = counter_of(4 * q, nsite, own);
+  const uint32_t ns = (uint32_t)nsite;
   bool a0, a1, a2, a3;
   finish_values<N>(g.acceptance, cubic, f2(k1), p.k2, c0, c0 + ns, true, make_float2(b4.x, b4.y), key, sl, vl, tl,
                    a0, a1);
@@ -359,13 +382,15 @@ __device__ __forceinline__ double measure_block_sum(const MeasureAcc<N>& m) {
 
 // Grid (ceil(L3 L2 L1 / P / 256), quads of this launch). Thread -> (row, position in the row's class segment).
 template <class Lat, int N, int P, int L1C, bool MEASURE>
-__global__ void __launch_bounds__(256, MEASURE ? SCK_QUAD_MEASURE_MIN_BLOCKS : SCK_QUAD_MIN_BLOCKS) quad_class_kernel(const __grid_constant__ QuadParams p) {
+__global__ void __launch_bounds__(256, MEASURE ? SCK_QUAD_MEASURE_MIN_BLOCKS : SCK_QUAD_MIN_BLOCKS)
+    quad_class_kernel(const __grid_constant__ QuadParams p) {
   const Geometry& g = p.g;
+  using D = QDim<L1C>;
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   uint32_t row, h;
-  if constexpr (L1C > 0) {
-    row = t / (uint32_t)(L1C / P);
-    h = t - row * (uint32_t)(L1C / P);
+  if constexpr (D::E > 0) {
+    row = t / (uint32_t)(D::E / P);
+    h = t - row * (uint32_t)(D::E / P);
   } else {
     row = fdiv(t, p.fd_hp);
     h = t - row * (uint32_t)p.hp;
@@ -378,9 +403,9 @@ __global__ void __launch_bounds__(256, MEASURE ? SCK_QUAD_MEASURE_MIN_BLOCKS : S
 #pragma unroll
       for (int v = 0; v <= N; ++v) m.v[j][v] = 0.0;
   }
-  if (row < (uint32_t)(g.L3 * g.L2)) {
-    const int z = (int)fdiv(row, p.fd_L2);
-    const int y = (int)row - z * g.L2;
+  if (row < (uint32_t)(D::L3(g) * D::L2(g))) {
+    const int z = D::cube ? (int)(row / (uint32_t)D::E) : (int)fdiv(row, p.fd_L2);
+    const int y = (int)row - z * D::L2(g);
     const int ph = class_residue<P>(p, p.colour, p.alpha, y, z);
     if (ph >= 0) {
       const int32_t key = sweep_key_at(p.state, p.sweep_offset);
@@ -481,9 +506,9 @@ __global__ void __launch_bounds__(256, SCK_QUAD_MIN_BLOCKS) quad_pipe_kernel(con
     if (chunk >= pp.blocks_x) break;
     const uint32_t t = (uint32_t)chunk * 256u + threadIdx.x;
     uint32_t row, h;
-    if constexpr (L1C > 0) {
-      row = t / (uint32_t)(L1C / P);
-      h = t - row * (uint32_t)(L1C / P);
+    if constexpr (QDim<L1C>::E > 0) {
+      row = t / (uint32_t)(QDim<L1C>::E / P);
+      h = t - row * (uint32_t)(QDim<L1C>::E / P);
     } else {
       row = fdiv(t, p.fd_hp);
       h = t - row * (uint32_t)p.hp;
@@ -652,6 +677,9 @@ inline void launch_quad_t(const QuadParams& p, dim3 grid, cudaStream_t s) {
 
 template <class Lat, int N, int P>
 inline void launch_quad_l1(const QuadParams& p, dim3 grid, cudaStream_t s) {
+  if constexpr (Lat::dim == 3) {
+    if (p.g.L1 == 64 && p.g.L2 == 64 && p.g.L3 == 64) return launch_quad_t<Lat, N, P, -64>(p, grid, s);
+  }
   if (p.g.L1 == 64) return launch_quad_t<Lat, N, P, 64>(p, grid, s);
   if (p.g.L1 == 32) return launch_quad_t<Lat, N, P, 32>(p, grid, s);
   if (p.g.L1 == 128) return launch_quad_t<Lat, N, P, 128>(p, grid, s);
