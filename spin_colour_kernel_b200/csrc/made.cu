@@ -643,8 +643,8 @@ __global__ void gather_kernel(const int8_t* __restrict__ spins, int R, int L, __
 // ======================================================================================= the colour step
 constexpr int XS = IN + 8;     // shared row strides (bfloat16): conflict-free ldmatrix rows
 constexpr int HS = H + 8;
-constexpr int WARP_SMEM = 16 * XS * 2 + 3 * 16 * HS * 2;
-constexpr int STEP_WARPS = 5;
+constexpr int WARP_SMEM = 16 * XS * 2 + 3 * 16 * HS * 2;   // one 16-row tile: inputs and three layers
+constexpr int STEP_WARPS = 5;                                 // 16-row tiles per block of threads
 
 // The weights one autoregressive step reads, staged per block of threads: rows [u0, u0 + 8 NT) of W1 (all 160
 // columns) and of W2, W3 (the 16 nkt columns of degree <= g), rows [S g, S g + 8) of W4.
@@ -657,6 +657,19 @@ struct Slice {
 
 template <int G>
 constexpr int step_smem() { return STEP_WARPS * WARP_SMEM + 2 * Slice<G>::BYTES; }
+
+// Warps per 16-row tile: with two n8 tiles of new units per layer and step (G = 16), a pair of warps shares the
+// tile, each computing one n8 tile of every layer, so that a step's chain of dependent MMAs is half as long and
+// the SM holds twice the warps; the logits, the draws and the acceptance stay with the first warp of the pair.
+template <int G>
+constexpr int tile_warps() { return Slice<G>::NT >= 2 ? 2 : 1; }
+template <int G>
+constexpr int step_threads() { return 32 * STEP_WARPS * tile_warps<G>(); }
+
+// the two warps of a tile meet at named barrier 1 + tile (barrier 0 is __syncthreads)
+__device__ __forceinline__ void tile_sync(int tile, int warps) {
+  if (warps > 1) asm volatile("bar.sync %0, %1;\n" ::"r"(1 + tile), "r"(32 * warps) : "memory");
+}
 
 struct StepParams {
   const __nv_bfloat16* W[4];
@@ -753,22 +766,24 @@ __device__ __forceinline__ void stage(float (&acc)[NT][4], const __nv_bfloat16* 
 __device__ __forceinline__ int wrap_block(int v, int L) { return v < 0 ? v + L : (v >= L ? v - L : v); }
 
 template <int G>
-__global__ void __launch_bounds__(32 * STEP_WARPS) step_kernel(StepParams p) {
+__global__ void __launch_bounds__(step_threads<G>()) step_kernel(StepParams p) {
   using SL = Slice<G>;
-  constexpr int U = SL::U, S = SL::S, NT = SL::NT;
+  constexpr int U = SL::U, S = SL::S, TW = tile_warps<G>(), NT = SL::NT / TW;
   extern __shared__ __align__(16) unsigned char smem[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, gr = lane >> 2, q = lane & 3;
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31, gr = lane >> 2, q = lane & 3;
+  const int warp = wid / TW, sub = wid - warp * TW;   // the tile, and this warp's n8 tile within a layer step
   __nv_bfloat16* X = (__nv_bfloat16*)(smem + warp * WARP_SMEM);
   __nv_bfloat16* const H0 = X + 16 * XS;       // layer l's activations at H0 + l * 16 * HS
   __nv_bfloat16* const slices = (__nv_bfloat16*)(smem + STEP_WARPS * WARP_SMEM);   // two buffers of ELEMS
-  for (int i = lane; i < WARP_SMEM / 16; i += 32) ((uint4*)X)[i] = make_uint4(0, 0, 0, 0);
-  __syncwarp();
+  for (int i = lane + 32 * sub; i < WARP_SMEM / 16; i += 32 * TW) ((uint4*)X)[i] = make_uint4(0, 0, 0, 0);
+  tile_sync(warp, TW);
 
   const long long tasks = (long long)p.R * p.nc;
   const long long ctasks = (tasks + 8 * STEP_WARPS - 1) / (8 * STEP_WARPS);   // 8 blocks per warp
   const int half = p.nb >> 1, L = p.L;
   if ((long long)blockIdx.x < ctasks) load_slice<G>(slices, p, 0);
   for (long long ct = blockIdx.x; ct < ctasks; ct += gridDim.x) {
+    tile_sync(warp, TW);   // the tile's first warp is done with the previous blocks' rows
     // ---- block r = gr of this warp (lanes 4r..4r+3): rows r (proposal) and r + 8 (current spins)
     const long long task = (ct * STEP_WARPS + warp) * 8 + gr;
     const bool valid = task < tasks;
@@ -779,7 +794,7 @@ __global__ void __launch_bounds__(32 * STEP_WARPS) step_kernel(StepParams p) {
     const int x0 = 4 * bx, y0 = 4 * by, z0 = 4 * bz;
     const long long uid = (long long)rep * p.nb * p.nb * p.nb + (bx + p.nb * (by + p.nb * bz));
     const int8_t* base = p.spins + (long long)rep * L * L * L;
-    for (int col = q; col < IN; col += 4) {
+    for (int col = q + 4 * sub; col < IN; col += 4 * TW) {
       float s = 0.f;
       if (valid) {
         const int x = wrap_block(x0 + c_tab.in_off[col][0], L), y = wrap_block(y0 + c_tab.in_off[col][1], L),
@@ -791,6 +806,7 @@ __global__ void __launch_bounds__(32 * STEP_WARPS) step_kernel(StepParams p) {
       X[gr * XS + col] = col < NBD ? v : __float2bfloat16_rn(0.f);
     }
     __syncwarp();
+    tile_sync(warp, TW);
 
     float lq_new = 0.f, lq_old = 0.f;
     Philox4 rnd{0, 0, 0, 0};
@@ -807,10 +823,11 @@ __global__ void __launch_bounds__(32 * STEP_WARPS) step_kernel(StepParams p) {
       // layer 1: inputs of degree <= g are the boundary and the spins of groups < g
       {
         float acc[NT][4];
-        stage<NT>(acc, X, XS, sl + SL::W1, XS, p.bias[0], H, g * U, (NBD + S * g + 15) / 16, lane);
+        stage<NT>(acc, X, XS, sl + SL::W1 + sub * 8 * XS, XS, p.bias[0], H, g * U + sub * 8,
+                  (NBD + S * g + 15) / 16, lane);
 #pragma unroll
         for (int t = 0; t < NT; ++t) {
-          const int c = g * U + t * 8 + 2 * q;
+          const int c = g * U + sub * 8 + t * 8 + 2 * q;
           if (2 * q < U) {
             *(uint32_t*)(H0 + gr * HS + c) = pack_bf16(fmaxf(acc[t][0], 0.f), fmaxf(acc[t][1], 0.f));
             *(uint32_t*)(H0 + (gr + 8) * HS + c) = pack_bf16(fmaxf(acc[t][2], 0.f), fmaxf(acc[t][3], 0.f));
@@ -818,14 +835,15 @@ __global__ void __launch_bounds__(32 * STEP_WARPS) step_kernel(StepParams p) {
         }
       }
       __syncwarp();
+      tile_sync(warp, TW);
 #pragma unroll
       for (int l = 1; l < 3; ++l) {
         float acc[NT][4];
-        stage<NT>(acc, H0 + (l - 1) * 16 * HS, HS, sl + (l == 1 ? SL::W2 : SL::W3), HS, p.bias[l], H, g * U, nkt,
-                  lane);
+        stage<NT>(acc, H0 + (l - 1) * 16 * HS, HS, sl + (l == 1 ? SL::W2 : SL::W3) + sub * 8 * HS, HS, p.bias[l], H,
+                  g * U + sub * 8, nkt, lane);
 #pragma unroll
         for (int t = 0; t < NT; ++t) {
-          const int c = g * U + t * 8 + 2 * q;
+          const int c = g * U + sub * 8 + t * 8 + 2 * q;
           if (2 * q < U) {
             *(uint32_t*)(H0 + l * 16 * HS + gr * HS + c) = pack_bf16(fmaxf(acc[t][0], 0.f), fmaxf(acc[t][1], 0.f));
             *(uint32_t*)(H0 + l * 16 * HS + (gr + 8) * HS + c) =
@@ -833,7 +851,9 @@ __global__ void __launch_bounds__(32 * STEP_WARPS) step_kernel(StepParams p) {
           }
         }
         __syncwarp();
+        tile_sync(warp, TW);
       }
+      if (sub != 0) continue;   // the logits and draws of the tile: its first warp
       // logits of group g (positions S g .. S g + S - 1 in the first columns of one n8 tile)
       float lo[1][4];
       stage<1>(lo, H0 + 2 * 16 * HS, HS, sl + SL::W4, HS, p.bias[3], NSP, g * S, nkt, lane);
@@ -860,6 +880,7 @@ __global__ void __launch_bounds__(32 * STEP_WARPS) step_kernel(StepParams p) {
       }
       __syncwarp();
     }
+    if (sub != 0) continue;   // energy change, acceptance and write-back: the tile's first warp
     lq_new += __shfl_xor_sync(0xffffffffu, lq_new, 1);
     lq_new += __shfl_xor_sync(0xffffffffu, lq_new, 2);
     lq_old += __shfl_xor_sync(0xffffffffu, lq_old, 1);
@@ -1237,12 +1258,12 @@ int sck_made_colour_step(const void* params, int32_t groups, int8_t* spins, int3
     rc = cuda_status(cudaFuncSetAttribute(step_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           step_smem<16>()), "made step smem");
     if (rc) return rc;
-    step_kernel<16><<<(unsigned)grid, 32 * STEP_WARPS, step_smem<16>(), s>>>(p);
+    step_kernel<16><<<(unsigned)grid, step_threads<16>(), step_smem<16>(), s>>>(p);
   } else {
     rc = cuda_status(cudaFuncSetAttribute(step_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           step_smem<64>()), "made step smem");
     if (rc) return rc;
-    step_kernel<64><<<(unsigned)grid, 32 * STEP_WARPS, step_smem<64>(), s>>>(p);
+    step_kernel<64><<<(unsigned)grid, step_threads<64>(), step_smem<64>(), s>>>(p);
   }
   return cuda_status(cudaGetLastError(), "made colour step");
 }
