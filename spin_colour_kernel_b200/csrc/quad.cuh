@@ -235,10 +235,10 @@ __device__ __forceinline__ void quad_site(const QuadParams& p, int q, int h, int
     for (int k = 0; k < N; ++k) gl[k] = gh[k] = f2(0.0f);
     static_for<Rg::begin, Rg::end>([&](auto ic) {
       constexpr BondC bd = Lat::bond(A, decltype(ic)::value);
-      const float4* pq = base + nb.elem(bd);
+      const float4* pq = base + nb.elem(bd);   // never written during a class launch: the read-only path
 #pragma unroll
       for (int k = 0; k < N; ++k) {
-        const float4 t = pq[k * L1];
+        const float4 t = __ldg(pq + k * L1);
         gl[k] = __fadd2_rn(gl[k], lo2(t));
         gh[k] = __fadd2_rn(gh[k], hi2(t));
       }
@@ -388,7 +388,12 @@ __global__ void __launch_bounds__(256, MEASURE ? SCK_QUAD_MEASURE_MIN_BLOCKS : S
   using D = QDim<L1C>;
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   uint32_t row, h;
-  if constexpr (D::E > 0) {
+  if constexpr (D::cube && D::E / P == 32) {
+    // a cubic box with 32 class sites per row: a block takes 2 rows of 4 planes (neighbour rows shared in L1)
+    const uint32_t tile = blockIdx.x, lz = threadIdx.x >> 6, ly = (threadIdx.x >> 5) & 1;
+    h = threadIdx.x & 31;
+    row = ((tile / (D::E / 2)) * 4 + lz) * D::E + (tile % (D::E / 2)) * 2 + ly;
+  } else if constexpr (D::E > 0) {
     row = t / (uint32_t)(D::E / P);
     h = t - row * (uint32_t)(D::E / P);
   } else {
