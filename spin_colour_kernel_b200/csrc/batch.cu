@@ -88,6 +88,7 @@ struct sck_batch {
   int resident_blocks;
   long long step_items;           // streaming items per sweep
   int grid;                       // persistent blocks of a launch (resident capacity of the device)
+  int device;                     // the device bind sized the grid for
   unsigned wait_limit;
   int* giveup_host;               // host-mapped flag a block raises when a wait gives up
   int* giveup_dev;
@@ -267,6 +268,7 @@ static int batch_prepare(sck_batch* b) {
   if (e != cudaSuccess) return cuda_status(e, "batch shared memory");
   int dev = 0, sms = 0, per_sm = 0;
   e = cudaGetDevice(&dev);
+  b->device = dev;
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (e == cudaSuccess)
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_persistent_kernel<N, ST>, 256, b->resident_smem);
@@ -387,6 +389,7 @@ int sck_batch_create(const sck_plan* const* plans, int32_t n_plans, int64_t resi
   b->resident_blocks = 0;
   b->step_items = 0;
   b->grid = 0;
+  b->device = -1;
   b->wait_limit = 1u << 20;
   b->giveup_host = nullptr;
   b->giveup_dev = nullptr;
@@ -512,6 +515,10 @@ int sck_batch_sweep(sck_batch* b, void* workspace, int32_t n_sweeps, void* strea
   if (n_sweeps == 0) return SCK_OK;
   if (b->giveup_host != nullptr && *(volatile int*)b->giveup_host)
     return batch_fail(SCK_ERR_TIMEOUT, "an earlier bounded wait of this batch gave up (read sck_batch_wait_status)");
+  int dev = -1;
+  const int rc = cuda_status(cudaGetDevice(&dev), "batch sweep");
+  if (rc != SCK_OK) return rc;
+  if (dev != b->device) return batch_fail(SCK_ERR_INVALID, "the batch was bound on another device: bind it here");
   return batch_sweep_dispatch(b, (unsigned char*)workspace, n_sweeps, (cudaStream_t)stream);
 }
 
