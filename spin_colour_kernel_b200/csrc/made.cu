@@ -943,6 +943,310 @@ __global__ void __launch_bounds__(step_threads<G>()) step_kernel(StepParams p) {
   cp_async_wait<0>();
 }
 
+// ================================================================= the colour step, 16 proposals per tile (G = 16)
+// The kernel above carries the current spins of a tile's 8 blocks through the autoregressive chain in rows
+// 8..15 of its MMA tiles. This one fills all 16 rows with proposals (16 blocks per tile, two blocks per lane
+// group) and evaluates the current spins' density afterwards in one dense pass: the network's masks make every
+// logit of x a function of x alone, so the 16 x 4 layer steps need no chaining there — layer by layer, 32 units at
+// a time, the weights streamed through the same double buffer. Every unit is computed with the same k-tiles and
+// summation order as in the chain (the extra k-tiles of a chunk meet masked zero weights and add exact zeros), and
+// log q(x) sums its 64 terms in the chain's order, so that the density of a configuration is the same number
+// whether it is drawn or current: the Metropolis-Hastings ratio stays exact to the last bit.
+constexpr int PAIR_TILE_SMEM = WARP_SMEM + 2 * 16 * NSP;   // + the current and the proposed spins
+constexpr int DENSE_CHUNKS = 26;      // 8 per hidden layer (32 units each), 2 for the output layer
+// the dense pass splits the two slice buffers into three chunk buffers, so that two chunks load while one is used
+constexpr int DENSE_BUF_ELEMS = 2 * 13248 / 3;
+static_assert(3 * DENSE_BUF_ELEMS == 2 * Slice<16>::ELEMS, "three chunk buffers fill the two slice buffers");
+static_assert(32 * HS <= DENSE_BUF_ELEMS && 32 * XS <= DENSE_BUF_ELEMS, "a chunk fits its buffer");
+
+constexpr int pair_smem() { return STEP_WARPS * PAIR_TILE_SMEM + 2 * Slice<16>::BYTES; }
+
+struct DenseChunk {
+  int layer, u0, nkt, ld;
+};
+
+// chunk i: rows [u0, u0 + 32) of W_{layer + 1} with the k-tiles of degree <= the chunk's highest unit degree
+__device__ __forceinline__ DenseChunk dense_chunk(int i) {
+  DenseChunk d;
+  if (i < 24) {
+    const int c = i & 7;
+    d.layer = i >> 3;
+    d.u0 = 32 * c;
+    d.nkt = d.layer == 0 ? (NBD + 4 * (2 * c + 1) + 15) / 16 : 2 * c + 2;
+    d.ld = d.layer == 0 ? XS : HS;
+  } else {
+    const int c = i - 24;
+    d.layer = 3;
+    d.u0 = 32 * c;
+    d.nkt = 8 * c + 8;
+    d.ld = HS;
+  }
+  return d;
+}
+
+// all threads of the block: copy dense chunk i into `dst` (cp.async, one commit group)
+__device__ __forceinline__ void load_dense_chunk(__nv_bfloat16* dst, const StepParams& p, int i) {
+  const DenseChunk d = dense_chunk(i);
+  const int K = d.layer == 0 ? IN : H;
+  const int ch = 2 * d.nkt;                       // 16-byte pieces per row
+  const __nv_bfloat16* W = p.W[d.layer];
+  for (int j = threadIdx.x; j < 32 * ch; j += blockDim.x) {
+    const int r = j / ch, c = j - r * ch;
+    cp_async16(dst + r * d.ld + c * 8, W + (long long)(d.u0 + r) * K + c * 8, 16);
+  }
+  cp_async_commit();
+}
+
+// Grid of persistent blocks of 5 tiles x 2 warps; tile rows r = 0..15 are the proposals of blocks 16 t + r, lanes
+// (gr, q) of the tile's first warp own blocks gr and gr + 8 for the draws, densities, energy and write-back.
+__global__ void __launch_bounds__(32 * STEP_WARPS * 2) step_pair_kernel(StepParams p) {
+  using SL = Slice<16>;
+  constexpr int U = SL::U, S = SL::S;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31, gr = lane >> 2, q = lane & 3;
+  const int warp = wid >> 1, sub = wid & 1;
+  unsigned char* tbase = smem + warp * PAIR_TILE_SMEM;
+  __nv_bfloat16* X = (__nv_bfloat16*)tbase;
+  __nv_bfloat16* const H0 = X + 16 * XS;
+  int8_t* const CUR = (int8_t*)(tbase + WARP_SMEM);           // [16][64] current spins of the tile's blocks
+  int8_t* const PROP = CUR + 16 * NSP;                        // [16][64] proposed spins
+  float* const LS = (float*)H0;   // [16][64] log-sigmoid terms of x, over layer 1's activations once they are spent
+  __nv_bfloat16* const slices = (__nv_bfloat16*)(smem + STEP_WARPS * PAIR_TILE_SMEM);
+  for (int i = lane + 32 * sub; i < WARP_SMEM / 16; i += 64) ((uint4*)X)[i] = make_uint4(0, 0, 0, 0);
+  tile_sync(warp, 2);
+
+  const long long tasks = (long long)p.R * p.nc;
+  const long long ctasks = (tasks + 16 * STEP_WARPS - 1) / (16 * STEP_WARPS);   // 16 blocks per tile
+  const int half = p.nb >> 1, L = p.L;
+  if ((long long)blockIdx.x < ctasks) load_slice<16>(slices, p, 0);
+  for (long long ct = blockIdx.x; ct < ctasks; ct += gridDim.x) {
+    tile_sync(warp, 2);   // the first warp is done with the previous blocks' rows
+    const bool more = ct + gridDim.x < ctasks;
+    // ---- gather: row r = block 16 (ct * tiles + tile) + r; both warps, rows split by lane group and warp
+    for (int rr = 0; rr < 2; ++rr) {
+      const int r = gr + 8 * rr;
+      const long long task = (ct * STEP_WARPS + warp) * 16 + r;
+      const bool valid = task < tasks;
+      const int rep = valid ? (int)(task / p.nc) : 0;
+      const int k = valid ? (int)(task % p.nc) : 0;
+      const int bx = 2 * (k % half) + (p.colour & 1), by = 2 * (k / half % half) + ((p.colour >> 1) & 1),
+                bz = 2 * (k / (half * half)) + (p.colour >> 2);
+      const int8_t* base = p.spins + (long long)rep * L * L * L;
+      for (int col = q + 4 * sub; col < IN; col += 8) {
+        float s = 0.f;
+        if (valid) {
+          const int x = wrap_block(4 * bx + c_tab.in_off[col][0], L), y = wrap_block(4 * by + c_tab.in_off[col][1], L),
+                    z = wrap_block(4 * bz + c_tab.in_off[col][2], L);
+          s = (float)base[((long long)z * L + y) * L + x];
+        }
+        X[r * XS + col] = col < NBD ? __float2bfloat16_rn(s) : __float2bfloat16_rn(0.f);
+        if (col >= NBD) CUR[r * NSP + col - NBD] = (int8_t)(int)s;
+      }
+    }
+    __syncwarp();
+    tile_sync(warp, 2);
+
+    // ---- the first warp's two blocks
+    long long task2[2];
+    bool valid2[2];
+    int rep2[2], b3[2][3];
+    long long uid2[2];
+#pragma unroll
+    for (int rr = 0; rr < 2; ++rr) {
+      task2[rr] = (ct * STEP_WARPS + warp) * 16 + gr + 8 * rr;
+      valid2[rr] = task2[rr] < tasks;
+      rep2[rr] = valid2[rr] ? (int)(task2[rr] / p.nc) : 0;
+      const int k = valid2[rr] ? (int)(task2[rr] % p.nc) : 0;
+      b3[rr][0] = 2 * (k % half) + (p.colour & 1);
+      b3[rr][1] = 2 * (k / half % half) + ((p.colour >> 1) & 1);
+      b3[rr][2] = 2 * (k / (half * half)) + (p.colour >> 2);
+      uid2[rr] = (long long)rep2[rr] * p.nb * p.nb * p.nb + (b3[rr][0] + p.nb * (b3[rr][1] + p.nb * b3[rr][2]));
+    }
+    float lq_new[2] = {0.f, 0.f};
+    Philox4 rnd[2] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+    int rnd_w = -1;
+    // ---- the autoregressive chain: 16 steps of 4 spins
+    for (int g = 0; g < 16; ++g) {
+      cp_async_wait<0>();
+      __syncthreads();   // slice g has landed; every warp is done with the other buffer
+      __nv_bfloat16* const next = slices + ((g + 1) & 1) * SL::ELEMS;
+      if (g + 1 < 16) load_slice<16>(next, p, g + 1);
+      else load_dense_chunk(slices, p, 0);   // chunk buffer 0 lies in slice buffer 0, unused by step 15
+      const __nv_bfloat16* sl = slices + (g & 1) * SL::ELEMS;
+      const int nkt = (U * (g + 1) + 15) / 16;
+      {
+        float acc[1][4];
+        stage<1>(acc, X, XS, sl + SL::W1 + sub * 8 * XS, XS, p.bias[0], H, g * U + sub * 8, (NBD + S * g + 15) / 16,
+                 lane);
+        const int c = g * U + sub * 8 + 2 * q;
+        *(uint32_t*)(H0 + gr * HS + c) = pack_bf16(fmaxf(acc[0][0], 0.f), fmaxf(acc[0][1], 0.f));
+        *(uint32_t*)(H0 + (gr + 8) * HS + c) = pack_bf16(fmaxf(acc[0][2], 0.f), fmaxf(acc[0][3], 0.f));
+      }
+      __syncwarp();
+      tile_sync(warp, 2);
+#pragma unroll
+      for (int l = 1; l < 3; ++l) {
+        float acc[1][4];
+        stage<1>(acc, H0 + (l - 1) * 16 * HS, HS, sl + (l == 1 ? SL::W2 : SL::W3) + sub * 8 * HS, HS, p.bias[l], H,
+                 g * U + sub * 8, nkt, lane);
+        const int c = g * U + sub * 8 + 2 * q;
+        *(uint32_t*)(H0 + l * 16 * HS + gr * HS + c) = pack_bf16(fmaxf(acc[0][0], 0.f), fmaxf(acc[0][1], 0.f));
+        *(uint32_t*)(H0 + l * 16 * HS + (gr + 8) * HS + c) = pack_bf16(fmaxf(acc[0][2], 0.f), fmaxf(acc[0][3], 0.f));
+        __syncwarp();
+        tile_sync(warp, 2);
+      }
+      if (sub == 0) {
+        float lo[1][4];
+        stage<1>(lo, H0 + 2 * 16 * HS, HS, sl + SL::W4, HS, p.bias[3], NSP, g * S, nkt, lane);
+        if (g != rnd_w) {
+#pragma unroll
+          for (int rr = 0; rr < 2; ++rr) rnd[rr] = philox4x32_10((uint32_t)(int32_t)(17 * uid2[rr] + g), 0u, p.k0, p.k1);
+          rnd_w = g;
+        }
+#pragma unroll
+        for (int rr = 0; rr < 2; ++rr) {
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const int j = 2 * q + e;
+            if (j < S) {
+              const int pos = g * S + j;
+              const int o = pos & 3;
+              const uint32_t bits = o == 0 ? rnd[rr].x0 : (o == 1 ? rnd[rr].x1 : (o == 2 ? rnd[rr].x2 : rnd[rr].x3));
+              const float u = to_uniform(bits);
+              const float ln = lo[0][2 * rr + e];
+              const float xn = u < 1.f / (1.f + __expf(-ln)) ? 1.f : -1.f;
+              lq_new[rr] += log_sigmoid(xn * ln);
+              X[(gr + 8 * rr) * XS + NBD + pos] = __float2bfloat16_rn(xn);
+            }
+          }
+        }
+      }
+      __syncwarp();
+    }
+    tile_sync(warp, 2);   // the last draws are in X
+    // ---- keep the proposals, put the current spins in their place
+    for (int i = lane + 32 * sub; i < 16 * NSP; i += 64) {
+      const int r = i / NSP, j = i - r * NSP;
+      PROP[i] = (int8_t)(int)__bfloat162float(X[r * XS + NBD + j]);
+      X[r * XS + NBD + j] = __float2bfloat16_rn((float)CUR[i]);
+    }
+    // ---- the dense pass over the current spins: the terms of log q(x) of the 16 blocks
+    for (int i = 0; i < DENSE_CHUNKS; ++i) {
+      // chunk i has landed (chunk i + 1, issued a step earlier, may still be in flight); after the barrier every
+      // warp is done with chunk i - 1, whose buffer takes chunk i + 2, and with the previous layer's activations
+      if (i == 0 || i + 1 == DENSE_CHUNKS) cp_async_wait<0>();
+      else cp_async_wait<1>();
+      __syncthreads();
+      if (i == 0) load_dense_chunk(slices + DENSE_BUF_ELEMS, p, 1);
+      if (i + 2 < DENSE_CHUNKS) load_dense_chunk(slices + ((i + 2) % 3) * DENSE_BUF_ELEMS, p, i + 2);
+      const __nv_bfloat16* wc = slices + (i % 3) * DENSE_BUF_ELEMS;
+      const DenseChunk d = dense_chunk(i);
+      float acc[2][4];
+      const int u0 = d.u0 + 16 * sub;
+      if (d.layer == 0) {
+        stage<2>(acc, X, XS, wc + 16 * sub * XS, XS, p.bias[0], H, u0, d.nkt, lane);
+      } else {
+        stage<2>(acc, H0 + (d.layer - 1) * 16 * HS, HS, wc + 16 * sub * HS, HS, p.bias[d.layer],
+                 d.layer == 3 ? NSP : H, u0, d.nkt, lane);
+      }
+#pragma unroll
+      for (int tt = 0; tt < 2; ++tt) {
+        const int c = u0 + tt * 8 + 2 * q;
+        if (d.layer < 3) {
+          *(uint32_t*)(H0 + d.layer * 16 * HS + gr * HS + c) =
+              pack_bf16(fmaxf(acc[tt][0], 0.f), fmaxf(acc[tt][1], 0.f));
+          *(uint32_t*)(H0 + d.layer * 16 * HS + (gr + 8) * HS + c) =
+              pack_bf16(fmaxf(acc[tt][2], 0.f), fmaxf(acc[tt][3], 0.f));
+        } else {
+#pragma unroll
+          for (int rr = 0; rr < 2; ++rr)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+              const int o = (gr + 8 * rr) * NSP + c + e;
+              LS[o] = log_sigmoid((float)CUR[o] * acc[tt][2 * rr + e]);
+            }
+        }
+      }
+    }
+    __syncthreads();   // every warp is done with the chunk buffers and the terms of log q(x) are in place
+    if (more) load_slice<16>(slices, p, 0);
+    if (sub != 0) continue;   // densities, energy change, acceptance and write-back: the tile's first warp
+    // log q(x) in the chain's order: lane q < 2 adds positions 4 g + 2 q, 4 g + 2 q + 1 for g = 0 .. 15
+    float lq_old[2] = {0.f, 0.f};
+#pragma unroll
+    for (int rr = 0; rr < 2; ++rr) {
+      if (q < 2)
+        for (int g = 0; g < 16; ++g) {
+          lq_old[rr] += LS[(gr + 8 * rr) * NSP + 4 * g + 2 * q];
+          lq_old[rr] += LS[(gr + 8 * rr) * NSP + 4 * g + 2 * q + 1];
+        }
+      lq_old[rr] += __shfl_xor_sync(0xffffffffu, lq_old[rr], 1);
+      lq_old[rr] += __shfl_xor_sync(0xffffffffu, lq_old[rr], 2);
+    }
+#pragma unroll
+    for (int rr = 0; rr < 2; ++rr) {
+      const int r = gr + 8 * rr;
+      float lqn = lq_new[rr];
+      lqn += __shfl_xor_sync(0xffffffffu, lqn, 1);
+      lqn += __shfl_xor_sync(0xffffffffu, lqn, 2);
+      const float lqo = lq_old[rr];
+      // energy change, integer: -(sum_internal (x'x' - xx) + sum_face (x' - x) b)
+      const int8_t* xn_row = PROP + r * NSP;
+      const int8_t* xc_row = CUR + r * NSP;
+      int de = 0;
+      for (int i = q; i < 144; i += 4) {
+        const int a = c_tab.internal[i][0], b = c_tab.internal[i][1];
+        de -= (int)xn_row[a] * (int)xn_row[b] - (int)xc_row[a] * (int)xc_row[b];
+      }
+      for (int i = q; i < NBD; i += 4) {
+        const int a = c_tab.face[i];
+        const int bd = (int)__bfloat162float(X[r * XS + i]);
+        de -= ((int)xn_row[a] - (int)xc_row[a]) * bd;
+      }
+      de += __shfl_xor_sync(0xffffffffu, de, 1);
+      de += __shfl_xor_sync(0xffffffffu, de, 2);
+      const bool valid = valid2[rr];
+      const int rep = rep2[rr];
+      int acc_flag = 0;
+      if (q == 0 && valid) {
+        const Philox4 ra = philox4x32_10((uint32_t)(int32_t)(17 * uid2[rr] + 16), 0u, p.k0, p.k1);
+        const float ua = to_uniform(ra.x0);
+        const float logr = -p.beta[rep] * (float)de + lqo - lqn;
+        acc_flag = ua < __expf(fminf(logr, 0.f)) ? 1 : 0;
+        if (acc_flag && p.accepted) atomicAdd(p.accepted + rep, 1);
+      }
+      acc_flag = __shfl_sync(0xffffffffu, acc_flag, lane & ~3);
+      if (valid && acc_flag) {
+        // lane q writes the four x-rows of layer lz = q
+        int8_t* dst = p.spins + (long long)rep * L * L * L;
+        const int x0 = 4 * b3[rr][0], y0 = 4 * b3[rr][1], z0 = 4 * b3[rr][2];
+        for (int ly = 0; ly < 4; ++ly) {
+          uint32_t word = 0;
+#pragma unroll
+          for (int lx = 0; lx < 4; ++lx) {
+            const int pos = c_tab.pos_of_raster[lx + 4 * ly + 16 * q];
+            word |= (uint32_t)(uint8_t)xn_row[pos] << (8 * lx);
+          }
+          *(uint32_t*)(dst + ((long long)(z0 + q) * L + (y0 + ly)) * L + x0) = word;
+        }
+      }
+      if (valid && p.record) {
+        unsigned char* rec = p.record + 80 * task2[rr];
+        for (int pos = q; pos < NSP; pos += 4) rec[pos] = (unsigned char)xn_row[pos];
+        if (q == 0) {
+          float* f = (float*)(rec + NSP);
+          f[0] = lqn;
+          f[1] = lqo;
+          f[2] = (float)de;
+          f[3] = (float)acc_flag;
+        }
+      }
+    }
+    __syncwarp();
+  }
+  cp_async_wait<0>();
+}
+
 // ======================================================================================= workspace layout
 struct TrainLayout {
   long long h[3], logits, g4, gh[3], wpart[4], bpart[4], grads, total;
@@ -1255,10 +1559,13 @@ int sck_made_colour_step(const void* params, int32_t groups, int8_t* spins, int3
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const long long grid = ctasks < sms ? ctasks : sms;
   if (groups == 16) {
-    rc = cuda_status(cudaFuncSetAttribute(step_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          step_smem<16>()), "made step smem");
+    // 16 proposals per tile, the current spins' densities in a dense pass
+    const long long ctasks2 = ((long long)R * p.nc + 16 * STEP_WARPS - 1) / (16 * STEP_WARPS);
+    const long long grid2 = ctasks2 < sms ? ctasks2 : sms;
+    rc = cuda_status(cudaFuncSetAttribute(step_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, pair_smem()),
+                     "made step smem");
     if (rc) return rc;
-    step_kernel<16><<<(unsigned)grid, step_threads<16>(), step_smem<16>(), s>>>(p);
+    step_pair_kernel<<<(unsigned)grid2, 32 * STEP_WARPS * 2, pair_smem(), s>>>(p);
   } else {
     rc = cuda_status(cudaFuncSetAttribute(step_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           step_smem<64>()), "made step smem");
