@@ -952,7 +952,7 @@ __global__ void __launch_bounds__(step_threads<G>()) step_kernel(StepParams p) {
 // summation order as in the chain (the extra k-tiles of a chunk meet masked zero weights and add exact zeros), and
 // log q(x) sums its 64 terms in the chain's order, so that the density of a configuration is the same number
 // whether it is drawn or current: the Metropolis-Hastings ratio stays exact to the last bit.
-constexpr int PAIR_TILE_SMEM = WARP_SMEM + 2 * 16 * NSP;   // + the current and the proposed spins
+constexpr int PAIR_TILE_SMEM = WARP_SMEM + 2 * 16 * NSP + 16 * 4;   // + current and proposed spins, log q(x')
 constexpr int DENSE_CHUNKS = 26;      // 8 per hidden layer (32 units each), 2 for the output layer
 // the dense pass splits the two slice buffers into three chunk buffers, so that two chunks load while one is used
 constexpr int DENSE_BUF_ELEMS = 2 * 13248 / 3;
@@ -1011,6 +1011,7 @@ __global__ void __launch_bounds__(32 * STEP_WARPS * 2) step_pair_kernel(StepPara
   int8_t* const CUR = (int8_t*)(tbase + WARP_SMEM);           // [16][64] current spins of the tile's blocks
   int8_t* const PROP = CUR + 16 * NSP;                        // [16][64] proposed spins
   float* const LS = (float*)H0;   // [16][64] log-sigmoid terms of x, over layer 1's activations once they are spent
+  float* const LQN = (float*)(PROP + 16 * NSP);               // [16] log q(x') of the rows the second warp drew
   __nv_bfloat16* const slices = (__nv_bfloat16*)(smem + STEP_WARPS * PAIR_TILE_SMEM);
   for (int i = lane + 32 * sub; i < WARP_SMEM / 16; i += 64) ((uint4*)X)[i] = make_uint4(0, 0, 0, 0);
   tile_sync(warp, 2);
@@ -1062,11 +1063,13 @@ __global__ void __launch_bounds__(32 * STEP_WARPS * 2) step_pair_kernel(StepPara
       b3[rr][2] = 2 * (k / (half * half)) + (p.colour >> 2);
       uid2[rr] = (long long)rep2[rr] * p.nb * p.nb * p.nb + (b3[rr][0] + p.nb * (b3[rr][1] + p.nb * b3[rr][2]));
     }
-    float lq_new[2] = {0.f, 0.f};
-    Philox4 rnd[2] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
-    int rnd_w = -1;
+    // warp `sub` draws the spins of rows gr + 8 sub (block uid_mine)
+    const long long uid_mine = sub ? uid2[1] : uid2[0];
+    float lq_mine = 0.f;
     // ---- the autoregressive chain: 16 steps of 4 spins
     for (int g = 0; g < 16; ++g) {
+      // this step's uniforms first: their Philox rounds overlap the layers' MMA chains
+      const Philox4 rnd = philox4x32_10((uint32_t)(int32_t)(17 * uid_mine + g), 0u, p.k0, p.k1);
       cp_async_wait<0>();
       __syncthreads();   // slice g has landed; every warp is done with the other buffer
       __nv_bfloat16* const next = slices + ((g + 1) & 1) * SL::ELEMS;
@@ -1095,35 +1098,31 @@ __global__ void __launch_bounds__(32 * STEP_WARPS * 2) step_pair_kernel(StepPara
         __syncwarp();
         tile_sync(warp, 2);
       }
-      if (sub == 0) {
+      {
+        // logits of group g in both warps (the same MMAs), each warp drawing the spins of its own rows
         float lo[1][4];
         stage<1>(lo, H0 + 2 * 16 * HS, HS, sl + SL::W4, HS, p.bias[3], NSP, g * S, nkt, lane);
-        if (g != rnd_w) {
 #pragma unroll
-          for (int rr = 0; rr < 2; ++rr) rnd[rr] = philox4x32_10((uint32_t)(int32_t)(17 * uid2[rr] + g), 0u, p.k0, p.k1);
-          rnd_w = g;
-        }
-#pragma unroll
-        for (int rr = 0; rr < 2; ++rr) {
-#pragma unroll
-          for (int e = 0; e < 2; ++e) {
-            const int j = 2 * q + e;
-            if (j < S) {
-              const int pos = g * S + j;
-              const int o = pos & 3;
-              const uint32_t bits = o == 0 ? rnd[rr].x0 : (o == 1 ? rnd[rr].x1 : (o == 2 ? rnd[rr].x2 : rnd[rr].x3));
-              const float u = to_uniform(bits);
-              const float ln = lo[0][2 * rr + e];
-              const float xn = u < 1.f / (1.f + __expf(-ln)) ? 1.f : -1.f;
-              lq_new[rr] += log_sigmoid(xn * ln);
-              X[(gr + 8 * rr) * XS + NBD + pos] = __float2bfloat16_rn(xn);
-            }
+        for (int e = 0; e < 2; ++e) {
+          const int j = 2 * q + e;
+          if (j < S) {
+            const int pos = g * S + j;
+            const int o = pos & 3;
+            const uint32_t bits = o == 0 ? rnd.x0 : (o == 1 ? rnd.x1 : (o == 2 ? rnd.x2 : rnd.x3));
+            const float u = to_uniform(bits);
+            const float ln = sub ? lo[0][2 + e] : lo[0][e];
+            const float xn = u < 1.f / (1.f + __expf(-ln)) ? 1.f : -1.f;
+            lq_mine += log_sigmoid(xn * ln);
+            X[(gr + 8 * sub) * XS + NBD + pos] = __float2bfloat16_rn(xn);
           }
         }
       }
       __syncwarp();
     }
-    tile_sync(warp, 2);   // the last draws are in X
+    lq_mine += __shfl_xor_sync(0xffffffffu, lq_mine, 1);
+    lq_mine += __shfl_xor_sync(0xffffffffu, lq_mine, 2);
+    if (sub == 1 && q == 0) LQN[gr + 8] = lq_mine;
+    tile_sync(warp, 2);   // the last draws are in X, the second warp's densities in LQN
     // ---- keep the proposals, put the current spins in their place
     for (int i = lane + 32 * sub; i < 16 * NSP; i += 64) {
       const int r = i / NSP, j = i - r * NSP;
@@ -1186,9 +1185,7 @@ __global__ void __launch_bounds__(32 * STEP_WARPS * 2) step_pair_kernel(StepPara
 #pragma unroll
     for (int rr = 0; rr < 2; ++rr) {
       const int r = gr + 8 * rr;
-      float lqn = lq_new[rr];
-      lqn += __shfl_xor_sync(0xffffffffu, lqn, 1);
-      lqn += __shfl_xor_sync(0xffffffffu, lqn, 2);
+      const float lqn = rr ? LQN[r] : lq_mine;
       const float lqo = lq_old[rr];
       // energy change, integer: -(sum_internal (x'x' - xx) + sum_face (x' - x) b)
       const int8_t* xn_row = PROP + r * NSP;
