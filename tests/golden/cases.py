@@ -180,7 +180,7 @@ def batch_twin_tune(R, resident_limit):
     generic resident kernel when the batch keeps the system on-chip, the lattice kernels when the system is on the
     square, triangular or simple cubic table (the batch streams those with the lattice kernels' update), else
     the generic class kernels."""
-    if R.sys.nsite * R.sys.n * 4 <= resident_limit:
+    if R.sys.nsite * R.sys.n * (1 if R.mode == 0 else 4) <= resident_limit:   # mode 0: int8 storage
         return R.tune(0, 0, resident_limit)
     if R.sys.crystal.name in ("square", "triangular", "sc") and R.tune(1, 0, 0)["specialised"] > 0:
         return R.tune(1, 0, 0)

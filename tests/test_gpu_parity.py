@@ -412,6 +412,38 @@ def test_ragged_batch_equals_individual_samplers(resident_limit):
         assert int(A.state[1]) == 6
 
 
+@pytest.mark.parametrize("resident_limit", [0, 4 << 10])
+def test_ragged_ising_batch_is_bit_exact(resident_limit):
+    """An int8 Ising batch (square, triangular and simple cubic systems of several sizes, periodic and open,
+    Metropolis and Barker) equals each system swept on its own, spin for spin: the lattice kernels' integer-key
+    site update for the streamed systems, the generic one on-chip."""
+    from spin_colour_kernel_b200.sampler import Sampler, SamplerBatch
+    systems = [sy.ising("square", 24), sy.ising("triangular", 18), sy.ising("sc", 10), sy.ising("square", 40),
+               sy.System("Ising sc open", 1, cr.make("sc"), (8, 8, 8), (False, True, True), {1: 1.0}),
+               sy.System("Ising square Barker", 1, cr.make("square"), (30, 30), (True, True), {1: 1.0},
+                         acceptance="barker")]
+    samplers, spins, refs, ref_spins = [], [], [], []
+    for i, s in enumerate(systems):
+        B = 5 + i % 3
+        A = Sampler(s, B, device="cuda", seed=80 + i, packed=False)
+        R = Sampler(s, B, device="cuda", seed=80 + i, packed=False)
+        C.batch_twin_tune(R, resident_limit)
+        for X in (A, R):
+            X.set_temperature(torch.linspace(1.5, 4.5, B))
+        S = A.init_spins(seed=i)
+        samplers.append(A)
+        spins.append(S)
+        refs.append(R)
+        ref_spins.append(S.clone())
+    batch = SamplerBatch(samplers, spins, resident_limit=resident_limit)
+    batch.sweep(3)
+    for R, S in zip(refs, ref_spins):
+        R.sweep(S, 3)
+    batch.check_waits()
+    for S, S2 in zip(spins, ref_spins):
+        assert torch.equal(S, S2)
+
+
 def test_ragged_batch_wait_that_gives_up_reports_timeout():
     """The persistent batch kernel orders each system's classes by completion counters; with zero polls an item
     whose class predecessor has not finished gives up, the batch reports SCK_ERR_TIMEOUT (sweeps refused until
