@@ -737,12 +737,12 @@ __device__ __forceinline__ void stage_tile(float (&c)[NT][4], const __nv_bfloat1
 }
 
 // one layer's new units of a 16-row tile: acc = bias + A[16 x 16 nkt] B^T, B rows in shared memory (row-major
-// [unit][k]); even and odd k-tiles accumulate separately to halve the MMA chain
+// [unit][k])
 template <int NT>
 __device__ __forceinline__ void stage(float (&acc)[NT][4], const __nv_bfloat16* A, int lda, const __nv_bfloat16* B,
                                       int ldb, const float* __restrict__ bias, int nbias, int u0, int nkt, int lane) {
   const int q = lane & 3;
-  float acc2[NT][4];
+  float acc2[NT][4], acc3[NT][4], acc4[NT][4];
 #pragma unroll
   for (int t = 0; t < NT; ++t) {
     const int n = u0 + t * 8 + 2 * q;   // columns past the layer (last tiles of small U) are computed and dropped
@@ -750,17 +750,20 @@ __device__ __forceinline__ void stage(float (&acc)[NT][4], const __nv_bfloat16* 
     acc[t][0] = acc[t][2] = b0;
     acc[t][1] = acc[t][3] = b1;
 #pragma unroll
-    for (int e = 0; e < 4; ++e) acc2[t][e] = 0.f;
+    for (int e = 0; e < 4; ++e) acc2[t][e] = acc3[t][e] = acc4[t][e] = 0.f;
   }
   const __nv_bfloat16* arow = A + ((lane & 7) + ((lane >> 3) & 1) * 8) * lda + (lane >> 4) * 8;
-  for (int kt = 0; kt < nkt; kt += 2) {
+  // k-tiles kt = 0, 1, 2, 3 (mod 4) accumulate in four independent chains: a quarter of the MMA dependency depth
+  for (int kt = 0; kt < nkt; kt += 4) {
     stage_tile<NT>(acc, arow, B, ldb, kt, lane);
     if (kt + 1 < nkt) stage_tile<NT>(acc2, arow, B, ldb, kt + 1, lane);
+    if (kt + 2 < nkt) stage_tile<NT>(acc3, arow, B, ldb, kt + 2, lane);
+    if (kt + 3 < nkt) stage_tile<NT>(acc4, arow, B, ldb, kt + 3, lane);
   }
 #pragma unroll
   for (int t = 0; t < NT; ++t)
 #pragma unroll
-    for (int e = 0; e < 4; ++e) acc[t][e] += acc2[t][e];
+    for (int e = 0; e < 4; ++e) acc[t][e] = (acc[t][e] + acc2[t][e]) + (acc3[t][e] + acc4[t][e]);
 }
 
 __device__ __forceinline__ int wrap_block(int v, int L) { return v < 0 ? v + L : (v >= L ? v - L : v); }
