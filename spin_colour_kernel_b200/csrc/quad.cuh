@@ -381,8 +381,10 @@ __device__ __forceinline__ double measure_block_sum(const MeasureAcc<N>& m) {
 #endif
 
 // Grid (ceil(L3 L2 L1 / P / 256), quads of this launch). Thread -> (row, position in the row's class segment).
+// The cubic instantiations run four blocks per SM (64 registers): 78 against 77 attempts/ns at three on the 3D
+// Heisenberg bcc J1-J2 workload.
 template <class Lat, int N, int P, int L1C, bool MEASURE>
-__global__ void __launch_bounds__(256, MEASURE ? SCK_QUAD_MEASURE_MIN_BLOCKS : SCK_QUAD_MIN_BLOCKS)
+__global__ void __launch_bounds__(256, MEASURE ? SCK_QUAD_MEASURE_MIN_BLOCKS : (L1C < 0 ? 4 : SCK_QUAD_MIN_BLOCKS))
     quad_class_kernel(const __grid_constant__ QuadParams p) {
   const Geometry& g = p.g;
   using D = QDim<L1C>;
