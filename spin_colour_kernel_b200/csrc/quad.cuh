@@ -208,7 +208,10 @@ __device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); 
 // MEASURE: also the site's share of the energy of the configuration the sweep leaves, -s'.v_low - h.s' +
 // anisotropy(s') with v_low the coupling-group fields of the neighbours updated earlier in the sweep (each bond
 // is counted once, at its later endpoint, when both its spins are final), and its components s', added in FP64.
-template <class Lat, int A, int N, int P, int L1C, bool MEASURE>
+// NC: neighbour loads through the non-coherent read-only path, for kernels in which no neighbour is written (a
+// class launch); the pipeline kernel, whose later tasks read what earlier tasks of the same launch wrote, keeps
+// coherent loads.
+template <class Lat, int A, int N, int P, int L1C, bool MEASURE, bool NC = false>
 __device__ __forceinline__ void quad_site(const QuadParams& p, int q, int h, int ph, int y, int z, int32_t key,
                                           MeasureAcc<N>& m) {
   const Geometry& g = p.g;
@@ -235,10 +238,10 @@ __device__ __forceinline__ void quad_site(const QuadParams& p, int q, int h, int
     for (int k = 0; k < N; ++k) gl[k] = gh[k] = f2(0.0f);
     static_for<Rg::begin, Rg::end>([&](auto ic) {
       constexpr BondC bd = Lat::bond(A, decltype(ic)::value);
-      const float4* pq = base + nb.elem(bd);   // never written during a class launch: the read-only path
+      const float4* pq = base + nb.elem(bd);
 #pragma unroll
       for (int k = 0; k < N; ++k) {
-        const float4 t = __ldg(pq + k * L1);
+        const float4 t = NC ? __ldg(pq + k * L1) : pq[k * L1];
         gl[k] = __fadd2_rn(gl[k], lo2(t));
         gh[k] = __fadd2_rn(gh[k], hi2(t));
       }
@@ -418,7 +421,7 @@ __global__ void __launch_bounds__(256, MEASURE ? SCK_QUAD_MEASURE_MIN_BLOCKS : (
       const int32_t key = sweep_key_at(p.state, p.sweep_offset);
       static_for<0, Lat::b>([&](auto ac) {
         constexpr int a = decltype(ac)::value;
-        if (a == p.alpha) quad_site<Lat, a, N, P, L1C, MEASURE>(p, q, (int)h, ph, y, z, key, m);
+        if (a == p.alpha) quad_site<Lat, a, N, P, L1C, MEASURE, true>(p, q, (int)h, ph, y, z, key, m);
       });
     }
   }
