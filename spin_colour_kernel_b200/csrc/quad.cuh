@@ -102,10 +102,12 @@ void quad_obs(const sck_plan* plan, const QuadObsParams& p, dim3 grid, cudaStrea
 #ifdef SCK_QUAD_KERNELS
 namespace sck {
 
-// FP64 sums one thread adds to a measure sweep: per lane j, the site's energy share and its N components.
-template <int N>
+// Sums one thread adds to a measure sweep: per lane j, the site's energy share and its N components. The
+// pipeline kernel adds several sites per thread in FP64 (T = double); a class launch has one site per thread and
+// keeps its float32 values as they are (0 + x is exact) until the block sum converts them to FP64.
+template <int N, class T = double>
 struct MeasureAcc {
-  double v[4][1 + N];
+  T v[4][1 + N];
 };
 
 // Residue (0 .. P-1) along x of the class's sites in row (y, z) of the launch's sublattice, or -1 when the row
@@ -205,15 +207,16 @@ __device__ __forceinline__ float2 lo2(float4 v) { return make_float2(v.x, v.y); 
 __device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); }
 
 // One class site (row segment position h, residue ph, row (y, z), sublattice A) of the four replicas of quad q.
-// MEASURE: also the site's share of the energy of the configuration the sweep leaves, -s'.v_low - h.s' +
+// MEASURE: also the site's share of the energy of the configuration the sweep leaves, -s'.(v_low + h) +
 // anisotropy(s') with v_low the coupling-group fields of the neighbours updated earlier in the sweep (each bond
 // is counted once, at its later endpoint, when both its spins are final), and its components s', added in FP64.
 // NC: neighbour loads through the non-coherent read-only path, for kernels in which no neighbour is written (a
 // class launch); the pipeline kernel, whose later tasks read what earlier tasks of the same launch wrote, keeps
-// coherent loads.
-template <class Lat, int A, int N, int P, int L1C, bool MEASURE, bool NC = false>
+// coherent loads. LOW: the class's lower coupling groups as a compile-time mask (-1: p.lower_groups at run time);
+// when every group is lower the measure field is the Metropolis field itself and needs no registers of its own.
+template <class Lat, int A, int N, int P, int L1C, bool MEASURE, bool NC = false, int LOW = -1, class Acc>
 __device__ __forceinline__ void quad_site(const QuadParams& p, int q, int h, int ph, int y, int z, int32_t key,
-                                          MeasureAcc<N>& m) {
+                                          Acc& m) {
   const Geometry& g = p.g;
   using D = QDim<L1C>;
   const int L1 = D::L1(g);
@@ -227,6 +230,7 @@ __device__ __forceinline__ void quad_site(const QuadParams& p, int q, int h, int
   float4 s4[N];
 #pragma unroll
   for (int k = 0; k < N; ++k) s4[k] = base[own_e + k * L1];
+  constexpr bool kFullLow = LOW == (1 << Lat::groups) - 1;
   float2 vl[N], vh[N], wl[N], wh[N];
 #pragma unroll
   for (int k = 0; k < N; ++k) vl[k] = vh[k] = wl[k] = wh[k] = f2(0.0f);
@@ -252,8 +256,8 @@ __device__ __forceinline__ void quad_site(const QuadParams& p, int q, int h, int
       vl[k] = __fadd2_rn(vl[k], __fmul2_rn(J, gl[k]));
       vh[k] = __fadd2_rn(vh[k], __fmul2_rn(J, gh[k]));
     }
-    if constexpr (MEASURE) {
-      if ((p.lower_groups >> gi) & 1u) {
+    if constexpr (MEASURE && !kFullLow) {
+      if (LOW >= 0 ? ((LOW >> gi) & 1) != 0 : ((p.lower_groups >> gi) & 1u) != 0) {
 #pragma unroll
         for (int k = 0; k < N; ++k) {
           wl[k] = __fadd2_rn(wl[k], __fmul2_rn(J, gl[k]));
@@ -267,6 +271,10 @@ __device__ __forceinline__ void quad_site(const QuadParams& p, int q, int h, int
     if (p.hnz[k]) {
       vl[k] = __fadd2_rn(vl[k], f2(p.h[k]));
       vh[k] = __fadd2_rn(vh[k], f2(p.h[k]));
+      if constexpr (MEASURE && !kFullLow) {
+        wl[k] = __fadd2_rn(wl[k], f2(p.h[k]));
+        wh[k] = __fadd2_rn(wh[k], f2(p.h[k]));
+      }
     }
   float2 sl[N], sh[N], tl[N], th[N];
 #pragma unroll
@@ -280,10 +288,11 @@ __device__ __forceinline__ void quad_site(const QuadParams& p, int q, int h, int
   const uint32_t c0 = counter_of(4 * q, nsite, own);
   const uint32_t ns = (uint32_t)nsite;
   bool a0, a1, a2, a3;
-  finish_values<N>(g.acceptance, cubic, f2(k1), p.k2, c0, c0 + ns, true, make_float2(b4.x, b4.y), key, sl, vl, tl,
-                   a0, a1);
-  finish_values<N>(g.acceptance, cubic, f2(k1), p.k2, c0 + 2 * ns, c0 + 3 * ns, true, make_float2(b4.z, b4.w), key,
-                   sh, vh, th, a2, a3);
+  FinishMeasure fl, fh;
+  finish_values<N, MEASURE>(g.acceptance, cubic, f2(k1), p.k2, c0, c0 + ns, true, make_float2(b4.x, b4.y), key, sl,
+                            vl, tl, a0, a1, kFullLow ? &vl : &wl, &fl);
+  finish_values<N, MEASURE>(g.acceptance, cubic, f2(k1), p.k2, c0 + 2 * ns, c0 + 3 * ns, true,
+                            make_float2(b4.z, b4.w), key, sh, vh, th, a2, a3, kFullLow ? &vh : &wh, &fh);
   float4 n4[N];
 #pragma unroll
   for (int k = 0; k < N; ++k)
@@ -294,36 +303,25 @@ __device__ __forceinline__ void quad_site(const QuadParams& p, int q, int h, int
     for (int k = 0; k < N; ++k) base[own_e + k * L1] = n4[k];
   }
   if constexpr (MEASURE) {
-    // float32 share of the site in each lane, then FP64 sums
-    auto share = [&](float2 n0, float2 n1, float2 n2, const float2 (&w)[N]) {
-      const float2 nn[3] = {n0, n1, n2};
-      float2 bond = __fmul2_rn(nn[0], w[0]);
-#pragma unroll
-      for (int k = 1; k < N; ++k) bond = __fadd2_rn(bond, __fmul2_rn(nn[k], w[k]));
-      float2 e = make_float2(-bond.x, -bond.y);
-#pragma unroll
-      for (int k = 0; k < N; ++k)
-        if (p.hnz[k]) e = __fadd2_rn(e, __fmul2_rn(f2(-p.h[k]), nn[k]));
-      if (cubic) {
-        const float2 q01 = __fmul2_rn(nn[0], nn[1]), q02 = __fmul2_rn(nn[0], nn[2]), q12 = __fmul2_rn(nn[1], nn[2]);
-        const float2 tri = __fmul2_rn(q01, nn[2]);
-        const float2 quad = __fadd2_rn(__fadd2_rn(__fmul2_rn(q01, q01), __fmul2_rn(q02, q02)), __fmul2_rn(q12, q12));
-        e = __fadd2_rn(e, __fadd2_rn(__fmul2_rn(f2(k1), quad), __fmul2_rn(__fmul2_rn(f2(p.k2), tri), tri)));
-      }
-      return e;
+    // float32 share of the site in each lane, -s'.w + anisotropy(s') from the products of both candidate spins,
+    // then its components
+    auto share = [](bool acc, float es, float et, float as, float at) {
+      return acc ? __fadd_rn(-et, at) : __fadd_rn(-es, as);
     };
-    const float2 el = share(lo2(n4[0]), lo2(n4[1 % N]), N == 3 ? lo2(n4[2 % N]) : f2(0.0f), wl);
-    const float2 eh = share(hi2(n4[0]), hi2(n4[1 % N]), N == 3 ? hi2(n4[2 % N]) : f2(0.0f), wh);
-    m.v[0][0] += (double)el.x;
-    m.v[1][0] += (double)el.y;
-    m.v[2][0] += (double)eh.x;
-    m.v[3][0] += (double)eh.y;
+    const float2 el = make_float2(share(a0, fl.es.x, fl.et.x, fl.as.x, fl.at.x),
+                                  share(a1, fl.es.y, fl.et.y, fl.as.y, fl.at.y));
+    const float2 eh = make_float2(share(a2, fh.es.x, fh.et.x, fh.as.x, fh.at.x),
+                                  share(a3, fh.es.y, fh.et.y, fh.as.y, fh.at.y));
+    m.v[0][0] += el.x;
+    m.v[1][0] += el.y;
+    m.v[2][0] += eh.x;
+    m.v[3][0] += eh.y;
 #pragma unroll
     for (int k = 0; k < N; ++k) {
-      m.v[0][1 + k] += (double)n4[k].x;
-      m.v[1][1 + k] += (double)n4[k].y;
-      m.v[2][1 + k] += (double)n4[k].z;
-      m.v[3][1 + k] += (double)n4[k].w;
+      m.v[0][1 + k] += n4[k].x;
+      m.v[1][1 + k] += n4[k].y;
+      m.v[2][1 + k] += n4[k].z;
+      m.v[3][1 + k] += n4[k].w;
     }
   }
 }
@@ -331,14 +329,14 @@ __device__ __forceinline__ void quad_site(const QuadParams& p, int q, int h, int
 template <int V>
 __device__ __forceinline__ void block_sum(double (&x)[V], double (*red)[8]);
 
-// FP64 warp sums of 16 values per lane by recursive halving: at offset o (16, 8, 4, 2) each lane keeps one half
-// of its remaining values, sends the other half to lane ^ o and adds what it receives; the last step (offset 1)
-// adds the pair's single values. Lane l ends with the warp total of value (l >> 1) & 15 in x[0]. 16 shuffles of
-// a double instead of 80; every total is the same fixed binary tree of additions on every call.
-__device__ __forceinline__ void warp_halving_sum16(double (&x)[16]) {
+// FP64 warp sums of 8 values per lane by recursive halving: at offset o (16, 8, 4) each lane keeps one half of its
+// remaining values, sends the other half to lane ^ o and adds what it receives; offsets 2 and 1 then add the single
+// values of the lane groups. Lane l ends with the warp total of value (l >> 2) & 7, the same fixed binary tree of
+// additions on every call.
+__device__ __forceinline__ double warp_halving_sum8(double (&x)[8]) {
   const int lane = threadIdx.x & 31;
 #pragma unroll
-  for (int o = 16, h = 8; o >= 2; o >>= 1, h >>= 1) {
+  for (int o = 16, h = 4; o >= 4; o >>= 1, h >>= 1) {
     const bool hi = (lane & o) != 0;
 #pragma unroll
     for (int i = 0; i < h; ++i) {
@@ -347,30 +345,38 @@ __device__ __forceinline__ void warp_halving_sum16(double (&x)[16]) {
       x[i] = keep + __shfl_xor_sync(0xFFFFFFFFu, send, o);
     }
   }
+  x[0] += __shfl_xor_sync(0xFFFFFFFFu, x[0], 2);
   x[0] += __shfl_xor_sync(0xFFFFFFFFu, x[0], 1);
+  return x[0];
 }
 
 // Measure-step epilogue of a block of 256 threads: the block totals of the (1 + N) values of each of the four
-// lanes of a quad, in a fixed order (warp halving sums, then the 8 warps in order); thread v < 4 (1 + N) gets
-// value v (lane v / (1 + N), component v % (1 + N)), the other threads 0. Every thread of the block must call it.
-template <int N>
-__device__ __forceinline__ double measure_block_sum(const MeasureAcc<N>& m) {
+// lanes of a quad, in a fixed order (two warp halving sums, of lanes 0-1 and of lanes 2-3, each converting its
+// eight values to FP64 only when it runs; then the 8 warps in order); thread v < 4 (1 + N) gets value v (lane
+// v / (1 + N), component v % (1 + N)), the other threads 0. Every thread of the block must call it.
+template <int N, class T>
+__device__ __forceinline__ double measure_block_sum(const MeasureAcc<N, T>& m) {
   __shared__ double red[8][16];
-  double x[16];
-#pragma unroll
-  for (int i = 0; i < 16; ++i) x[i] = 0.0;
-#pragma unroll
-  for (int j = 0; j < 4; ++j)
-#pragma unroll
-    for (int v = 0; v <= N; ++v) x[j * (1 + N) + v] = m.v[j][v];
-  warp_halving_sum16(x);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if ((lane & 1) == 0) red[warp][lane >> 1] = x[0];
+#pragma unroll
+  for (int pass = 0; pass < 2; ++pass) {
+    double x[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) x[i] = 0.0;
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int v = 0; v <= N; ++v) x[j * (1 + N) + v] = (double)m.v[2 * pass + j][v];
+    const double t = warp_halving_sum8(x);
+    if ((lane & 3) == 0) red[warp][pass * 8 + (lane >> 2)] = t;
+  }
   __syncthreads();
   double v = 0.0;
   if (threadIdx.x < 4 * (1 + N)) {
+    const int j = threadIdx.x / (1 + N), c = threadIdx.x - j * (1 + N);
+    const int slot = (j >> 1) * 8 + (j & 1) * (1 + N) + c;
 #pragma unroll
-    for (int w = 0; w < 8; ++w) v += red[w][threadIdx.x];
+    for (int w = 0; w < 8; ++w) v += red[w][slot];
   }
   return v;
 }
@@ -382,12 +388,21 @@ __device__ __forceinline__ double measure_block_sum(const MeasureAcc<N>& m) {
 #ifndef SCK_QUAD_MEASURE_MIN_BLOCKS
 #define SCK_QUAD_MEASURE_MIN_BLOCKS 3
 #endif
+#ifndef SCK_QUAD_CUBE_MEASURE_MIN_BLOCKS
+#define SCK_QUAD_CUBE_MEASURE_MIN_BLOCKS 3
+#endif
 
 // Grid (ceil(L3 L2 L1 / P / 256), quads of this launch). Thread -> (row, position in the row's class segment).
 // The cubic instantiations run four blocks per SM (64 registers): 78 against 77 attempts/ns at three on the 3D
 // Heisenberg bcc J1-J2 workload.
-template <class Lat, int N, int P, int L1C, bool MEASURE>
-__global__ void __launch_bounds__(256, MEASURE ? SCK_QUAD_MEASURE_MIN_BLOCKS : (L1C < 0 ? 4 : SCK_QUAD_MIN_BLOCKS))
+// Measure kernels of the cubic boxes take the class's lower coupling groups as a compile-time mask LOW; the
+// others read them at run time (LOW = -1). Both run three blocks per SM: at four (64 registers) the measure
+// kernels spill 140-244 bytes a thread, and a measure sweep of the 3D Heisenberg bcc J1-J2 workload ran at 60
+// attempts/ns against 64 at three (12-44 bytes).
+template <class Lat, int N, int P, int L1C, bool MEASURE, int LOW = -1>
+__global__ void __launch_bounds__(256, MEASURE ? (LOW >= 0 ? SCK_QUAD_CUBE_MEASURE_MIN_BLOCKS
+                                                            : SCK_QUAD_MEASURE_MIN_BLOCKS)
+                                               : (L1C < 0 ? 4 : SCK_QUAD_MIN_BLOCKS))
     quad_class_kernel(const __grid_constant__ QuadParams p) {
   const Geometry& g = p.g;
   using D = QDim<L1C>;
@@ -406,12 +421,12 @@ __global__ void __launch_bounds__(256, MEASURE ? SCK_QUAD_MEASURE_MIN_BLOCKS : (
     h = t - row * (uint32_t)p.hp;
   }
   const int q = p.q0 + (int)blockIdx.y;
-  MeasureAcc<N> m;
+  MeasureAcc<N, float> m;
   if constexpr (MEASURE) {
 #pragma unroll
     for (int j = 0; j < 4; ++j)
 #pragma unroll
-      for (int v = 0; v <= N; ++v) m.v[j][v] = 0.0;
+      for (int v = 0; v <= N; ++v) m.v[j][v] = 0.0f;
   }
   if (row < (uint32_t)(D::L3(g) * D::L2(g))) {
     const int z = D::cube ? (int)(row / (uint32_t)D::E) : (int)fdiv(row, p.fd_L2);
@@ -421,13 +436,13 @@ __global__ void __launch_bounds__(256, MEASURE ? SCK_QUAD_MEASURE_MIN_BLOCKS : (
       const int32_t key = sweep_key_at(p.state, p.sweep_offset);
       static_for<0, Lat::b>([&](auto ac) {
         constexpr int a = decltype(ac)::value;
-        if (a == p.alpha) quad_site<Lat, a, N, P, L1C, MEASURE, true>(p, q, (int)h, ph, y, z, key, m);
+        if (a == p.alpha) quad_site<Lat, a, N, P, L1C, MEASURE, true, LOW>(p, q, (int)h, ph, y, z, key, m);
       });
     }
   }
   if constexpr (MEASURE) {
     // every thread of the block reaches here: block sums in a fixed order, one partial per (replica, value)
-    const double val = measure_block_sum<N>(m);
+    const double val = measure_block_sum(m);
     if (threadIdx.x < 4 * (1 + N)) {
       const int j = threadIdx.x / (1 + N), v = threadIdx.x - j * (1 + N);
       const int rep = 4 * q + j;
@@ -548,7 +563,7 @@ __global__ void __launch_bounds__(256, SCK_QUAD_MIN_BLOCKS) quad_pipe_kernel(con
   }
   if constexpr (MEASURE) {
     if (measuring) {
-      const double val = measure_block_sum<N>(m);
+      const double val = measure_block_sum(m);
       if (threadIdx.x < 4 * (1 + N) && s.q < pp.Q) {
         const int j = threadIdx.x / (1 + N), v = threadIdx.x - j * (1 + N);
         const int rep = 4 * s.q + j;
@@ -677,12 +692,25 @@ __global__ void __launch_bounds__(256) quad_observables_kernel(const __grid_cons
 
 
 // ------------------------------------------------------------------------------------------- launchers
+// Measure launch with the compile-time mask of p.lower_groups, tried from LOW down to 0 (-1: the run-time mask).
+template <class Lat, int N, int P, int L1C, int LOW>
+inline void launch_measure_low(const QuadParams& p, dim3 grid, cudaStream_t s) {
+  if constexpr (LOW < 0) {
+    quad_class_kernel<Lat, N, P, L1C, true, -1><<<grid, 256, 0, s>>>(p);
+  } else {
+    if (p.lower_groups == (unsigned)LOW) quad_class_kernel<Lat, N, P, L1C, true, LOW><<<grid, 256, 0, s>>>(p);
+    else launch_measure_low<Lat, N, P, L1C, LOW - 1>(p, grid, s);
+  }
+}
+
 template <class Lat, int N, int P, int L1C>
 inline void launch_quad_t(const QuadParams& p, dim3 grid, cudaStream_t s) {
-  if (p.partial != nullptr)
-    quad_class_kernel<Lat, N, P, L1C, true><<<grid, 256, 0, s>>>(p);
-  else
+  if (p.partial != nullptr) {
+    if constexpr (L1C < 0 && N == 3) launch_measure_low<Lat, N, P, L1C, (1 << Lat::groups) - 1>(p, grid, s);
+    else quad_class_kernel<Lat, N, P, L1C, true><<<grid, 256, 0, s>>>(p);
+  } else {
     quad_class_kernel<Lat, N, P, L1C, false><<<grid, 256, 0, s>>>(p);
+  }
 }
 
 template <class Lat, int N, int P>

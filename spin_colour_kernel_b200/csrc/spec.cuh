@@ -109,10 +109,18 @@ __device__ __forceinline__ void sincos_2pi(float phi, float& sn, float& cs) {
 // float32x2 operations round each lane to nearest. With two == false lane .y repeats lane .x's draws and its
 // result is ignored. The lattice kernels (finish_core below) and the interleaved kernels (quad.cu) both call it,
 // so the two storage layouts compute identical numbers.
-template <int N>
+// With MEAS (a measure step), also fm: the products s.wm and t.wm with the measure field wm (the fields of the
+// neighbours updated earlier in the sweep and the external field), and the anisotropy energies of s and t (0
+// without cubic anisotropy), so that the energy share of the site's final spin needs no second evaluation.
+struct FinishMeasure {
+  float2 es, et, as, at;
+};
+
+template <int N, bool MEAS = false>
 __device__ __forceinline__ void finish_values(int acceptance, bool cubic, float2 k1, float k2c, uint32_t cnt0,
                                               uint32_t cnt1, bool two, float2 beta, int32_t key, const float2 (&s)[N],
-                                              const float2 (&v)[N], float2 (&t)[N], bool& acc0, bool& acc1) {
+                                              const float2 (&v)[N], float2 (&t)[N], bool& acc0, bool& acc1,
+                                              const float2 (*wm)[N] = nullptr, FinishMeasure* fm = nullptr) {
   const Philox4 ra = philox4x32_10(cnt0, 0u, key_lo(key), key_hi(key));
   const Philox4 rb = two ? philox4x32_10(cnt1, 0u, key_lo(key), key_hi(key)) : ra;
   const float2 u0 = make_float2(to_uniform(ra.x0), to_uniform(rb.x0));
@@ -138,6 +146,17 @@ __device__ __forceinline__ void finish_values(int acceptance, bool cubic, float2
   }
   // -1 * x is exact, so the reference's t + (-1) s and (-1) d are written as a subtraction and a negation
   auto neg = [](float2 a) { return make_float2(-a.x, -a.y); };
+  if constexpr (MEAS) {
+    float2 es = __fmul2_rn(s[0], (*wm)[0]), et = __fmul2_rn(t[0], (*wm)[0]);
+#pragma unroll
+    for (int k = 1; k < N; ++k) {
+      es = __fadd2_rn(es, __fmul2_rn(s[k], (*wm)[k]));
+      et = __fadd2_rn(et, __fmul2_rn(t[k], (*wm)[k]));
+    }
+    fm->es = es;
+    fm->et = et;
+    fm->as = fm->at = f2(0.0f);
+  }
   float2 d = __fmul2_rn(__fadd2_rn(t[0], neg(s[0])), v[0]);
 #pragma unroll
   for (int k = 1; k < N; ++k) d = __fadd2_rn(d, __fmul2_rn(__fadd2_rn(t[k], neg(s[k])), v[k]));
@@ -151,7 +170,12 @@ __device__ __forceinline__ void finish_values(int acceptance, bool cubic, float2
         const float2 quad = __fadd2_rn(__fadd2_rn(__fmul2_rn(q01, q01), __fmul2_rn(q02, q02)), __fmul2_rn(q12, q12));
         return __fadd2_rn(__fmul2_rn(k1, quad), __fmul2_rn(__fmul2_rn(k2, tri), tri));
       };
-      dE = __fadd2_rn(dE, __fadd2_rn(aniso(t), neg(aniso(s))));
+      const float2 an_t = aniso(t), an_s = aniso(s);
+      dE = __fadd2_rn(dE, __fadd2_rn(an_t, neg(an_s)));
+      if constexpr (MEAS) {
+        fm->as = an_s;
+        fm->at = an_t;
+      }
     }
   }
   if (acceptance == SCK_BARKER) {
