@@ -288,11 +288,21 @@ __device__ __forceinline__ void quad_site(const QuadParams& p, int q, int h, int
   const uint32_t c0 = counter_of(4 * q, nsite, own);
   const uint32_t ns = (uint32_t)nsite;
   bool a0, a1, a2, a3;
+  // measure: the float32 energy share of each lane's final spin, -s'.w + anisotropy(s'), from the products of
+  // both candidates, taken as soon as each pair's decision is known
   FinishMeasure fl, fh;
+  auto share = [](bool acc, float es, float et, float as, float at) {
+    return acc ? __fadd_rn(-et, at) : __fadd_rn(-es, as);
+  };
+  float2 el, eh;
   finish_values<N, MEASURE>(g.acceptance, cubic, f2(k1), p.k2, c0, c0 + ns, true, make_float2(b4.x, b4.y), key, sl,
                             vl, tl, a0, a1, kFullLow ? &vl : &wl, &fl);
+  if constexpr (MEASURE)
+    el = make_float2(share(a0, fl.es.x, fl.et.x, fl.as.x, fl.at.x), share(a1, fl.es.y, fl.et.y, fl.as.y, fl.at.y));
   finish_values<N, MEASURE>(g.acceptance, cubic, f2(k1), p.k2, c0 + 2 * ns, c0 + 3 * ns, true,
                             make_float2(b4.z, b4.w), key, sh, vh, th, a2, a3, kFullLow ? &vh : &wh, &fh);
+  if constexpr (MEASURE)
+    eh = make_float2(share(a2, fh.es.x, fh.et.x, fh.as.x, fh.at.x), share(a3, fh.es.y, fh.et.y, fh.as.y, fh.at.y));
   float4 n4[N];
 #pragma unroll
   for (int k = 0; k < N; ++k)
@@ -303,15 +313,7 @@ __device__ __forceinline__ void quad_site(const QuadParams& p, int q, int h, int
     for (int k = 0; k < N; ++k) base[own_e + k * L1] = n4[k];
   }
   if constexpr (MEASURE) {
-    // float32 share of the site in each lane, -s'.w + anisotropy(s') from the products of both candidate spins,
-    // then its components
-    auto share = [](bool acc, float es, float et, float as, float at) {
-      return acc ? __fadd_rn(-et, at) : __fadd_rn(-es, as);
-    };
-    const float2 el = make_float2(share(a0, fl.es.x, fl.et.x, fl.as.x, fl.at.x),
-                                  share(a1, fl.es.y, fl.et.y, fl.as.y, fl.at.y));
-    const float2 eh = make_float2(share(a2, fh.es.x, fh.et.x, fh.as.x, fh.at.x),
-                                  share(a3, fh.es.y, fh.et.y, fh.as.y, fh.at.y));
+    // the lanes' shares and components
     m.v[0][0] += el.x;
     m.v[1][0] += el.y;
     m.v[2][0] += eh.x;
