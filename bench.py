@@ -216,10 +216,11 @@ def reference_arm(args, rank, world):
 def reference_triton_arm(args, rank, world):
     """The reference's own GPU path on this B200: its generated Triton class kernels, driven through its public
     Sampler (Sampler(...).graph(S, k) replays timed with CUDA events, as its exp_perf.rate times them), from the
-    unmodified package installed in baseline/_ref; none of this repository's kernels is loaded. Same workload as
-    the default arm (Heisenberg bcc 64^3 x 2, J1-J2, K1, h_z, 1,536 replicas at 24 temperatures; spins uniform on
-    the sphere drawn on the device). Prints the `unavailable` line with the reason when the package or its Triton
-    compilation is missing here."""
+    unmodified package installed in baseline/_ref; none of this repository's kernels is loaded. Same workloads as
+    this repository's arm: `heisenberg-bcc` (64^3 x 2, J1-J2, K1, h_z, 1,536 replicas at 24 temperatures; spins
+    uniform on the sphere drawn on the device), `ising-square` (32^2, 32 int8 replicas) and `ising-sc-bitwise`
+    (128^3, 512 replicas in shared-draw bitwise words). Prints the `unavailable` line with the reason when the
+    package or its Triton compilation is missing here."""
     if rank != 0:
         return
     import tempfile
@@ -237,13 +238,33 @@ def reference_triton_arm(args, rank, world):
         device = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
         torch.cuda.set_device(device)
         L, B = args.L, args.replicas
-        s = rsy.System("Heisenberg bcc J1-J2", 3, rcr.make("bcc", (1, 2)), (L, L, L), (True,) * 3, {1: 1.0, 2: 0.3},
-                       h=(0.0, 0.0, 0.1), cubic_k1=np.full((2, L, L, L), 0.05, np.float32))
-        A = RefSampler(s, B, device, 1234)
-        A.set_temperature(torch.linspace(0.5, 2.5, 24).repeat_interleave(-(-B // 24))[:B])
         g = torch.Generator(device=device).manual_seed(2)
-        S = torch.randn((B, 3) + s.shape, device=device, generator=g)
-        S = (S / S.norm(dim=1, keepdim=True)).contiguous()
+        if args.workload == "ising-square":
+            s = rsy.ising("square", 32)
+            B = 32
+            A = RefSampler(s, B, device, 1234, packed=False)
+            A.set_temperature(torch.tensor([1.5, 2.0, 2.269, 3.0]).repeat_interleave(8))
+            S = A.init_spins(seed=0)
+            workload, dtype, sites = "ising-square-32^2-int8", "i8", int(s.n_active)
+        elif args.workload == "ising-sc-bitwise":
+            s = rsy.ising("sc", 128)
+            B = 512
+            A = RefSampler(s, B, device, 1, bitwise=True)
+            A.set_temperature(torch.linspace(4.0, 5.0, 16)[:8].repeat_interleave(64))
+            S = A.pack(torch.randint(0, 2, (B, 1) + s.shape, device=device, generator=g, dtype=torch.int8) * 2 - 1)
+            workload, dtype, sites = "ising-sc-128^3-bitwise-shared", "u32", int(s.n_active)
+        elif args.workload == "heisenberg-bcc":
+            s = rsy.System("Heisenberg bcc J1-J2", 3, rcr.make("bcc", (1, 2)), (L, L, L), (True,) * 3,
+                           {1: 1.0, 2: 0.3}, h=(0.0, 0.0, 0.1), cubic_k1=np.full((2, L, L, L), 0.05, np.float32))
+            A = RefSampler(s, B, device, 1234)
+            A.set_temperature(torch.linspace(0.5, 2.5, 24).repeat_interleave(-(-B // 24))[:B])
+            S = torch.randn((B, 3) + s.shape, device=device, generator=g)
+            S = (S / S.norm(dim=1, keepdim=True)).contiguous()
+            workload, dtype, sites = f"heisenberg-bcc-{L}^3x2-J1J2-K1-hz", "f32", 2 * L ** 3
+        else:
+            print(json.dumps({**base, "unavailable": f"no reference-triton form of workload {args.workload}"}),
+                  flush=True)
+            return
         replay = A.graph(S, 1)
         for _ in range(max(1, args.warmup)):
             replay()
@@ -265,17 +286,18 @@ def reference_triton_arm(args, rank, world):
         return
     value = B * s.n_active * args.steps / (ms * 1e6)
     peak, kind = hbm_peak()
-    achieved = value * 24.0
+    bpa = BYTES_PER_ATTEMPT[args.workload]
+    achieved = value * bpa
     loaded = sorted({m.__name__.split(".")[0] for m in list(sys.modules.values()) if m is not None and
                      getattr(m, "__name__", "").startswith(("spin_colour_kernel_b200", "Spin_Colour_Kernel"))})
     line = {**base, "value": value, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"heisenberg-bcc-{L}^3x2-J1J2-K1-hz", "replicas": B, "sites": 2 * L ** 3,
+            "dtype": dtype, "data": "synthetic",
+            "config": {"workload": workload, "replicas": B, "sites": sites,
                        "path": "reference Sampler.graph(S, 1) replays (generated Triton class kernels)",
                        "python_packages_loaded": loaded},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "note": f"algorithmic 24 B/attempt over the replay; peak {kind}"},
+                         "traffic": None, "note": f"algorithmic {bpa} B/attempt over the replay; peak {kind}"},
             "clocks": clk}
     print(json.dumps(line), flush=True)
 

@@ -17,20 +17,36 @@ namespace sck {
 
 constexpr int bitlen(int v) { return v <= 0 ? 0 : 1 + bitlen(v >> 1); }
 
-// Count planes of one (word, site): returns z_eff; planes c[0..NP).
-template <int NP>
-__device__ __forceinline__ int count_planes(const Common& c, const SubDev& sub, int x, int y, int z, uint32_t s0,
-                                            const uint32_t* sp, size_t wb, uint32_t (&cp)[NP]) {
+// Neighbour site indices of (x, y, z) along the sublattice's bonds, in bond order (-1: absent, outside an open box
+// or masked); returns z_eff. Computed once per site and shared by every word the thread updates.
+template <int ZM>
+__device__ __forceinline__ int neighbour_sites(const Common& c, const SubDev& sub, int x, int y, int z,
+                                               int (&nq)[ZM]) {
   const Geometry& g = c.g;
+  int ze = 0;
+#pragma unroll
+  for (int bi = 0; bi < ZM; ++bi) {
+    int q = -1;
+    if (bi < sub.n_bonds) {
+      q = neighbour_index(g, sub.bonds[bi], x, y, z);
+      if (q >= 0 && g.has_mask && c.mask[q] == 0) q = -1;
+    }
+    nq[bi] = q;
+    ze += q >= 0 ? 1 : 0;
+  }
+  return ze;
+}
+
+// Count planes c[0..NP) of one (word, site) from its neighbour sites: a ripple adder over the present bonds.
+template <int NP, int ZM>
+__device__ __forceinline__ void count_planes(const int (&nq)[ZM], uint32_t s0, const uint32_t* sp, size_t wb,
+                                             uint32_t (&cp)[NP]) {
 #pragma unroll
   for (int p = 0; p < NP; ++p) cp[p] = 0u;
-  int ze = 0;
-  for (int bi = 0; bi < sub.n_bonds; ++bi) {
-    const BondDev bd = sub.bonds[bi];
-    const int q = neighbour_index(g, bd, x, y, z);
-    if (q < 0 || (g.has_mask && c.mask[q] == 0)) continue;
-    ++ze;
-    uint32_t cy = s0 ^ sp[wb + q];
+#pragma unroll
+  for (int bi = 0; bi < ZM; ++bi) {
+    if (nq[bi] < 0) continue;
+    uint32_t cy = s0 ^ sp[wb + nq[bi]];
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
       const uint32_t carry = cp[p] & cy;
@@ -38,7 +54,6 @@ __device__ __forceinline__ int count_planes(const Common& c, const SubDev& sub, 
       cy = carry;
     }
   }
-  return ze;
 }
 
 template <int NP>
@@ -60,6 +75,8 @@ __device__ __forceinline__ void shared_site(const Common& c, const SubDev& sub, 
   const Philox4 r = philox4x32_10((uint32_t)((unsigned long long)grp * g.nsite + own), 0u, key_lo(key), key_hi(key));
   const float us[4] = {to_uniform(r.x0), to_uniform(r.x1), to_uniform(r.x2), to_uniform(r.x3)};
   const float* table = (const float*)c.table;
+  int nq[ZM];
+  const int ze = neighbour_sites<ZM>(c, sub, x, y, z, nq);
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     const int w = grp * 4 + q;
@@ -67,7 +84,7 @@ __device__ __forceinline__ void shared_site(const Common& c, const SubDev& sub, 
     const size_t wb = (size_t)w * g.nsite;
     const uint32_t s0 = src[wb + own];
     uint32_t cp[NP];
-    const int ze = count_planes<NP>(c, sub, x, y, z, s0, src, wb, cp);
+    count_planes<NP, ZM>(nq, s0, src, wb, cp);
     const float* tb = table + (size_t)w * c.NT + ze * c.Z1;
     const float u = us[q];
     uint32_t acc = 0u;
@@ -100,7 +117,9 @@ __device__ __forceinline__ void independent_site(const Common& c, const SubDev& 
   const size_t wb = (size_t)w * g.nsite;
   const uint32_t s0 = src[wb + own];
   uint32_t cp[NP];
-  const int ze = count_planes<NP>(c, sub, x, y, z, s0, src, wb, cp);
+  int nq[ZM];
+  const int ze = neighbour_sites<ZM>(c, sub, x, y, z, nq);
+  count_planes<NP, ZM>(nq, s0, src, wb, cp);
   const long long* tb = (const long long*)c.table + (size_t)w * c.NT + ze * c.Z1;
   uint32_t em[ZM + 1], ep[ZM + 1], Pm[ZM + 1], Pp[ZM + 1];
   uint32_t acc = 0u, und = 0u;
@@ -143,9 +162,14 @@ __device__ __forceinline__ void independent_site(const Common& c, const SubDev& 
   dst[wb + own] = s0 ^ acc;
 }
 
+// Blocks of 256 threads per SM the class kernel is compiled for.
+#ifndef SCK_BITWISE_MIN_BLOCKS
+#define SCK_BITWISE_MIN_BLOCKS 4
+#endif
+
 // Grid (ceil(rows * bx / 256), units): units are groups of four words (shared) or words (independent).
 template <int ZM, bool INDEP>
-__global__ void __launch_bounds__(256) bitwise_class_kernel(const __grid_constant__ ClassParams p) {
+__global__ void __launch_bounds__(256, SCK_BITWISE_MIN_BLOCKS) bitwise_class_kernel(const __grid_constant__ ClassParams p) {
   const Common& c = p.c;
   const uint32_t per = (uint32_t)c.rows * (uint32_t)c.bx;
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
