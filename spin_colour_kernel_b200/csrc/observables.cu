@@ -444,8 +444,19 @@ static bool obs_tiled(const sck_plan* plan, int storage) {
 
 // Blocks per replica, hence partial-sum slots per replica, of one observables call: the one count that both the
 // launch and the size checks of its callers use, so the slots written and the slots summed always agree.
+static bool obs_words_ok(const sck_plan* plan, int storage);
+
+// Blocks per word of 32 replicas of the word-parallel kernel: about 8 blocks per SM over all words.
+static int obs_blocks_words(const sck_plan* plan, int batch) {
+  const int per_rep = (plan->geom.nsite + 255) / 256;
+  const int words = (batch + 31) / 32;
+  const int want = (148 * 8 + words - 1) / words;
+  return want < per_rep ? (want < 1 ? 1 : want) : per_rep;
+}
+
 int obs_launch_blocks(const sck_plan* plan, int storage, int batch) {
   if (storage == SCK_MODE_QUAD) return quad_obs_blocks(plan);
+  if (obs_words_ok(plan, storage)) return obs_blocks_words(plan, batch);
   return obs_tiled(plan, storage) ? plan->geom.L2 / OBS_TY : obs_blocks_generic(plan, batch);
 }
 
@@ -456,6 +467,7 @@ int obs_blocks_per_rep(const sck_plan* plan, int batch) {
   const int tile = obs_tile_geometry(plan) ? plan->geom.L2 / OBS_TY : 0;
   if (tile > most) most = tile;
   if (plan->mode == SCK_MODE_QUAD && quad_obs_blocks(plan) > most) most = quad_obs_blocks(plan);
+  if (obs_words_ok(plan, SCK_MODE_PACKED) && obs_blocks_words(plan, batch) > most) most = obs_blocks_words(plan, batch);
   return most;
 }
 
@@ -547,6 +559,114 @@ int launch_topological_charge(const sck_plan* plan, const float* spins, const in
   return cuda_status(cudaGetLastError(), "topological charge");
 }
 
+// Packed words of a single-sublattice Ising system with isotropic bonds (at most 8): one thread per (word, site)
+// updates 32 replicas at once. Per present bond b, x_b = s XOR s_j marks the anti-aligned replicas; a warp turns
+// each per-thread lane mask into per-replica counts over its 32 sites (lane l: popcount of the ballot of bit l),
+// so lane l accumulates, in integers (exact in any order), A_b = anti-aligned pairs of bond b, U = up spins, and
+// the lane-independent P_b = present pairs and S = present sites. Then replica 32 w + l of the block:
+//   E = sum_b -J_b (P_b - 2 A_b) / 2 - h (2 U - S),   M = 2 U - S,
+// the same site energy -1/2 s v - h s as observables_kernel, written to the same partial slots.
+constexpr int kWordObsBonds = 8;
+
+__global__ void __launch_bounds__(256) observables_words_kernel(const __grid_constant__ ObsParams p) {
+  const Geometry& g = p.g;
+  const int w = blockIdx.y;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const SubDev& sub = p.sub[0];
+  const int nb = sub.n_bonds;
+  unsigned A[kWordObsBonds], P[kWordObsBonds], U = 0u, S = 0u;
+#pragma unroll
+  for (int b = 0; b < kWordObsBonds; ++b) A[b] = P[b] = 0u;
+  const uint32_t* words = (const uint32_t*)p.spins + (size_t)w * g.nsite;
+  const int stride = p.blocks_per_rep * blockDim.x;
+  // every thread of a warp runs the same iterations (the ballots need the whole warp)
+  for (int base = blockIdx.x * blockDim.x + warp * 32; base < g.nsite; base += stride) {
+    const int site = base + lane;
+    bool present = site < g.nsite && (p.mask == nullptr || p.mask[site] != 0);
+    uint32_t s0 = 0u;
+    int x = 0, y = 0, z = 0;
+    if (present) {
+      const int row = (int)fdiv((uint32_t)site, p.fd_L1);
+      x = site - row * g.L1;
+      z = (int)fdiv((uint32_t)row, p.fd_L2);
+      y = row - z * g.L2;
+      s0 = words[site];
+    }
+    const unsigned sites_here = __popc(__ballot_sync(0xFFFFFFFFu, present));
+    S += sites_here;
+#pragma unroll 1
+    for (int l = 0; l < 32; ++l) {
+      const unsigned c = __popc(__ballot_sync(0xFFFFFFFFu, present && ((s0 >> l) & 1u)));
+      if (lane == l) U += c;
+    }
+#pragma unroll
+    for (int b = 0; b < kWordObsBonds; ++b) {
+      if (b >= nb) break;
+      bool pb = false;
+      uint32_t xb = 0u;
+      if (present) {
+        const int q = neighbour_index(g, sub.bonds[b], x, y, z);
+        if (q >= 0 && (p.mask == nullptr || p.mask[q] != 0)) {
+          pb = true;
+          xb = s0 ^ words[q];
+        }
+      }
+      P[b] += __popc(__ballot_sync(0xFFFFFFFFu, pb));
+#pragma unroll 1
+      for (int l = 0; l < 32; ++l) {
+        const unsigned c = __popc(__ballot_sync(0xFFFFFFFFu, pb && ((xb >> l) & 1u)));
+        if (lane == l) A[b] += c;
+      }
+    }
+  }
+  // block sums per lane (integers), then FP64 per replica
+  __shared__ unsigned red[8][2 * kWordObsBonds + 2][32];
+#pragma unroll
+  for (int b = 0; b < kWordObsBonds; ++b) {
+    red[warp][b][lane] = A[b];
+    red[warp][kWordObsBonds + b][lane] = P[b];
+  }
+  red[warp][2 * kWordObsBonds][lane] = U;
+  red[warp][2 * kWordObsBonds + 1][lane] = S;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    unsigned long long a[kWordObsBonds], pp[kWordObsBonds], u = 0, sn = 0;
+#pragma unroll
+    for (int b = 0; b < kWordObsBonds; ++b) a[b] = pp[b] = 0;
+    for (int wi = 0; wi < (int)(blockDim.x >> 5); ++wi) {
+#pragma unroll
+      for (int b = 0; b < kWordObsBonds; ++b) {
+        a[b] += red[wi][b][lane];
+        pp[b] += red[wi][kWordObsBonds + b][lane];
+      }
+      u += red[wi][2 * kWordObsBonds][lane];
+      sn += red[wi][2 * kWordObsBonds + 1][lane];
+    }
+    double e = 0.0;
+#pragma unroll
+    for (int b = 0; b < kWordObsBonds; ++b)
+      if (b < nb) e += -0.5 * p.obs[0].J[b] * ((double)pp[b] - 2.0 * (double)a[b]);
+    const double m = 2.0 * (double)u - (double)sn;
+    e -= p.h64[0] * m;
+    const int rep = 32 * w + lane;
+    if (rep < p.B) {
+      double* out = p.partial + ((size_t)rep * p.blocks_per_rep + blockIdx.x) * OBS_VALUES;
+      out[0] = e;
+      out[1] = m;
+    }
+  }
+}
+
+// The word kernel's conditions: packed words, one sublattice, n = 1, at most kWordObsBonds isotropic bonds.
+static bool obs_words_ok(const sck_plan* plan, int storage) {
+  if (storage != SCK_MODE_PACKED || plan->geom.b != 1 || plan->geom.n != 1) return false;
+  const SubDev& sub = plan->sub[0];
+  if (sub.n_bonds > kWordObsBonds) return false;
+  for (int i = 0; i < sub.n_bonds; ++i)
+    if (sub.bonds[i].extra >= 0) return false;
+  return true;
+}
+
 int launch_observables(const sck_plan* plan, const void* spins, int storage, int batch, const int8_t* mask,
                        const float* k1, double* E, double* M, void* workspace, cudaStream_t s) {
   if (storage == SCK_MODE_QUAD) return launch_quad_observables(plan, spins, batch, k1, E, M, workspace, s);
@@ -595,6 +715,8 @@ int launch_observables(const sck_plan* plan, const void* spins, int storage, int
       case Lat_bcc_1_2::id: launch_obs_spec<Lat_bcc_1_2>(p, grid, s); break;
       default: launch_obs_spec<Lat_fcc_1>(p, grid, s); break;
     }
+  } else if (p.storage == 2 && obs_words_ok(plan, storage)) {
+    observables_words_kernel<<<dim3(p.blocks_per_rep, (p.B + 31) / 32), 256, 0, s>>>(p);
   } else if (p.storage == 2) observables_kernel<1, 2><<<grid, 256, 0, s>>>(p);
   else if (p.storage == 0) observables_kernel<1, 0><<<grid, 256, 0, s>>>(p);
   else if (n == 1) observables_kernel<1, 1><<<grid, 256, 0, s>>>(p);

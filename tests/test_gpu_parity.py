@@ -170,6 +170,32 @@ def test_packed_equals_int8_on_larger_box():
     assert torch.allclose(P.energy(Sp), I8.energy(S8), rtol=0, atol=1e-9)
 
 
+@pytest.mark.parametrize("make, B, kw", [
+    (lambda: sy.System("Ising sc h", 1, cr.make("sc"), (12, 10, 14), (True,) * 3, {1: 1.0}, h=(0.15,)), 72, {}),
+    (lambda: C._masked_square(sy, cr), 40, {}),
+    (lambda: C._masked_open_sc(sy, cr), 33, {}),
+    (lambda: sy.ising("triangular", 16), 96, {}),
+    (lambda: sy.ising("sc", 16), 64, {"bitwise": True})])
+def test_packed_word_observables_equal_int8(make, B, kw):
+    """The word-parallel observables of packed storage (32 replicas per thread, per-replica counts by warp
+    ballots) equal the int8 path's FP64 energies and magnetizations: masks, open boundaries, a field and a
+    partial last word included."""
+    from spin_colour_kernel_b200.sampler import Sampler
+    s = make()
+    P = Sampler(s, B, device="cuda", seed=5, **kw)
+    I8 = Sampler(s, B, device="cuda", seed=5, packed=False)
+    T = torch.linspace(3.5, 5.5, B // 32).repeat_interleave(32) if kw else torch.linspace(1.5, 6.0, B)
+    for X in (P, I8):
+        X.set_temperature(T)
+    Sp = P.init_spins(seed=9)
+    P.sweep(Sp, 3)
+    S8 = P.unpack(Sp)
+    E1, M1 = P.observables(Sp)
+    E2, M2 = I8.observables(S8)
+    np.testing.assert_allclose(E1.cpu().numpy(), E2.cpu().numpy(), rtol=1e-12, atol=1e-9, err_msg=s.name)
+    np.testing.assert_array_equal(M1.cpu().numpy(), M2.cpu().numpy(), err_msg=s.name)
+
+
 @pytest.mark.parametrize("build", [lambda: C.heisenberg_bcc_j1j2(sy, cr, 8), lambda: sy.ising("sc", 10),
                                    lambda: sy.xy("square", 24), lambda: sy.ising("fcc", 4)])
 def test_l2_group_pipeline_equals_class_by_class(build):
