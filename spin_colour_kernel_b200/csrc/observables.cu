@@ -561,12 +561,25 @@ int launch_topological_charge(const sck_plan* plan, const float* spins, const in
 
 // Packed words of a single-sublattice Ising system with isotropic bonds (at most 8): one thread per (word, site)
 // updates 32 replicas at once. Per present bond b, x_b = s XOR s_j marks the anti-aligned replicas; a warp turns
-// each per-thread lane mask into per-replica counts over its 32 sites (lane l: popcount of the ballot of bit l),
-// so lane l accumulates, in integers (exact in any order), A_b = anti-aligned pairs of bond b, U = up spins, and
+// each per-thread lane mask into per-replica counts over its 32 sites (a 32 x 32 bit transpose across the warp,
+// then a popcount: lane l ends with bit l of every thread's mask), so lane l accumulates, in integers (exact in any order), A_b = anti-aligned pairs of bond b, U = up spins, and
 // the lane-independent P_b = present pairs and S = present sites. Then replica 32 w + l of the block:
 //   E = sum_b -J_b (P_b - 2 A_b) / 2 - h (2 U - S),   M = 2 U - S,
 // the same site energy -1/2 s v - h s as observables_kernel, written to the same partial slots.
 constexpr int kWordObsBonds = 8;
+
+// Number of threads of the warp whose mask has bit `lane` set, for every lane at once: the warp's 32 masks as a
+// 32 x 32 bit matrix (row = thread, column = bit) transposed by exchanging off-diagonal blocks of 16, 8, 4, 2 and
+// 1 across lane ^ s, then the popcount of the lane's column.
+__device__ __forceinline__ unsigned warp_lane_counts(uint32_t x, int lane) {
+  const uint32_t lo[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
+#pragma unroll
+  for (int i = 0, sh = 16; i < 5; ++i, sh >>= 1) {
+    const uint32_t y = __shfl_xor_sync(0xFFFFFFFFu, x, sh);
+    x = (lane & sh) ? ((x & ~lo[i]) | ((y & ~lo[i]) >> sh)) : ((x & lo[i]) | ((y & lo[i]) << sh));
+  }
+  return (unsigned)__popc(x);
+}
 
 __global__ void __launch_bounds__(256) observables_words_kernel(const __grid_constant__ ObsParams p) {
   const Geometry& g = p.g;
@@ -579,7 +592,7 @@ __global__ void __launch_bounds__(256) observables_words_kernel(const __grid_con
   for (int b = 0; b < kWordObsBonds; ++b) A[b] = P[b] = 0u;
   const uint32_t* words = (const uint32_t*)p.spins + (size_t)w * g.nsite;
   const int stride = p.blocks_per_rep * blockDim.x;
-  // every thread of a warp runs the same iterations (the ballots need the whole warp)
+  // every thread of a warp runs the same iterations (the ballots and shuffles need the whole warp)
   for (int base = blockIdx.x * blockDim.x + warp * 32; base < g.nsite; base += stride) {
     const int site = base + lane;
     bool present = site < g.nsite && (p.mask == nullptr || p.mask[site] != 0);
@@ -594,11 +607,7 @@ __global__ void __launch_bounds__(256) observables_words_kernel(const __grid_con
     }
     const unsigned sites_here = __popc(__ballot_sync(0xFFFFFFFFu, present));
     S += sites_here;
-#pragma unroll 1
-    for (int l = 0; l < 32; ++l) {
-      const unsigned c = __popc(__ballot_sync(0xFFFFFFFFu, present && ((s0 >> l) & 1u)));
-      if (lane == l) U += c;
-    }
+    U += warp_lane_counts(present ? s0 : 0u, lane);
 #pragma unroll
     for (int b = 0; b < kWordObsBonds; ++b) {
       if (b >= nb) break;
@@ -612,11 +621,7 @@ __global__ void __launch_bounds__(256) observables_words_kernel(const __grid_con
         }
       }
       P[b] += __popc(__ballot_sync(0xFFFFFFFFu, pb));
-#pragma unroll 1
-      for (int l = 0; l < 32; ++l) {
-        const unsigned c = __popc(__ballot_sync(0xFFFFFFFFu, pb && ((xb >> l) & 1u)));
-        if (lane == l) A[b] += c;
-      }
+      A[b] += warp_lane_counts(xb, lane);
     }
   }
   // block sums per lane (integers), then FP64 per replica
