@@ -617,7 +617,7 @@ def main():
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "note": f"algorithmic {bpa} B/attempt; peak {peak_kind}; kernel = "
-                             f"{['generic', 'lattice', 'segment', 'tile', 'interleaved'][path['specialised'] // 100]} class update, "
+                             f"{'bitwise' if A.bitwise else ['generic', 'lattice', 'segment', 'tile', 'interleaved'][path['specialised'] // 100]} class update, "
                              f"{launches_per_sweep} launches per sweep (L2 group {path['group']}), "
                              f"step times from CUDA events"},
         "e2e": {"value": e2e, "unit": "attempts/ns", "h2d_bytes_per_step": int(beta_h.numel() * 4),
